@@ -1,0 +1,170 @@
+/* osn_tsdf_b200: B200-native (sm_100a) hash-blocked TSDF volume behind the
+ * reference's CUDA C ABI.
+ *
+ * The first block below is the reference's CUDA section of
+ * cpp/include/osn_tsdf/c_api.h (lines 223-293), re-declared with identical
+ * names, argument meanings and return codes, so a caller of the reference's
+ * CUDA arm (A3) links against this library instead without a source change.
+ * The CPU section of that header (c_api.h:181-213) is the reference's own CPU
+ * arm and is not part of this library.
+ *
+ * Conventions (same as the reference):
+ *   - positions are DEVICE pointers owned by the caller, 3 floats per point,
+ *     world space; the volume owns every other device allocation;
+ *   - calls are asynchronous on the volume's own stream; block_count,
+ *     drop_count, extract_mesh and synchronize wait for it;
+ *   - nothing throws across the boundary; one host thread per volume.
+ *
+ * The second block holds extensions with no counterpart in the reference;
+ * each says what it adds.
+ */
+#ifndef OSN_TSDF_B200_H
+#define OSN_TSDF_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct OsnTsdfCudaVolume OsnTsdfCudaVolume;
+
+/* Device pointers and parameters describing a volume's storage.
+ * Same 104-byte layout as the reference (c_api.h:228-245, size asserted at
+ * cpp/src/c_api_cuda.cu:14): table slots are (int64 key, int32 block_idx,
+ * int32 pad); tsdf/weight/r/g/b hold weighted SUMS, 512 floats per block at
+ * block_idx * 512, voxel (lx,ly,lz) at (lz*8+ly)*8+lx. */
+typedef struct {
+    void* table;          /* hash_mask+1 live slots, then 2^20 scratch slots (key -2) */
+    void* block_count;    /* int32 */
+    void* drop_count;     /* uint64 */
+    void* block_coord;    /* int32[3] per pool slot */
+    void* tsdf;           /* float, weighted sum */
+    void* weight;         /* float */
+    void* r;
+    void* g;
+    void* b;
+    uint32_t hash_mask;
+    uint32_t scratch_base;  /* first scratch slot = hash_mask + 1 */
+    int32_t pool_capacity;
+    int32_t block_dim;
+    float voxel_size_m;
+    float trunc_m;
+    float weight_cap;
+} OsnTsdfDeviceView;
+
+/* ---- reference CUDA section (cpp/include/osn_tsdf/c_api.h:247-293) ---- */
+
+/* c_api.h:247. NULL on invalid parameters or device allocation failure.
+ * trunc_m <= 0 selects 4 * voxel_size_m; weight_cap <= 0 disables capping.
+ * The table has next_pow2(2 * pool) slots, as in the reference. */
+OsnTsdfCudaVolume* osn_tsdf_cuda_create(float voxel_size_m, int32_t pool_capacity_blocks,
+                                        float trunc_m, float weight_cap);
+/* c_api.h:249 */
+void osn_tsdf_cuda_destroy(OsnTsdfCudaVolume* v);
+/* c_api.h:250. 1 when every device allocation succeeded. */
+int32_t osn_tsdf_cuda_valid(const OsnTsdfCudaVolume* v);
+/* c_api.h:253. Returns 0 on success, 1 on a NULL or invalid volume. */
+int32_t osn_tsdf_cuda_device_view(const OsnTsdfCudaVolume* v, OsnTsdfDeviceView* out);
+
+/* c_api.h:256-258. Allocate the blocks the batch's truncation bands touch.
+ * Returns 0 (queued), 1 on bad arguments (NULL volume or positions, n <= 0),
+ * 3 when the kernel launch failed. */
+int32_t osn_tsdf_cuda_allocate_blocks(OsnTsdfCudaVolume* v, const float* d_positions,
+                                      int32_t n_points, float cam_x, float cam_y, float cam_z,
+                                      float radius_m);
+/* c_api.h:259-261. Accumulate the batch into allocated blocks: unit weights,
+ * grey colour (128), contributions applied as if in (point, band step) order
+ * with the weight cap "accept while weight before < cap". Return codes as
+ * allocate_blocks. */
+int32_t osn_tsdf_cuda_update_voxels(OsnTsdfCudaVolume* v, const float* d_positions,
+                                    int32_t n_points, float cam_x, float cam_y, float cam_z,
+                                    float radius_m);
+/* c_api.h:264-265. Marching-tetrahedra triangle soup into HOST buffers:
+ * buffer_posnor holds vert_cap * 6 floats (position, face normal),
+ * buffer_rgb vert_cap * 3 bytes or NULL. Returns the vertex count, or -1 if
+ * vert_cap was too small or the arguments are invalid. */
+int32_t osn_tsdf_cuda_extract_mesh(OsnTsdfCudaVolume* v, float* buffer_posnor, uint8_t* buffer_rgb,
+                                   int32_t vert_cap, float min_weight, float iso);
+/* c_api.h:273. Back to the just-created state without reallocating. Waits. */
+int32_t osn_tsdf_cuda_reset(OsnTsdfCudaVolume* v);
+/* c_api.h:277-279. MEASUREMENT: allocate, adding every compare-exchange
+ * ATTEMPT to drop_count. Only meaningful on a pool that drops nothing. */
+int32_t osn_tsdf_cuda_allocate_counting_cas(OsnTsdfCudaVolume* v, const float* d_positions,
+                                            int32_t n_points, float cam_x, float cam_y,
+                                            float cam_z, float radius_m);
+/* c_api.h:282-284. MEASUREMENT: probe and read, never insert. */
+int32_t osn_tsdf_cuda_allocate_no_cas(OsnTsdfCudaVolume* v, const float* d_positions,
+                                      int32_t n_points, float cam_x, float cam_y, float cam_z,
+                                      float radius_m);
+/* c_api.h:287-289. MEASUREMENT: block index = hash slot, hash masked to the
+ * pool (which must be a power of two; 2 otherwise); no publication wait. */
+int32_t osn_tsdf_cuda_allocate_slot_index(OsnTsdfCudaVolume* v, const float* d_positions,
+                                          int32_t n_points, float cam_x, float cam_y, float cam_z,
+                                          float radius_m);
+/* c_api.h:291-293. Waiting reads of the counters; 0 for a NULL volume. */
+int32_t osn_tsdf_cuda_block_count(const OsnTsdfCudaVolume* v);
+uint64_t osn_tsdf_cuda_drop_count(const OsnTsdfCudaVolume* v);
+void osn_tsdf_cuda_synchronize(const OsnTsdfCudaVolume* v);
+
+/* ---- extensions (no counterpart in the reference) ---------------------- */
+
+/* Storage modes for create_ex. */
+#define OSN_TSDF_STORAGE_FP32 0
+
+/* create with an explicit table size. The reference always sizes the table
+ * to next_pow2(2 * pool), which caps its load factor below 0.5; hash_slots
+ * (a power of two >= 2, or 0 for the reference sizing) reaches the 0.75 and
+ * 0.9 load factors of the irregularity sweep. storage must be
+ * OSN_TSDF_STORAGE_FP32. */
+OsnTsdfCudaVolume* osn_tsdf_cuda_create_ex(float voxel_size_m, int32_t pool_capacity_blocks,
+                                           float trunc_m, float weight_cap, uint32_t hash_slots,
+                                           int32_t storage);
+
+/* allocate_blocks then update_voxels on the same points, as the reference's
+ * CPU integrate (cpp/src/volume.cpp:301-304). Return codes as allocate_blocks. */
+int32_t osn_tsdf_cuda_integrate(OsnTsdfCudaVolume* v, const float* d_positions, int32_t n_points,
+                                float cam_x, float cam_y, float cam_z, float radius_m);
+
+/* Extraction into DEVICE buffers (same layout as extract_mesh), skipping the
+ * host copy. Returns the vertex count or -1 (overflow / bad arguments).
+ * Waits for the count only. */
+int32_t osn_tsdf_cuda_extract_mesh_device(OsnTsdfCudaVolume* v, float* d_posnor, uint8_t* d_rgb,
+                                          int32_t vert_cap, float min_weight, float iso);
+
+/* Device error word, after waiting for the stream: 0 when every bounded
+ * wait in the kernels finished in time; bit 0 = a publication wait gave up,
+ * bit 1 = an update batch exceeded its scratch. */
+uint32_t osn_tsdf_cuda_status(const OsnTsdfCudaVolume* v);
+
+/* The volume's cudaStream_t, for callers that order their own work after it. */
+void* osn_tsdf_cuda_stream(const OsnTsdfCudaVolume* v);
+
+/* MEASUREMENT: one allocate pass that also records, per warp-leader probe
+ * sequence, how many slots it visited: hist[min(steps, n_bins-1)] += 1.
+ * hist is a HOST array of n_bins uint64 (overwritten). Also allocates. */
+int32_t osn_tsdf_cuda_allocate_probe_histogram(OsnTsdfCudaVolume* v, const float* d_positions,
+                                               int32_t n_points, float cam_x, float cam_y,
+                                               float cam_z, float radius_m, uint64_t* hist,
+                                               int32_t n_bins);
+
+/* Per-stage statistics of the last update_voxels call (waits):
+ * out[0] blocks that received a record, out[1] records binned,
+ * out[2] blocks that accepted at least one contribution,
+ * out[3] blocks that needed ordered cap selection. */
+int32_t osn_tsdf_cuda_last_update_stats(const OsnTsdfCudaVolume* v, int64_t* out4);
+
+/* Kernel timing. When enabled, every kernel launch of the volume is
+ * bracketed by CUDA events on the volume's stream; kernel_times reads (and
+ * waits for) the accumulated per-kernel milliseconds and launch counts.
+ * Kernel ids: 0 allocate, 1 update-count, 2 update-scan, 3 update-scatter,
+ * 4 update-apply, 5 extract, 6 reset. Returns the number of ids written. */
+int32_t osn_tsdf_cuda_set_timing(OsnTsdfCudaVolume* v, int32_t enabled);
+int32_t osn_tsdf_cuda_kernel_times(OsnTsdfCudaVolume* v, double* ms, int64_t* launches,
+                                   int32_t n_ids);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OSN_TSDF_B200_H */

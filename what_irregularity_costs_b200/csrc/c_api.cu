@@ -1,0 +1,221 @@
+// The C ABI: the reference's CUDA section of cpp/include/osn_tsdf/c_api.h
+// (implemented there by cpp/src/c_api_cuda.cu) plus this library's
+// extensions, declared in include/osn_tsdf_b200.h.
+#include <cstring>
+
+#include "../../include/osn_tsdf_b200.h"
+#include "volume.h"
+
+using osn_b200::BatchArgs;
+using osn_b200::Volume;
+
+static_assert(sizeof(OsnTsdfDeviceView) == 104,
+              "OsnTsdfDeviceView must keep the reference's 104-byte layout");
+
+struct OsnTsdfCudaVolume {
+    Volume vol;
+    OsnTsdfCudaVolume(float voxel, int32_t pool, float trunc, float cap, uint32_t slots)
+        : vol(voxel, pool, trunc, cap, slots) {}
+};
+
+namespace {
+
+BatchArgs batch(const float* pos, int32_t n, float cx, float cy, float cz, float radius) {
+    BatchArgs a;
+    a.pos = pos;
+    a.n = n;
+    a.cam_x = cx;
+    a.cam_y = cy;
+    a.cam_z = cz;
+    a.radius_sq = radius > 0.0f ? radius * radius : 0.0f;
+    return a;
+}
+
+bool usable(const OsnTsdfCudaVolume* v) { return v && v->vol.ok(); }
+
+// A batch's records carry the 32-bit id point * (2*steps+1) + step.
+bool batch_fits(const OsnTsdfCudaVolume* v, int32_t n) {
+    const int64_t steps = 2 * (int64_t)v->vol.dev().steps + 1;
+    return (int64_t)n * steps < (int64_t(1) << 32);
+}
+
+int32_t allocate_mode(OsnTsdfCudaVolume* v, const float* d_positions, int32_t n, float cx,
+                      float cy, float cz, float radius, int mode) {
+    if (!usable(v) || !d_positions || n <= 0) return 1;
+    return v->vol.allocate(batch(d_positions, n, cx, cy, cz, radius), mode, nullptr, 0) ==
+                   cudaSuccess
+               ? 0
+               : 3;
+}
+
+}  // namespace
+
+extern "C" {
+
+OsnTsdfCudaVolume* osn_tsdf_cuda_create(float voxel_size_m, int32_t pool_capacity_blocks,
+                                        float trunc_m, float weight_cap) {
+    return osn_tsdf_cuda_create_ex(voxel_size_m, pool_capacity_blocks, trunc_m, weight_cap, 0u,
+                                   OSN_TSDF_STORAGE_FP32);
+}
+
+OsnTsdfCudaVolume* osn_tsdf_cuda_create_ex(float voxel_size_m, int32_t pool_capacity_blocks,
+                                           float trunc_m, float weight_cap, uint32_t hash_slots,
+                                           int32_t storage) {
+    if (storage != OSN_TSDF_STORAGE_FP32) return nullptr;
+    if (!(voxel_size_m > 0.0f) || pool_capacity_blocks <= 0) return nullptr;
+    auto* v = new (std::nothrow) OsnTsdfCudaVolume(voxel_size_m, pool_capacity_blocks, trunc_m,
+                                                   weight_cap, hash_slots);
+    if (!v) return nullptr;
+    if (!v->vol.ok()) {
+        delete v;
+        return nullptr;
+    }
+    return v;
+}
+
+void osn_tsdf_cuda_destroy(OsnTsdfCudaVolume* v) { delete v; }
+
+int32_t osn_tsdf_cuda_valid(const OsnTsdfCudaVolume* v) { return usable(v) ? 1 : 0; }
+
+int32_t osn_tsdf_cuda_device_view(const OsnTsdfCudaVolume* v, OsnTsdfDeviceView* out) {
+    if (!usable(v) || !out) return 1;
+    const auto& d = v->vol.dev();
+    out->table = d.table;
+    out->block_count = d.block_count;
+    out->drop_count = d.drop_count;
+    out->block_coord = d.block_coord;
+    out->tsdf = d.tsdf;
+    out->weight = d.weight;
+    out->r = d.r;
+    out->g = d.g;
+    out->b = d.b;
+    out->hash_mask = d.hash_mask;
+    out->scratch_base = d.hash_mask + 1;
+    out->pool_capacity = d.pool_capacity;
+    out->block_dim = osn_b200::kBlockDim;
+    out->voxel_size_m = d.voxel_size;
+    out->trunc_m = d.trunc;
+    out->weight_cap = d.weight_cap;
+    return 0;
+}
+
+int32_t osn_tsdf_cuda_allocate_blocks(OsnTsdfCudaVolume* v, const float* d_positions,
+                                      int32_t n_points, float cam_x, float cam_y, float cam_z,
+                                      float radius_m) {
+    return allocate_mode(v, d_positions, n_points, cam_x, cam_y, cam_z, radius_m,
+                         osn_b200::kAllocInsert);
+}
+
+int32_t osn_tsdf_cuda_update_voxels(OsnTsdfCudaVolume* v, const float* d_positions,
+                                    int32_t n_points, float cam_x, float cam_y, float cam_z,
+                                    float radius_m) {
+    if (!usable(v) || !d_positions || n_points <= 0 || !batch_fits(v, n_points)) return 1;
+    return v->vol.update(batch(d_positions, n_points, cam_x, cam_y, cam_z, radius_m)) ==
+                   cudaSuccess
+               ? 0
+               : 3;
+}
+
+int32_t osn_tsdf_cuda_integrate(OsnTsdfCudaVolume* v, const float* d_positions, int32_t n_points,
+                                float cam_x, float cam_y, float cam_z, float radius_m) {
+    const int32_t rc =
+        osn_tsdf_cuda_allocate_blocks(v, d_positions, n_points, cam_x, cam_y, cam_z, radius_m);
+    if (rc) return rc;
+    return osn_tsdf_cuda_update_voxels(v, d_positions, n_points, cam_x, cam_y, cam_z, radius_m);
+}
+
+int32_t osn_tsdf_cuda_extract_mesh(OsnTsdfCudaVolume* v, float* buffer_posnor, uint8_t* buffer_rgb,
+                                   int32_t vert_cap, float min_weight, float iso) {
+    if (!usable(v) || !buffer_posnor || vert_cap <= 0) return -1;
+    return v->vol.extract(buffer_posnor, buffer_rgb, vert_cap, min_weight, iso, true);
+}
+
+int32_t osn_tsdf_cuda_extract_mesh_device(OsnTsdfCudaVolume* v, float* d_posnor, uint8_t* d_rgb,
+                                          int32_t vert_cap, float min_weight, float iso) {
+    if (!usable(v) || !d_posnor || vert_cap <= 0) return -1;
+    return v->vol.extract(d_posnor, d_rgb, vert_cap, min_weight, iso, false);
+}
+
+int32_t osn_tsdf_cuda_reset(OsnTsdfCudaVolume* v) {
+    if (!usable(v)) return 1;
+    return v->vol.reset() == cudaSuccess ? 0 : 3;
+}
+
+int32_t osn_tsdf_cuda_allocate_counting_cas(OsnTsdfCudaVolume* v, const float* d_positions,
+                                            int32_t n_points, float cam_x, float cam_y,
+                                            float cam_z, float radius_m) {
+    return allocate_mode(v, d_positions, n_points, cam_x, cam_y, cam_z, radius_m,
+                         osn_b200::kAllocCountingCas);
+}
+
+int32_t osn_tsdf_cuda_allocate_no_cas(OsnTsdfCudaVolume* v, const float* d_positions,
+                                      int32_t n_points, float cam_x, float cam_y, float cam_z,
+                                      float radius_m) {
+    return allocate_mode(v, d_positions, n_points, cam_x, cam_y, cam_z, radius_m,
+                         osn_b200::kAllocNoCas);
+}
+
+int32_t osn_tsdf_cuda_allocate_slot_index(OsnTsdfCudaVolume* v, const float* d_positions,
+                                          int32_t n_points, float cam_x, float cam_y, float cam_z,
+                                          float radius_m) {
+    return allocate_mode(v, d_positions, n_points, cam_x, cam_y, cam_z, radius_m,
+                         osn_b200::kAllocSlotIndex);
+}
+
+int32_t osn_tsdf_cuda_allocate_probe_histogram(OsnTsdfCudaVolume* v, const float* d_positions,
+                                               int32_t n_points, float cam_x, float cam_y,
+                                               float cam_z, float radius_m, uint64_t* hist,
+                                               int32_t n_bins) {
+    if (!usable(v) || !d_positions || n_points <= 0 || !hist || n_bins <= 0 || n_bins > 64) return 1;
+    unsigned long long* d_hist = nullptr;
+    cudaStream_t s = v->vol.stream();
+    if (cudaMallocAsync(&d_hist, (size_t)n_bins * sizeof(unsigned long long), s) != cudaSuccess)
+        return 3;
+    cudaMemsetAsync(d_hist, 0, (size_t)n_bins * sizeof(unsigned long long), s);
+    const cudaError_t e = v->vol.allocate(batch(d_positions, n_points, cam_x, cam_y, cam_z, radius_m),
+                                          osn_b200::kAllocProbeHist, d_hist, n_bins);
+    cudaMemcpyAsync(hist, d_hist, (size_t)n_bins * sizeof(unsigned long long),
+                    cudaMemcpyDeviceToHost, s);
+    cudaFreeAsync(d_hist, s);
+    cudaStreamSynchronize(s);
+    return e == cudaSuccess ? 0 : 3;
+}
+
+int32_t osn_tsdf_cuda_block_count(const OsnTsdfCudaVolume* v) {
+    return usable(v) ? const_cast<OsnTsdfCudaVolume*>(v)->vol.block_count() : 0;
+}
+
+uint64_t osn_tsdf_cuda_drop_count(const OsnTsdfCudaVolume* v) {
+    return usable(v) ? const_cast<OsnTsdfCudaVolume*>(v)->vol.drop_count() : 0;
+}
+
+void osn_tsdf_cuda_synchronize(const OsnTsdfCudaVolume* v) {
+    if (usable(v)) const_cast<OsnTsdfCudaVolume*>(v)->vol.synchronize();
+}
+
+uint32_t osn_tsdf_cuda_status(const OsnTsdfCudaVolume* v) {
+    return usable(v) ? const_cast<OsnTsdfCudaVolume*>(v)->vol.status() : 0u;
+}
+
+void* osn_tsdf_cuda_stream(const OsnTsdfCudaVolume* v) {
+    return usable(v) ? (void*)v->vol.stream() : nullptr;
+}
+
+int32_t osn_tsdf_cuda_last_update_stats(const OsnTsdfCudaVolume* v, int64_t* out4) {
+    if (!usable(v) || !out4) return 1;
+    return const_cast<OsnTsdfCudaVolume*>(v)->vol.last_update_stats(out4) ? 0 : 3;
+}
+
+int32_t osn_tsdf_cuda_set_timing(OsnTsdfCudaVolume* v, int32_t enabled) {
+    if (!usable(v)) return 1;
+    v->vol.set_timing(enabled != 0);
+    return 0;
+}
+
+int32_t osn_tsdf_cuda_kernel_times(OsnTsdfCudaVolume* v, double* ms, int64_t* launches,
+                                   int32_t n_ids) {
+    if (!usable(v) || n_ids <= 0) return 0;
+    return v->vol.kernel_times(ms, launches, n_ids);
+}
+
+}  // extern "C"

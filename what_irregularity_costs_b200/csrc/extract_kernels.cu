@@ -1,0 +1,314 @@
+// Extract: marching-tetrahedra triangle soup over every allocated block.
+//
+// Reference: cpp/src/marching_tets.cpp:31-245 (CPU arm) and
+// cpp/src/marching_tets_cuda.cu:33-167 (CUDA arm: one CTA per block, one
+// thread per cube, a full hash probe for each of the 8 corners of every cube
+// and one global atomic per emitting tetrahedron).
+//
+// B200 design. One CTA per block, one thread per cube, but the 7 neighbour
+// blocks are looked up once per CTA and the 9x9x9 halo of corner samples
+// (mean TSDF, validity, mean colour) is staged in shared memory with
+// coalesced reads, so the corner loop reads shared memory only. Emission is
+// compacted: each thread counts its vertices, a block-wide scan (warp
+// shuffles) gives every thread its offset, and one atomic per CTA reserves
+// the block's output range, so a block's triangles are contiguous and in a
+// fixed order (cube, then tetrahedron).
+//
+// Arithmetic follows the reference operation for operation, unfused, so a
+// volume whose voxels match bit-for-bit extracts bit-identical vertices.
+#include <algorithm>
+
+#include "volume.h"
+
+namespace osn_b200 {
+namespace {
+
+constexpr int kExtractThreads = 512;
+constexpr int kHalo = 9;
+constexpr int kHaloCells = kHalo * kHalo * kHalo;
+
+// marching_tets.cpp:37-40: six tetrahedra around the 0-7 diagonal.
+__constant__ int c_tets[6][4] = {
+    {0, 5, 1, 7}, {0, 1, 3, 7}, {0, 3, 2, 7}, {0, 6, 4, 7}, {0, 4, 5, 7}, {0, 2, 6, 7},
+};
+
+struct Halo {
+    float val[kHaloCells];
+    float col[3][kHaloCells];
+    unsigned char ok[kHaloCells];
+};
+
+// Case table of marching_tets.cpp:165-182 as (a, b, c, d, quad).
+__device__ __forceinline__ int tet_case(int code, const int* q, int& a, int& b, int& c, int& d) {
+    const int i0 = q[0], i1 = q[1], i2 = q[2], i3 = q[3];
+    switch (code) {
+        case 0x01: case 0x0E: a = i0; b = i1; c = i2; d = i3; return 1;
+        case 0x02: case 0x0D: a = i1; b = i0; c = i2; d = i3; return 1;
+        case 0x04: case 0x0B: a = i2; b = i0; c = i1; d = i3; return 1;
+        case 0x08: case 0x07: a = i3; b = i0; c = i1; d = i2; return 1;
+        case 0x03: a = i0; b = i1; c = i2; d = i3; return 2;
+        case 0x0C: a = i2; b = i3; c = i0; d = i1; return 2;
+        case 0x05: a = i0; b = i2; c = i1; d = i3; return 2;
+        case 0x0A: a = i1; b = i3; c = i0; d = i2; return 2;
+        case 0x06: a = i1; b = i2; c = i0; d = i3; return 2;
+        case 0x09: a = i0; b = i3; c = i1; d = i2; return 2;
+        default: return 0;
+    }
+}
+
+struct Cube {
+    int vx, vy, vz;  // voxel coordinate of corner 0
+    int h0;          // halo index of corner 0
+    float vs;
+};
+
+__device__ __forceinline__ int corner_halo(const Cube& q, int c) {
+    return q.h0 + ((c >> 2) & 1) * kHalo * kHalo + ((c >> 1) & 1) * kHalo + (c & 1);
+}
+
+// Voxel centre of a corner (marching_tets.cpp:126-128).
+__device__ __forceinline__ void corner_pos(const Cube& q, int c, float p[3]) {
+    p[0] = __fmul_rn(__fadd_rn((float)(q.vx + (c & 1)), 0.5f), q.vs);
+    p[1] = __fmul_rn(__fadd_rn((float)(q.vy + ((c >> 1) & 1)), 0.5f), q.vs);
+    p[2] = __fmul_rn(__fadd_rn((float)(q.vz + ((c >> 2) & 1)), 0.5f), q.vs);
+}
+
+struct Vert {
+    float p[3];
+    float c[3];
+};
+
+// marching_tets.cpp:59-80: position-ordered interpolation.
+__device__ __forceinline__ Vert interp(const Halo& h, const Cube& q, float iso, int ia, int ib,
+                                       bool want_col) {
+    float pa[3], pb[3];
+    corner_pos(q, ia, pa);
+    corner_pos(q, ib, pb);
+    const bool sw = (pb[0] < pa[0]) || (pb[0] == pa[0] && pb[1] < pa[1]) ||
+                    (pb[0] == pa[0] && pb[1] == pa[1] && pb[2] < pa[2]);
+    const int i0 = sw ? ib : ia, i1 = sw ? ia : ib;
+    const float* p0 = sw ? pb : pa;
+    const float* p1 = sw ? pa : pb;
+    const int h0 = corner_halo(q, i0), h1 = corner_halo(q, i1);
+    const float v0 = h.val[h0], v1 = h.val[h1];
+    const float den = __fsub_rn(v1, v0);
+    const float t = fabsf(den) < 1e-12f ? 0.5f : __fdiv_rn(__fsub_rn(iso, v0), den);
+    const float tc = fminf(fmaxf(t, 0.0f), 1.0f);
+    Vert o;
+    for (int k = 0; k < 3; ++k) o.p[k] = __fadd_rn(p0[k], __fmul_rn(tc, __fsub_rn(p1[k], p0[k])));
+    if (want_col) {
+        for (int k = 0; k < 3; ++k) {
+            const float c0 = h.col[k][h0], c1 = h.col[k][h1];
+            o.c[k] = __fadd_rn(c0, __fmul_rn(tc, __fsub_rn(c1, c0)));
+        }
+    }
+    return o;
+}
+
+__device__ __forceinline__ void emit_triangle(const Vert& a, const Vert& b, const Vert& c,
+                                              float* posnor, uint8_t* rgb, int64_t at) {
+    // marching_tets.cpp:206-218: face normal of the emitted triangle.
+    const float e1[3] = {__fsub_rn(b.p[0], a.p[0]), __fsub_rn(b.p[1], a.p[1]), __fsub_rn(b.p[2], a.p[2])};
+    const float e2[3] = {__fsub_rn(c.p[0], a.p[0]), __fsub_rn(c.p[1], a.p[1]), __fsub_rn(c.p[2], a.p[2])};
+    float nx = __fsub_rn(__fmul_rn(e1[1], e2[2]), __fmul_rn(e1[2], e2[1]));
+    float ny = __fsub_rn(__fmul_rn(e1[2], e2[0]), __fmul_rn(e1[0], e2[2]));
+    float nz = __fsub_rn(__fmul_rn(e1[0], e2[1]), __fmul_rn(e1[1], e2[0]));
+    const float len =
+        __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(nx, nx), __fmul_rn(ny, ny)), __fmul_rn(nz, nz)));
+    if (len > 1e-20f) {
+        nx = __fdiv_rn(nx, len);
+        ny = __fdiv_rn(ny, len);
+        nz = __fdiv_rn(nz, len);
+    }
+    const Vert* vs[3] = {&a, &b, &c};
+    for (int k = 0; k < 3; ++k) {
+        float* dst = posnor + (at + k) * 6;
+        dst[0] = vs[k]->p[0];
+        dst[1] = vs[k]->p[1];
+        dst[2] = vs[k]->p[2];
+        dst[3] = nx;
+        dst[4] = ny;
+        dst[5] = nz;
+        if (rgb) {
+            uint8_t* cc = rgb + (at + k) * 3;
+            cc[0] = (uint8_t)fminf(fmaxf(vs[k]->c[0], 0.0f), 255.0f);
+            cc[1] = (uint8_t)fminf(fmaxf(vs[k]->c[1], 0.0f), 255.0f);
+            cc[2] = (uint8_t)fminf(fmaxf(vs[k]->c[2], 0.0f), 255.0f);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kExtractThreads)
+extract_kernel(DevVolume v, int32_t n_blocks, float min_w, float iso, float* out_posnor,
+               uint8_t* out_rgb, int32_t cap, int32_t* ctl) {
+    __shared__ Halo h;
+    __shared__ int s_nb[8];
+    __shared__ int s_warp[kExtractThreads / 32];
+    __shared__ int s_base;
+
+    const int b = blockIdx.x;
+    if (b >= n_blocks) return;
+    const int t = threadIdx.x;
+    const bool want_col = out_rgb != nullptr;
+    const BlockCoord bc = v.block_coord[b];
+    if (t < 8) {
+        const int dx = t & 1, dy = (t >> 1) & 1, dz = (t >> 2) & 1;
+        const int nx = bc.x + dx, ny = bc.y + dy, nz = bc.z + dz;
+        s_nb[t] = t == 0 ? b : find_block(v, nx, ny, nz, pack_key(nx, ny, nz));
+    }
+    __syncthreads();
+
+    // Stage the halo: corner samples of this block plus the +x/+y/+z faces,
+    // edges and corner of its neighbours (volume.cpp:306-329 per sample).
+    for (int k = t; k < kHaloCells; k += kExtractThreads) {
+        const int hx = k % kHalo, hy = (k / kHalo) % kHalo, hz = k / (kHalo * kHalo);
+        const int nb = s_nb[(hx >> 3) | ((hy >> 3) << 1) | ((hz >> 3) << 2)];
+        unsigned char ok = 0;
+        h.val[k] = 0.0f;
+        if (nb >= 0) {
+            const size_t idx = (size_t)nb * kBlockVoxels + (size_t)((((hz & 7) * kBlockDim) + (hy & 7)) * kBlockDim + (hx & 7));
+            const float w = v.weight[idx];
+            if (!(w < min_w || w <= 0.0f)) {
+                ok = 1;
+                const float inv = __fdiv_rn(1.0f, w);
+                h.val[k] = __fmul_rn(v.tsdf[idx], inv);
+                if (want_col) {
+                    h.col[0][k] = __fmul_rn(v.r[idx], inv);
+                    h.col[1][k] = __fmul_rn(v.g[idx], inv);
+                    h.col[2][k] = __fmul_rn(v.b[idx], inv);
+                }
+            }
+        }
+        h.ok[k] = ok;
+    }
+    __syncthreads();
+
+    Cube q;
+    const int lx = t & 7, ly = (t >> 3) & 7, lz = t >> 6;
+    q.vx = bc.x * kBlockDim + lx;
+    q.vy = bc.y * kBlockDim + ly;
+    q.vz = bc.z * kBlockDim + lz;
+    q.h0 = (lz * kHalo + ly) * kHalo + lx;
+    q.vs = v.voxel_size;
+
+    bool all_ok = true;
+    unsigned below = 0;  // bit c set when corner c is below iso
+    for (int c = 0; c < 8; ++c) {
+        const int hc = corner_halo(q, c);
+        all_ok = all_ok && h.ok[hc];
+        if (h.val[hc] < iso) below |= 1u << c;
+    }
+
+    int n_vert = 0;
+    if (all_ok) {
+        for (int k = 0; k < 6; ++k) {
+            const int* tq = c_tets[k];
+            const int code = ((below >> tq[0]) & 1) | (((below >> tq[1]) & 1) << 1) |
+                             (((below >> tq[2]) & 1) << 2) | (((below >> tq[3]) & 1) << 3);
+            int a, bb, c, d;
+            n_vert += 3 * tet_case(code, tq, a, bb, c, d);
+        }
+    }
+
+    // Block-wide exclusive scan of the vertex counts.
+    const int lane = t & 31, warp = t >> 5;
+    int x = n_vert;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        int w = lane < kExtractThreads / 32 ? s_warp[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        if (lane < kExtractThreads / 32) s_warp[lane] = w;
+        if (lane == kExtractThreads / 32 - 1) {
+            const int total = w;
+            int base = 0;
+            if (total > 0) {
+                base = atomicAdd(&ctl[0], total);
+                if ((int64_t)base + total > (int64_t)cap) {
+                    atomicExch(&ctl[1], 1);
+                    base = -1;
+                }
+            }
+            s_base = base;
+        }
+    }
+    __syncthreads();
+    if (s_base < 0 || n_vert == 0) return;
+    int64_t at = (int64_t)s_base + (warp ? s_warp[warp - 1] : 0) + x - n_vert;
+
+    for (int k = 0; k < 6; ++k) {
+        const int* tq = c_tets[k];
+        const int code = ((below >> tq[0]) & 1) | (((below >> tq[1]) & 1) << 1) |
+                         (((below >> tq[2]) & 1) << 2) | (((below >> tq[3]) & 1) << 3);
+        int a, bb, c, d;
+        const int kind = tet_case(code, tq, a, bb, c, d);
+        if (kind == 1) {
+            const Vert v0 = interp(h, q, iso, a, bb, want_col);
+            const Vert v1 = interp(h, q, iso, a, c, want_col);
+            const Vert v2 = interp(h, q, iso, a, d, want_col);
+            emit_triangle(v0, v1, v2, out_posnor, out_rgb, at);
+            at += 3;
+        } else if (kind == 2) {
+            const Vert ac = interp(h, q, iso, a, c, want_col);
+            const Vert ad = interp(h, q, iso, a, d, want_col);
+            const Vert bd = interp(h, q, iso, bb, d, want_col);
+            const Vert bcv = interp(h, q, iso, bb, c, want_col);
+            emit_triangle(ac, ad, bd, out_posnor, out_rgb, at);
+            emit_triangle(ac, bd, bcv, out_posnor, out_rgb, at + 3);
+            at += 6;
+        }
+    }
+}
+
+__global__ void reset_table_kernel(HashEntry* table, uint32_t count, long long key) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
+        table[k].key = key;
+        table[k].block_idx = -1;
+        table[k].pad = 0;
+    }
+}
+
+__global__ void reset_voxels_kernel(DevVolume v, size_t n_vec4) {
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n_vec4;
+         k += (size_t)gridDim.x * blockDim.x) {
+        reinterpret_cast<float4*>(v.tsdf)[k] = z;
+        reinterpret_cast<float4*>(v.weight)[k] = z;
+        reinterpret_cast<float4*>(v.r)[k] = z;
+        reinterpret_cast<float4*>(v.g)[k] = z;
+        reinterpret_cast<float4*>(v.b)[k] = z;
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_extract(const DevVolume& v, int32_t n_blocks, float min_w, float iso,
+                           float* posnor, uint8_t* rgb, int32_t cap, int32_t* ctl, cudaStream_t s) {
+    if (n_blocks <= 0) return cudaSuccess;
+    extract_kernel<<<n_blocks, kExtractThreads, 0, s>>>(v, n_blocks, min_w, iso, posnor, rgb, cap, ctl);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_reset_table(HashEntry* first, uint32_t count, long long key, cudaStream_t s) {
+    if (count == 0) return cudaSuccess;
+    const int grid = (int)std::min<uint32_t>((count + 255) / 256, 148u * 16u);
+    reset_table_kernel<<<grid, 256, 0, s>>>(first, count, key);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_reset_voxels(const DevVolume& v, int32_t n_blocks, cudaStream_t s) {
+    if (n_blocks <= 0) return cudaSuccess;
+    const size_t n_vec4 = (size_t)n_blocks * kBlockVoxels / 4;
+    const int grid = (int)std::min<size_t>((n_vec4 + 255) / 256, (size_t)148 * 16);
+    reset_voxels_kernel<<<grid, 256, 0, s>>>(v, n_vec4);
+    return cudaGetLastError();
+}
+
+}  // namespace osn_b200

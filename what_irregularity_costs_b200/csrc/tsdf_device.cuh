@@ -1,0 +1,186 @@
+// Device-side layout and geometry shared by every kernel of the library.
+//
+// Layout (bit-compatible with the reference, cpp/include/osn_tsdf/types.hpp):
+//   - hash slot: 16 bytes {int64 key, int32 block_idx, int32 pad}; key is the
+//     packed block coordinate, kEmptyKey (-1) marks a free slot (types.hpp:44-50,
+//     :87-91); the 2^20 slots past the live table hold kScratchKey (-2) as in
+//     cpp/src/cuda_impl.cuh:84-85;
+//   - key = (x+2^20)<<42 | (y+2^20)<<21 | (z+2^20) (types.hpp:64-69);
+//   - slot = Teschner multiply-xor hash & mask (types.hpp:150-155);
+//   - voxels: five SoA float arrays of weighted sums, 512 per block at
+//     block_idx*512, voxel (lx,ly,lz) at (lz*8+ly)*8+lx (volume.cpp:271-276).
+//
+// The band walk is written with explicit round-to-nearest intrinsics so that
+// no multiply-add is contracted: the reference's CPU arm is compiled for
+// baseline x86-64 (no FMA) and every sample position, voxel index and signed
+// distance here must round exactly as it does there for the allocated block
+// set to be bit-identical.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace osn_b200 {
+
+constexpr int kBlockDim = 8;
+constexpr int kBlockVoxels = 512;
+constexpr long long kEmptyKey = -1;
+constexpr long long kScratchKey = -2;
+// A slot whose insertion was rolled back because the pool was full. Lookups
+// probe past it (unlike an empty slot), so a block inserted further along the
+// probe sequence while the rollback was in flight stays reachable.
+constexpr long long kReleasedKey = -3;
+constexpr long long kNoKey = -4;  // "no request" marker inside warps; never stored
+constexpr long long kCoordBias = 1LL << 20;
+constexpr int kCoordBits = 21;
+constexpr uint32_t kScratchSlots = 1u << 20;
+// Bound on every device-side wait (iterations of ~100 ns): far above any
+// legitimate publication delay, far below a watchdog.
+constexpr int kSpinLimit = 1 << 20;
+
+// Bits of the device status word.
+constexpr uint32_t kStatusSpinTimeout = 1u;
+constexpr uint32_t kStatusScratchOverflow = 2u;
+
+struct HashEntry {
+    long long key;
+    int32_t block_idx;
+    int32_t pad;
+};
+static_assert(sizeof(HashEntry) == 16, "hash slot must stay 16 bytes");
+
+struct BlockCoord {
+    int32_t x, y, z;
+};
+
+// Everything a kernel needs to address one volume.
+struct DevVolume {
+    HashEntry* table;
+    uint32_t hash_mask;
+    int32_t pool_capacity;
+    int32_t* block_count;
+    unsigned long long* drop_count;
+    BlockCoord* block_coord;
+    float* tsdf;
+    float* weight;
+    float* r;
+    float* g;
+    float* b;
+    float voxel_size;
+    float inv_voxel;  // 1.0f / voxel_size, computed on the host (volume.cpp:148)
+    float trunc;
+    float inv_trunc;  // 1.0f / trunc (volume.cpp:203)
+    float weight_cap;
+    int32_t steps;    // max(1, ceil(trunc * inv_voxel)) (volume.cpp:171)
+    uint32_t* status;
+};
+
+// One batch: camera origin and squared far cutoff (0 disables).
+struct BatchArgs {
+    const float* pos;
+    int32_t n;
+    float cam_x, cam_y, cam_z;
+    float radius_sq;
+};
+
+__device__ __forceinline__ long long pack_key(int32_t x, int32_t y, int32_t z) {
+    return (((long long)x + kCoordBias) << (2 * kCoordBits)) |
+           (((long long)y + kCoordBias) << kCoordBits) | ((long long)z + kCoordBias);
+}
+
+__device__ __forceinline__ uint32_t hash_slot(int32_t x, int32_t y, int32_t z, uint32_t mask) {
+    return ((uint32_t)x * 73856093u ^ (uint32_t)y * 19349663u ^ (uint32_t)z * 83492791u) & mask;
+}
+
+__device__ __forceinline__ int32_t unpack_axis(long long key, int shift) {
+    return (int32_t)((key >> shift) & ((1LL << kCoordBits) - 1)) - (int32_t)kCoordBias;
+}
+
+// ---- coherent memory helpers (the table is mutated by other SMs) ----------
+
+__device__ __forceinline__ long long ld_relaxed_s64(const long long* p) {
+    long long v;
+    asm volatile("ld.relaxed.gpu.global.s64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ int ld_acquire_s32(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ int ld_relaxed_s32(const int* p) {
+    int v;
+    asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// ---- the band walk (volume.cpp:153-196 and :208-296) ----------------------
+
+struct Ray {
+    float px, py, pz;
+    float ux, uy, uz;
+    float dist;
+};
+
+// Point set-up. False when the point is gated out by the far cutoff or sits
+// on the camera (volume.cpp:158-166).
+__device__ __forceinline__ bool ray_setup(const BatchArgs& a, int i, Ray& r) {
+    r.px = a.pos[(size_t)i * 3 + 0];
+    r.py = a.pos[(size_t)i * 3 + 1];
+    r.pz = a.pos[(size_t)i * 3 + 2];
+    const float dx = __fsub_rn(r.px, a.cam_x);
+    const float dy = __fsub_rn(r.py, a.cam_y);
+    const float dz = __fsub_rn(r.pz, a.cam_z);
+    const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+    if (a.radius_sq > 0.0f && d2 > a.radius_sq) return false;
+    r.dist = __fsqrt_rn(d2);
+    if (!(r.dist > 1e-6f)) return false;
+    r.ux = __fdiv_rn(dx, r.dist);
+    r.uy = __fdiv_rn(dy, r.dist);
+    r.uz = __fdiv_rn(dz, r.dist);
+    return true;
+}
+
+// Band sample s in [-steps, steps]: voxel index and signed distance at the
+// voxel CENTRE. False when the voxel is fully occluded (sdf < -trunc), the
+// gate both passes apply (volume.cpp:185-191, :260-268).
+__device__ __forceinline__ bool band_sample(const DevVolume& v, const BatchArgs& a, const Ray& r,
+                                            int s, int& vx, int& vy, int& vz, float& sdf) {
+    const float t = __fmul_rn((float)s, v.voxel_size);
+    vx = (int)floorf(__fmul_rn(__fadd_rn(r.px, __fmul_rn(r.ux, t)), v.inv_voxel));
+    vy = (int)floorf(__fmul_rn(__fadd_rn(r.py, __fmul_rn(r.uy, t)), v.inv_voxel));
+    vz = (int)floorf(__fmul_rn(__fadd_rn(r.pz, __fmul_rn(r.uz, t)), v.inv_voxel));
+    const float ex = __fsub_rn(__fmul_rn(__fadd_rn((float)vx, 0.5f), v.voxel_size), a.cam_x);
+    const float ey = __fsub_rn(__fmul_rn(__fadd_rn((float)vy, 0.5f), v.voxel_size), a.cam_y);
+    const float ez = __fsub_rn(__fmul_rn(__fadd_rn((float)vz, 0.5f), v.voxel_size), a.cam_z);
+    const float dv =
+        __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(ex, ex), __fmul_rn(ey, ey)), __fmul_rn(ez, ez)));
+    sdf = __fsub_rn(r.dist, dv);
+    return !(sdf < -v.trunc);
+}
+
+// ---- lookups after allocation has completed --------------------------------
+
+// Block index of a key, or -1 (volume.cpp:71-92). Only valid in kernels that
+// run after the allocating kernel finished, so every index is published and
+// the non-coherent 128-bit load of a whole slot is safe.
+__device__ __forceinline__ int32_t find_block(const DevVolume& v, int32_t bx, int32_t by, int32_t bz,
+                                              long long want) {
+    const uint32_t size = v.hash_mask + 1;
+    const uint32_t start = hash_slot(bx, by, bz, v.hash_mask);
+    for (uint32_t p = 0; p < size; ++p) {
+        const int4 raw = __ldg(reinterpret_cast<const int4*>(&v.table[(start + p) & v.hash_mask]));
+        const long long key = ((long long)(unsigned)raw.y << 32) | (unsigned)raw.x;
+        if (key == want) return (raw.z >= 0 && raw.z < v.pool_capacity) ? raw.z : -1;
+        if (key == kEmptyKey) return -1;
+    }
+    return -1;
+}
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+}  // namespace osn_b200

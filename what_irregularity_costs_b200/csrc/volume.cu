@@ -1,0 +1,320 @@
+// Host side of one volume: device memory, the volume's stream, stage
+// sequencing, counters and kernel timing.
+//
+// Reference: cpp/src/cuda_impl.cuh:44-112 (device allocation, table fill,
+// scratch slots) and cpp/src/volume_cuda.cu:343-480 (stream-ordered stages,
+// reset, counters).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+#include "volume.h"
+
+namespace osn_b200 {
+
+namespace {
+uint32_t next_pow2(uint32_t v) {  // cpp/src/volume.cpp:14-19
+    if (v < 2) return 2;
+    --v;
+    v |= v >> 1; v |= v >> 2; v |= v >> 4; v |= v >> 8; v |= v >> 16;
+    return v + 1;
+}
+
+#define OSN_TRY(expr)                                                                       \
+    do {                                                                                    \
+        const cudaError_t err_ = (expr);                                                    \
+        if (err_ != cudaSuccess) {                                                          \
+            std::fprintf(stderr, "[osn_tsdf_b200] %s:%d: %s -> %s\n", __FILE__, __LINE__,   \
+                         #expr, cudaGetErrorString(err_));                                  \
+            return false;                                                                   \
+        }                                                                                   \
+    } while (0)
+}  // namespace
+
+Volume::Volume(float voxel, int32_t pool, float trunc_m, float weight_cap, uint32_t hash_slots) {
+    if (!(voxel > 0.0f) || pool <= 0) return;
+    if (hash_slots != 0 && (hash_slots < 2 || (hash_slots & (hash_slots - 1)) != 0)) return;
+    dv_.voxel_size = voxel;
+    dv_.inv_voxel = 1.0f / voxel;
+    dv_.trunc = trunc_m > 0.0f ? trunc_m : 4.0f * voxel;  // types.hpp:104-106
+    dv_.inv_trunc = 1.0f / dv_.trunc;
+    dv_.weight_cap = weight_cap;
+    dv_.pool_capacity = pool;
+    dv_.steps = std::max(1, (int32_t)std::ceil(dv_.trunc * dv_.inv_voxel));
+    ok_ = alloc_device(hash_slots);
+}
+
+bool Volume::alloc_device(uint32_t hash_slots) {
+    const uint32_t size = hash_slots ? hash_slots : next_pow2((uint32_t)dv_.pool_capacity * 2u);
+    dv_.hash_mask = size - 1;
+    const size_t n_vox = (size_t)dv_.pool_capacity * kBlockVoxels;
+    int dev = 0;
+    OSN_TRY(cudaGetDevice(&dev));
+    OSN_TRY(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, dev));
+    OSN_TRY(cudaStreamCreate(&stream_));
+    OSN_TRY(cudaMalloc(&dv_.table, ((size_t)size + kScratchSlots) * sizeof(HashEntry)));
+    OSN_TRY(cudaMalloc(&dv_.block_count, sizeof(int32_t)));
+    OSN_TRY(cudaMalloc(&dv_.drop_count, sizeof(unsigned long long)));
+    OSN_TRY(cudaMalloc(&dv_.status, sizeof(uint32_t)));
+    OSN_TRY(cudaMalloc(&dv_.block_coord, (size_t)dv_.pool_capacity * sizeof(BlockCoord)));
+    OSN_TRY(cudaMalloc(&dv_.tsdf, n_vox * sizeof(float)));
+    OSN_TRY(cudaMalloc(&dv_.weight, n_vox * sizeof(float)));
+    OSN_TRY(cudaMalloc(&dv_.r, n_vox * sizeof(float)));
+    OSN_TRY(cudaMalloc(&dv_.g, n_vox * sizeof(float)));
+    OSN_TRY(cudaMalloc(&dv_.b, n_vox * sizeof(float)));
+    OSN_TRY(cudaMalloc(&us_.blk_cnt, (size_t)dv_.pool_capacity * sizeof(int32_t)));
+    OSN_TRY(cudaMalloc(&us_.blk_bin, (size_t)dv_.pool_capacity * sizeof(int2)));
+    OSN_TRY(cudaMalloc(&us_.touched, (size_t)dv_.pool_capacity * sizeof(int32_t)));
+    OSN_TRY(cudaMalloc(&us_.ctl, sizeof(UpdateControl)));
+    OSN_TRY(cudaMalloc(&mesh_ctl_, 2 * sizeof(int32_t)));
+    OSN_TRY(cudaMallocHost(&host_small_, 8 * sizeof(int64_t)));
+
+    // The table must hold kEmptyKey, not zero: zero is a valid packed key.
+    // The scratch slots past it hold kScratchKey and are never rewritten.
+    OSN_TRY(launch_reset_table(dv_.table, size, kEmptyKey, stream_));
+    OSN_TRY(launch_reset_table(dv_.table + size, kScratchSlots, kScratchKey, stream_));
+    OSN_TRY(cudaMemsetAsync(dv_.block_count, 0, sizeof(int32_t), stream_));
+    OSN_TRY(cudaMemsetAsync(dv_.drop_count, 0, sizeof(unsigned long long), stream_));
+    OSN_TRY(cudaMemsetAsync(dv_.status, 0, sizeof(uint32_t), stream_));
+    OSN_TRY(cudaMemsetAsync(dv_.tsdf, 0, n_vox * sizeof(float), stream_));
+    OSN_TRY(cudaMemsetAsync(dv_.weight, 0, n_vox * sizeof(float), stream_));
+    OSN_TRY(cudaMemsetAsync(dv_.r, 0, n_vox * sizeof(float), stream_));
+    OSN_TRY(cudaMemsetAsync(dv_.g, 0, n_vox * sizeof(float), stream_));
+    OSN_TRY(cudaMemsetAsync(dv_.b, 0, n_vox * sizeof(float), stream_));
+    OSN_TRY(cudaMemsetAsync(us_.blk_cnt, 0, (size_t)dv_.pool_capacity * sizeof(int32_t), stream_));
+    OSN_TRY(cudaMemsetAsync(us_.ctl, 0, sizeof(UpdateControl), stream_));
+    OSN_TRY(cudaStreamSynchronize(stream_));
+
+    // Persistent apply grid: two 512-thread CTAs per SM (its launch bounds).
+    apply_ctas_per_sm_ = 2;
+    return true;
+}
+
+Volume::~Volume() {
+    if (stream_) cudaStreamSynchronize(stream_);
+    cudaFree(dv_.table);
+    cudaFree(dv_.block_count);
+    cudaFree(dv_.drop_count);
+    cudaFree(dv_.status);
+    cudaFree(dv_.block_coord);
+    cudaFree(dv_.tsdf);
+    cudaFree(dv_.weight);
+    cudaFree(dv_.r);
+    cudaFree(dv_.g);
+    cudaFree(dv_.b);
+    cudaFree(us_.blk_cnt);
+    cudaFree(us_.blk_bin);
+    cudaFree(us_.touched);
+    cudaFree(us_.ctl);
+    cudaFree(us_.records);
+    cudaFree(mesh_posnor_);
+    cudaFree(mesh_rgb_);
+    cudaFree(mesh_ctl_);
+    if (host_small_) cudaFreeHost(host_small_);
+    for (auto& p : pending_) {
+        cudaEventDestroy(p.start);
+        cudaEventDestroy(p.end);
+    }
+    for (auto e : event_pool_) cudaEventDestroy(e);
+    if (stream_) cudaStreamDestroy(stream_);
+}
+
+// ---- timing ------------------------------------------------------------
+
+void Volume::mark_start(int) {
+    if (!timing_) return;
+    cudaEvent_t e;
+    if (!event_pool_.empty()) {
+        e = event_pool_.back();
+        event_pool_.pop_back();
+    } else {
+        cudaEventCreate(&e);
+    }
+    cudaEventRecord(e, stream_);
+    open_start_ = e;
+}
+
+void Volume::mark_end(int id) {
+    if (!timing_ || !open_start_) return;
+    cudaEvent_t e;
+    if (!event_pool_.empty()) {
+        e = event_pool_.back();
+        event_pool_.pop_back();
+    } else {
+        cudaEventCreate(&e);
+    }
+    cudaEventRecord(e, stream_);
+    pending_.push_back(Pending{id, open_start_, e});
+    open_start_ = nullptr;
+}
+
+int Volume::kernel_times(double* ms, int64_t* launches, int n_ids) {
+    cudaStreamSynchronize(stream_);
+    for (auto& p : pending_) {
+        float t = 0.0f;
+        if (cudaEventElapsedTime(&t, p.start, p.end) == cudaSuccess) {
+            acc_ms_[p.id] += t;
+            acc_launches_[p.id] += 1;
+        }
+        event_pool_.push_back(p.start);
+        event_pool_.push_back(p.end);
+    }
+    pending_.clear();
+    const int n = std::min(n_ids, (int)kNumKernelIds);
+    for (int k = 0; k < n; ++k) {
+        if (ms) ms[k] = acc_ms_[k];
+        if (launches) launches[k] = acc_launches_[k];
+    }
+    return n;
+}
+
+// ---- stages ------------------------------------------------------------
+
+cudaError_t Volume::allocate(const BatchArgs& a, int mode, unsigned long long* hist, int n_bins) {
+    mark_start(kKAllocate);
+    const cudaError_t e = launch_allocate(dv_, a, mode, hist, n_bins, stream_);
+    mark_end(kKAllocate);
+    return e;
+}
+
+bool Volume::ensure_records(int64_t n) {
+    if (n <= us_.record_cap) return true;
+    // Grows only; waits for in-flight work that may still read the old bins.
+    cudaStreamSynchronize(stream_);
+    cudaFree(us_.records);
+    us_.records = nullptr;
+    us_.record_cap = 0;
+    if (cudaMalloc(&us_.records, (size_t)n * sizeof(Record)) != cudaSuccess) return false;
+    us_.record_cap = n;
+    return true;
+}
+
+cudaError_t Volume::update(const BatchArgs& a) {
+    // Each point contributes at most one record per band step.
+    const int64_t need = (int64_t)a.n * (2 * dv_.steps + 1);
+    if (!ensure_records(need)) return cudaErrorMemoryAllocation;
+    cudaError_t e = cudaMemsetAsync(us_.ctl, 0, sizeof(UpdateControl), stream_);
+    if (e != cudaSuccess) return e;
+    mark_start(kKUpdateCount);
+    e = launch_update_count(dv_, a, us_, stream_);
+    mark_end(kKUpdateCount);
+    if (e != cudaSuccess) return e;
+    mark_start(kKUpdateScan);
+    e = launch_update_scan(dv_, us_, stream_);
+    mark_end(kKUpdateScan);
+    if (e != cudaSuccess) return e;
+    mark_start(kKUpdateScatter);
+    e = launch_update_scatter(dv_, a, us_, stream_);
+    mark_end(kKUpdateScatter);
+    if (e != cudaSuccess) return e;
+    mark_start(kKUpdateApply);
+    e = launch_update_apply(dv_, us_, sm_count_ * apply_ctas_per_sm_, stream_);
+    mark_end(kKUpdateApply);
+    return e;
+}
+
+bool Volume::ensure_mesh(int32_t cap, bool rgb) {
+    if (cap > mesh_cap_ || (rgb && !mesh_rgb_)) {
+        cudaStreamSynchronize(stream_);
+        cudaFree(mesh_posnor_);
+        cudaFree(mesh_rgb_);
+        mesh_posnor_ = nullptr;
+        mesh_rgb_ = nullptr;
+        mesh_cap_ = 0;
+        const int32_t c = std::max(cap, mesh_cap_);
+        if (cudaMalloc(&mesh_posnor_, (size_t)c * 6 * sizeof(float)) != cudaSuccess) return false;
+        if (rgb && cudaMalloc(&mesh_rgb_, (size_t)c * 3) != cudaSuccess) return false;
+        mesh_cap_ = c;
+    }
+    return true;
+}
+
+int32_t Volume::extract(float* posnor, uint8_t* rgb, int32_t cap, float min_w, float iso,
+                        bool host_out) {
+    const int32_t n_blocks = block_count();  // waits for the stream
+    if (n_blocks <= 0) return 0;
+    float* d_pos = posnor;
+    uint8_t* d_rgb = rgb;
+    if (host_out) {
+        if (!ensure_mesh(cap, rgb != nullptr)) return -1;
+        d_pos = mesh_posnor_;
+        d_rgb = rgb ? mesh_rgb_ : nullptr;
+    }
+    if (cudaMemsetAsync(mesh_ctl_, 0, 2 * sizeof(int32_t), stream_) != cudaSuccess) return -1;
+    mark_start(kKExtract);
+    const cudaError_t e =
+        launch_extract(dv_, std::min(n_blocks, dv_.pool_capacity), min_w, iso, d_pos, d_rgb, cap,
+                       mesh_ctl_, stream_);
+    mark_end(kKExtract);
+    if (e != cudaSuccess) return -1;
+    int32_t* hs = reinterpret_cast<int32_t*>(host_small_);
+    if (cudaMemcpyAsync(hs, mesh_ctl_, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(stream_) != cudaSuccess)
+        return -1;
+    const int32_t n = hs[0], ovf = hs[1];
+    if (ovf) return -1;
+    if (host_out && n > 0) {
+        if (cudaMemcpyAsync(posnor, mesh_posnor_, (size_t)n * 6 * sizeof(float),
+                            cudaMemcpyDeviceToHost, stream_) != cudaSuccess)
+            return -1;
+        if (rgb && cudaMemcpyAsync(rgb, mesh_rgb_, (size_t)n * 3, cudaMemcpyDeviceToHost,
+                                   stream_) != cudaSuccess)
+            return -1;
+        if (cudaStreamSynchronize(stream_) != cudaSuccess) return -1;
+    }
+    return n;
+}
+
+cudaError_t Volume::reset() {
+    const int32_t n_blocks = std::min(block_count(), dv_.pool_capacity);
+    mark_start(kKReset);
+    cudaError_t e = launch_reset_table(dv_.table, dv_.hash_mask + 1, kEmptyKey, stream_);
+    if (e == cudaSuccess) e = launch_reset_voxels(dv_, n_blocks, stream_);
+    mark_end(kKReset);
+    if (e == cudaSuccess) e = cudaMemsetAsync(dv_.block_count, 0, sizeof(int32_t), stream_);
+    if (e == cudaSuccess) e = cudaMemsetAsync(dv_.drop_count, 0, sizeof(unsigned long long), stream_);
+    if (e == cudaSuccess) e = cudaMemsetAsync(dv_.status, 0, sizeof(uint32_t), stream_);
+    if (e == cudaSuccess)
+        e = cudaMemsetAsync(us_.blk_cnt, 0, (size_t)dv_.pool_capacity * sizeof(int32_t), stream_);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+    return e;
+}
+
+int32_t Volume::block_count() {
+    int32_t* hs = reinterpret_cast<int32_t*>(host_small_);
+    cudaMemcpyAsync(hs, dv_.block_count, sizeof(int32_t), cudaMemcpyDeviceToHost, stream_);
+    cudaStreamSynchronize(stream_);
+    return hs[0];
+}
+
+uint64_t Volume::drop_count() {
+    uint64_t* hs = reinterpret_cast<uint64_t*>(host_small_);
+    cudaMemcpyAsync(hs, dv_.drop_count, sizeof(uint64_t), cudaMemcpyDeviceToHost, stream_);
+    cudaStreamSynchronize(stream_);
+    return hs[0];
+}
+
+uint32_t Volume::status() {
+    uint32_t* hs = reinterpret_cast<uint32_t*>(host_small_);
+    cudaMemcpyAsync(hs, dv_.status, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_);
+    cudaStreamSynchronize(stream_);
+    return hs[0];
+}
+
+bool Volume::last_update_stats(int64_t out[4]) {
+    UpdateControl c{};
+    if (cudaMemcpyAsync(host_small_, us_.ctl, sizeof(UpdateControl), cudaMemcpyDeviceToHost,
+                        stream_) != cudaSuccess ||
+        cudaStreamSynchronize(stream_) != cudaSuccess)
+        return false;
+    std::memcpy(&c, host_small_, sizeof(UpdateControl));
+    out[0] = c.n_touched;
+    out[1] = c.n_records;
+    out[2] = c.n_accepted;
+    out[3] = c.n_crossing;
+    return true;
+}
+
+}  // namespace osn_b200

@@ -1,0 +1,242 @@
+"""Python mirror of the reference's CUDA volume interface, over the C ABI.
+
+``CudaVolume`` wraps one ``OsnTsdfCudaVolume`` of libosn_tsdf_b200.so. Its
+methods keep the reference's names and argument meanings
+(cpp/include/osn_tsdf/c_api.h:247-293, cpp/include/osn_tsdf/volume_cuda.hpp:24-86):
+positions are device-resident float32 ``(n, 3)`` world points (a CUDA torch
+tensor or a raw device address), ``cam`` is the camera origin, ``radius_m``
+the far cutoff (<= 0 disables). Bad arguments raise ``ValueError`` where the
+C ABI returns 1; a failed launch raises ``RuntimeError`` (return code 3).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Sequence
+
+import numpy as np
+
+from . import _lib
+
+KERNEL_NAMES = ["allocate", "update_count", "update_scan", "update_scatter", "update_apply",
+                "extract", "reset"]
+
+
+def _addr(x) -> int:
+    """Device address of a CUDA tensor (or an int address)."""
+    if isinstance(x, int):
+        return x
+    if hasattr(x, "data_ptr"):
+        if not x.is_cuda:
+            raise ValueError("positions must be a CUDA tensor (device pointer)")
+        return int(x.data_ptr())
+    raise TypeError(f"expected a CUDA tensor or a device address, got {type(x)!r}")
+
+
+def _count(x, n):
+    if n is not None:
+        return int(n)
+    if hasattr(x, "shape"):
+        if x.dim() != 2 or x.shape[1] != 3:
+            raise ValueError("positions must have shape (n, 3)")
+        if not x.is_contiguous():
+            raise ValueError("positions must be contiguous")
+        import torch
+        if x.dtype != torch.float32:
+            raise ValueError("positions must be float32")
+        return int(x.shape[0])
+    raise ValueError("n is required with a raw device address")
+
+
+class _DeviceArray:
+    """Zero-copy view of device memory for torch.as_tensor."""
+
+    def __init__(self, ptr: int, shape, typestr: str):
+        self.__cuda_array_interface__ = {
+            "shape": tuple(shape), "typestr": typestr, "data": (int(ptr), False), "version": 3,
+            "strides": None,
+        }
+
+
+def device_tensor(ptr: int, shape, dtype: str):
+    """torch view of `shape` elements at device address `ptr` (dtype: numpy typestr)."""
+    import torch
+    return torch.as_tensor(_DeviceArray(ptr, shape, dtype), device="cuda")
+
+
+class CudaVolume:
+    """One hash-blocked TSDF volume on the GPU (drop-in for the reference's CudaVolume)."""
+
+    def __init__(self, voxel_size_m: float, pool_capacity_blocks: int, trunc_m: float = -1.0,
+                 weight_cap: float = 32.0, hash_slots: int = 0):
+        self.lib = _lib.load()
+        self.h = self.lib.osn_tsdf_cuda_create_ex(voxel_size_m, pool_capacity_blocks, trunc_m,
+                                                  weight_cap, hash_slots, 0)
+        if not self.h:
+            raise ValueError("osn_tsdf_cuda_create rejected the parameters or the device "
+                             "allocation failed")
+        self._keep = []
+
+    # -- lifetime -----------------------------------------------------------
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.osn_tsdf_cuda_destroy(self.h)
+            self.h = None
+            self._keep = []
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc: int, what: str):
+        if rc == 1:
+            raise ValueError(f"{what}: invalid arguments")
+        if rc != 0:
+            raise RuntimeError(f"{what}: CUDA launch failed (code {rc})")
+
+    def _batch(self, fn, positions, cam, radius_m, n, what):
+        count = _count(positions, n)
+        self._keep.append(positions)
+        rc = fn(self.h, _addr(positions), count, float(cam[0]), float(cam[1]), float(cam[2]),
+                float(radius_m))
+        self._check(rc, what)
+
+    # -- the reference's stages --------------------------------------------
+    def allocate_blocks(self, positions, cam: Sequence[float], radius_m: float = 0.0, n=None):
+        self._batch(self.lib.osn_tsdf_cuda_allocate_blocks, positions, cam, radius_m, n,
+                    "allocate_blocks")
+
+    def update_voxels(self, positions, cam: Sequence[float], radius_m: float = 0.0, n=None):
+        self._batch(self.lib.osn_tsdf_cuda_update_voxels, positions, cam, radius_m, n,
+                    "update_voxels")
+
+    def integrate(self, positions, cam: Sequence[float], radius_m: float = 0.0, n=None):
+        self._batch(self.lib.osn_tsdf_cuda_integrate, positions, cam, radius_m, n, "integrate")
+
+    def allocate_counting_cas(self, positions, cam, radius_m=0.0, n=None):
+        self._batch(self.lib.osn_tsdf_cuda_allocate_counting_cas, positions, cam, radius_m, n,
+                    "allocate_counting_cas")
+
+    def allocate_no_cas(self, positions, cam, radius_m=0.0, n=None):
+        self._batch(self.lib.osn_tsdf_cuda_allocate_no_cas, positions, cam, radius_m, n,
+                    "allocate_no_cas")
+
+    def allocate_slot_index(self, positions, cam, radius_m=0.0, n=None):
+        self._batch(self.lib.osn_tsdf_cuda_allocate_slot_index, positions, cam, radius_m, n,
+                    "allocate_slot_index")
+
+    def allocate_probe_histogram(self, positions, cam, radius_m=0.0, n_bins=32, n=None):
+        count = _count(positions, n)
+        hist = np.zeros(n_bins, dtype=np.uint64)
+        self._keep.append(positions)
+        rc = self.lib.osn_tsdf_cuda_allocate_probe_histogram(
+            self.h, _addr(positions), count, float(cam[0]), float(cam[1]), float(cam[2]),
+            float(radius_m), hist.ctypes.data, n_bins)
+        self._check(rc, "allocate_probe_histogram")
+        return hist
+
+    def extract_mesh(self, vert_cap: int = 4 << 20, min_weight: float = 0.5, iso: float = 0.0,
+                     rgb: bool = False):
+        """Triangle soup as host arrays: posnor (n, 6) float32 [, rgb (n, 3) uint8]; None on overflow."""
+        posnor = np.empty((vert_cap, 6), dtype=np.float32)
+        col = np.empty((vert_cap, 3), dtype=np.uint8) if rgb else None
+        n = self.lib.osn_tsdf_cuda_extract_mesh(self.h, posnor.ctypes.data,
+                                                col.ctypes.data if rgb else None, vert_cap,
+                                                min_weight, iso)
+        self._keep = []
+        if n < 0:
+            return (None, None) if rgb else None
+        return (posnor[:n], col[:n]) if rgb else posnor[:n]
+
+    def extract_mesh_device(self, posnor, rgb=None, vert_cap=None, min_weight=0.5, iso=0.0) -> int:
+        cap = int(vert_cap if vert_cap is not None else posnor.shape[0])
+        return self.lib.osn_tsdf_cuda_extract_mesh_device(
+            self.h, _addr(posnor), _addr(rgb) if rgb is not None else None, cap, min_weight, iso)
+
+    def reset(self):
+        self._check(self.lib.osn_tsdf_cuda_reset(self.h), "reset")
+        self._keep = []
+
+    def block_count(self) -> int:
+        return self.lib.osn_tsdf_cuda_block_count(self.h)
+
+    def drop_count(self) -> int:
+        return self.lib.osn_tsdf_cuda_drop_count(self.h)
+
+    def synchronize(self):
+        self.lib.osn_tsdf_cuda_synchronize(self.h)
+        self._keep = []
+
+    def valid(self) -> bool:
+        return bool(self.lib.osn_tsdf_cuda_valid(self.h))
+
+    # -- extensions ---------------------------------------------------------
+    def status(self) -> int:
+        return self.lib.osn_tsdf_cuda_status(self.h)
+
+    def stream_handle(self) -> int:
+        return int(self.lib.osn_tsdf_cuda_stream(self.h) or 0)
+
+    def device_view(self) -> _lib.OsnTsdfDeviceView:
+        view = _lib.OsnTsdfDeviceView()
+        rc = self.lib.osn_tsdf_cuda_device_view(self.h, C.byref(view))
+        if rc:
+            raise RuntimeError("device_view failed")
+        return view
+
+    def last_update_stats(self) -> dict:
+        out = np.zeros(4, dtype=np.int64)
+        self._check(self.lib.osn_tsdf_cuda_last_update_stats(self.h, out.ctypes.data),
+                    "last_update_stats")
+        return {"touched_blocks": int(out[0]), "records": int(out[1]),
+                "accepted_blocks": int(out[2]), "crossing_blocks": int(out[3])}
+
+    def set_timing(self, on: bool = True):
+        self.lib.osn_tsdf_cuda_set_timing(self.h, 1 if on else 0)
+
+    def kernel_times(self) -> dict:
+        ms = np.zeros(len(KERNEL_NAMES), dtype=np.float64)
+        launches = np.zeros(len(KERNEL_NAMES), dtype=np.int64)
+        self.lib.osn_tsdf_cuda_kernel_times(self.h, ms.ctypes.data, launches.ctypes.data,
+                                            len(KERNEL_NAMES))
+        return {k: (float(ms[i]), int(launches[i])) for i, k in enumerate(KERNEL_NAMES)}
+
+    # -- read-back helpers (tests, tools) ------------------------------------
+    def coords(self) -> np.ndarray:
+        """Block coordinates in pool order, (block_count, 3) int32."""
+        n = min(self.block_count(), self.device_view().pool_capacity)
+        if n <= 0:
+            return np.zeros((0, 3), dtype=np.int32)
+        view = self.device_view()
+        return device_tensor(view.block_coord, (n, 3), "<i4").cpu().numpy()
+
+    def coord_set(self) -> set:
+        return set(map(tuple, self.coords().tolist()))
+
+    def voxels(self):
+        """(coords, tsdf, weight, r, g, b): the five arrays as (block_count, 512) float32."""
+        n = min(self.block_count(), self.device_view().pool_capacity)
+        view = self.device_view()
+        out = [self.coords()]
+        for ptr in (view.tsdf, view.weight, view.r, view.g, view.b):
+            if n <= 0:
+                out.append(np.zeros((0, 512), dtype=np.float32))
+            else:
+                out.append(device_tensor(ptr, (n, 512), "<f4").cpu().numpy())
+        return tuple(out)
+
+    def table(self):
+        """(keys int64, block_idx int32) of the live table."""
+        self.synchronize()
+        view = self.device_view()
+        size = view.hash_mask + 1
+        raw = device_tensor(view.table, (size, 4), "<i4").cpu().numpy()
+        keys = raw[:, :2].copy().view(np.int64).reshape(-1)
+        return keys, raw[:, 2].copy()
