@@ -1,0 +1,423 @@
+"""Benchmark: 640x480 frames/s of the TSDF integrate path on B200.
+
+Workload (one step): reset the volume, then integrate every frame of the
+seeded 100-frame room trajectory (640x480, fx=fy=320, 2 cm voxels, trunc
+8 cm, 2^20 table slots, pool 2^19 blocks, weight cap 64), i.e. allocate +
+update per frame through the C ABI. frames/s = frames integrated / time.
+
+  value  device-resident points (uploaded once), CUDA events on the volume's
+         stream around exactly K steps, max over ranks;
+  e2e    the same steps from pinned HOST buffers: every frame's points are
+         copied host->device inside the timed region (double-buffered on a
+         copy stream) and the block and drop counters are read back per step;
+  roofline  per-kernel CUDA-event times of one instrumented step; the
+         dominant kernel's algorithmic bytes per launch / its mean duration
+         against the measured HBM copy bandwidth;
+  cpu_baseline  the reference's own CPU arm (oracle/_ref, all host threads)
+         on a bounded sample of the same frames.
+
+--impl reference times only the reference CPU arm (rank 0) on the same
+workload, each step a bounded sample of frames.
+
+Multi-GPU: one process per GPU under torchrun, each integrating its own
+replica of the trajectory (independent volumes, no collective on the data
+path): weak scaling.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import time
+from concurrent.futures import ProcessPoolExecutor
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+VOXEL, TRUNC, CAP = 0.02, 0.08, 64.0
+HASH_SLOTS, POOL = 1 << 20, 1 << 19
+N_FRAMES, SEED = 100, 0
+METRIC = "frames/s (640x480 integrate)"
+PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "update_apply_room640.md")
+
+
+def _frame_points(args):
+    seed, k = args
+    from what_irregularity_costs_b200 import scenes
+    scene = scenes.RoomScene.make(seed)
+    f = scenes.room_frame(scene, k)
+    return scenes.frame_points(f), f.cam
+
+
+def make_trajectory(n_frames=N_FRAMES, seed=SEED, workers=None):
+    """Points of every frame (generated in spawned workers, before any CUDA use)."""
+    workers = workers or min(16, os.cpu_count() or 1)
+    ctx = mp.get_context("spawn")
+    with ProcessPoolExecutor(max_workers=workers, mp_context=ctx) as ex:
+        out = list(ex.map(_frame_points, [(seed, k) for k in range(n_frames)]))
+    pts = [p for p, _ in out]
+    cams = [c for _, c in out]
+    return pts, cams
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """DRAM bytes per launch of the apply kernel from the committed ncu summary."""
+    try:
+        with open(PROFILE_TRAFFIC) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_launch:"):
+                    return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.rows = []
+        if self.proc is None:
+            return
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        for line in out.splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def summary(self):
+        rows = getattr(self, "rows", [])
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=None)
+        return rank, local, world, dist
+    return 0, 0, 1, None
+
+
+def barrier(dist, torch):
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+
+
+def max_over_ranks(x, dist, torch):
+    if dist is None:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+
+
+def cpu_reference_rate(pts, cams, budget_s=15.0, threads=None):
+    """Reference CPU arm (osn_tsdf_create/_integrate, all host threads) on the
+    first frames of the trajectory, from an empty volume, bounded by budget_s."""
+    import ctypes as C
+    import oracle
+    lib = oracle.ref_lib()
+    threads = threads or (os.cpu_count() or 1)
+    v = lib.osn_tsdf_create(VOXEL, POOL, TRUNC, CAP)
+    lib.osn_tsdf_set_thread_count(v, threads)
+    done, t_total = 0, 0.0
+    try:
+        for p, cam in zip(pts, cams):
+            ptr = p.ctypes.data_as(C.POINTER(C.c_float))
+            t0 = time.perf_counter()
+            rc = lib.osn_tsdf_integrate(v, ptr, None, None, p.shape[0], 0, *cam, 0.0)
+            t_total += time.perf_counter() - t0
+            if rc != 0:
+                raise RuntimeError(f"reference integrate returned {rc}")
+            done += 1
+            if t_total > budget_s:
+                break
+    finally:
+        lib.osn_tsdf_destroy(v)
+    return done / t_total, done, threads, t_total
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import oracle
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "reference CPU arm not built (oracle/_ref/libosn_tsdf_ref.so missing)"}))
+        return 0
+    frames = min(args.ref_frames, N_FRAMES)
+    all_pts, all_cams = make_trajectory(N_FRAMES)
+    pts, cams = all_pts[:frames], all_cams[:frames]
+    threads = os.cpu_count() or 1
+    rates = []
+    for i in range(args.warmup + args.steps):
+        rate, done, _, t = cpu_reference_rate(pts, cams, budget_s=1e9, threads=threads)
+        if i >= args.warmup:
+            rates.append((done, t))
+    total_frames = sum(d for d, _ in rates)
+    total_t = sum(t for _, t in rates)
+    value = total_frames / total_t
+    sample = f"first {frames} frames of the room trajectory per step, from an empty volume"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "frames/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * total_t / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": config_dict(points=int(sum(p.shape[0] for p in all_pts))),
+        "cpu_baseline": {"value": value, "unit": "frames/s", "cores": threads,
+                         "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": "frames/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def config_dict(points):
+    return {
+        "workload": "room trajectory, 100 frames 640x480 fx=fy=320, 2 cm voxels, trunc 8 cm, "
+                    "2^20 table slots, pool 2^19 blocks, weight cap 64; step = reset + "
+                    "allocate/update of every frame",
+        "frames_per_step": N_FRAMES, "resolution": [640, 480], "voxel_m": VOXEL,
+        "trunc_m": TRUNC, "hash_slots": HASH_SLOTS, "pool_blocks": POOL, "weight_cap": CAP,
+        "points_per_step": points, "seed": SEED,
+        "l2": "inputs larger than L2: %.0f MB of points per step" % (points * 12 / 1e6),
+    }
+
+
+def run_ours(args):
+    pts, cams = make_trajectory(N_FRAMES)   # before any CUDA use (spawned workers)
+    import torch
+    from what_irregularity_costs_b200 import CudaVolume, KERNEL_NAMES
+
+    rank, local, world, dist = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    n_points = int(sum(p.shape[0] for p in pts))
+    offsets = np.concatenate([[0], np.cumsum([p.shape[0] for p in pts])])
+    all_pts = np.concatenate(pts).astype(np.float32)
+    d_all = torch.from_numpy(all_pts).cuda()
+    host_pinned = torch.from_numpy(all_pts).pin_memory()
+
+    vol = CudaVolume(VOXEL, POOL, TRUNC, CAP, HASH_SLOTS)
+    vstream = torch.cuda.ExternalStream(vol.stream_handle())
+
+    def step_device():
+        vol.reset()
+        for k in range(N_FRAMES):
+            a, b = int(offsets[k]), int(offsets[k + 1])
+            vol.integrate(d_all[a:b], cams[k])
+
+    # -- value: device-resident inputs ---------------------------------------
+    for _ in range(args.warmup):
+        step_device()
+    barrier(dist, torch)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        ev0.record(vstream)
+        for _ in range(args.steps):
+            step_device()
+        ev1.record(vstream)
+        barrier(dist, torch)
+    ms = ev0.elapsed_time(ev1)
+    ms = max_over_ranks(ms, dist, torch)
+    blocks = vol.block_count()
+    drops = vol.drop_count()
+    status = vol.status()
+    frames_total = N_FRAMES * args.steps * world
+    value = frames_total / (ms / 1e3)
+
+    # -- e2e: pinned host buffers, copies inside the timed region ------------
+    max_n = int(np.max(np.diff(offsets)))
+    stage = [torch.empty((max_n, 3), dtype=torch.float32, device="cuda") for _ in range(2)]
+    cstream = torch.cuda.Stream()
+    copied = [torch.cuda.Event() for _ in range(2)]
+    free = [torch.cuda.Event() for _ in range(2)]
+    result = torch.zeros(2, dtype=torch.int64).pin_memory()
+
+    def step_e2e():
+        vol.reset()
+        for k in range(N_FRAMES):
+            a, b = int(offsets[k]), int(offsets[k + 1])
+            s = k & 1
+            with torch.cuda.stream(cstream):
+                cstream.wait_event(free[s])
+                stage[s][: b - a].copy_(host_pinned[a:b], non_blocking=True)
+                copied[s].record(cstream)
+            vstream.wait_event(copied[s])
+            vol.integrate(stage[s][: b - a], cams[k])
+            free[s].record(vstream)
+        result[0] = vol.block_count()
+        result[1] = vol.drop_count()
+
+    for s in range(2):
+        free[s].record(vstream)
+    for _ in range(args.warmup):
+        step_e2e()
+    barrier(dist, torch)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(vstream)
+    for _ in range(args.steps):
+        step_e2e()
+    e1.record(vstream)
+    barrier(dist, torch)
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), dist, torch)
+    e2e_value = frames_total / (e2e_ms / 1e3)
+
+    # -- one instrumented step: per-kernel times and stage statistics ---------
+    vol.set_timing(True)
+    vol.kernel_times()  # flush
+    base = vol.kernel_times()
+    vol.reset()
+    touched, accepted, records = [], [], []
+    for k in range(N_FRAMES):
+        a, b = int(offsets[k]), int(offsets[k + 1])
+        vol.integrate(d_all[a:b], cams[k])
+        st = vol.last_update_stats()
+        touched.append(st["touched_blocks"])
+        accepted.append(st["accepted_blocks"])
+        records.append(st["records"])
+    times = vol.kernel_times()
+    vol.set_timing(False)
+    per_kernel = {k: (times[k][0] - base[k][0], times[k][1] - base[k][1]) for k in KERNEL_NAMES}
+    launches_per_step = sum(n for _, n in per_kernel.values())
+    dominant = max((k for k in KERNEL_NAMES if per_kernel[k][1] > 0), key=lambda k: per_kernel[k][0])
+
+    peak, peak_kind = measured_peak()
+    t_alloc = per_kernel["allocate"][0] / 1e3
+    t_update = sum(per_kernel[k][0] for k in ("update_count", "update_scan", "update_scatter",
+                                               "update_apply")) / 1e3
+    tile_bytes = sum(accepted) * 512 * 2 * 8          # tsdf + weight, read + write
+    rgb_bytes = sum(accepted) * 512 * 2 * 12
+    update_alg_bytes = 12 * n_points + tile_bytes
+    # Algorithmic bytes per launch of each kernel (roofline).
+    alg = {
+        "update_apply": tile_bytes / N_FRAMES,
+        "update_count": 12 * n_points / N_FRAMES,
+        "update_scatter": 12 * n_points / N_FRAMES + 16 * sum(records) / N_FRAMES,
+        "allocate": 12 * n_points / N_FRAMES,
+    }
+    dom_ms, dom_n = per_kernel[dominant]
+    dom_alg = alg.get(dominant, 0.0)
+    achieved = dom_alg / (dom_ms / 1e3 / dom_n) / 1e9 if dom_n else 0.0
+    roofline = {
+        "bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
+        "frac": achieved / peak, "peak_source": peak_kind,
+        "traffic": profile_traffic() if dominant == "update_apply" else None,
+        "alg_bytes_per_launch": dom_alg, "mean_launch_us": 1e3 * dom_ms / dom_n if dom_n else None,
+    }
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        try:
+            import oracle
+            if oracle.ref_available():
+                rate, done, threads, t = cpu_reference_rate(pts, cams, budget_s=args.cpu_budget)
+                cpu = {"value": rate, "unit": "frames/s", "cores": threads, "kind": "reference",
+                       "sample": f"first {done} frames of the trajectory from an empty volume "
+                                 f"({t:.1f} s)"}
+        except Exception as e:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": "frames/s", "cores": None, "kind": "reference",
+                   "sample": f"failed: {e}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic: seeded room trajectory (3 spheres, 2 boxes), depth noise "
+                    "0.0015 z^2, 5% invalid pixels, FP64 backprojection",
+            "config": config_dict(n_points),
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "frames/s",
+                    "h2d_bytes_per_step": int(all_pts.nbytes), "d2h_bytes_per_step": 16},
+            "gpu_launches": int(launches_per_step * args.steps),
+            "clocks": clocks.summary(),
+            "alloc_mrays_per_s": n_points / t_alloc / 1e6 if t_alloc else None,
+            "update_gbps": update_alg_bytes / t_update / 1e9 if t_update else None,
+            "update_rgb_bytes_per_step": rgb_bytes,
+            "kernel_ms_per_step": {k: round(v[0], 4) for k, v in per_kernel.items()},
+            "kernel_launches_per_step": {k: v[1] for k, v in per_kernel.items()},
+            "blocks": blocks, "drops": int(drops), "status": status,
+            "touched_blocks_per_frame": float(np.mean(touched)),
+            "accepted_blocks_per_frame": float(np.mean(accepted)),
+        }
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--ref-frames", type=int, default=20,
+                    help="frames per step of the reference arm")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

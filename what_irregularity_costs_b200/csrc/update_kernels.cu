@@ -25,6 +25,13 @@
 //           (closed form for unit weights), an exact radix select of the
 //           accepted ids for the few voxels that cross the cap inside this
 //           batch, then one coalesced read and write of the block's tiles.
+//
+// The accepted sdf values of a voxel are summed in 64-bit fixed point
+// (2^-40 resolution, exact for |value| >= 2^-17) and added to the stored sum
+// with one rounding, so the result does not depend on the order in which
+// the CTA's threads meet the records: repeated runs are bit-identical, and a
+// voxel with one contribution per batch gets exactly the reference's
+// fl(tsdf + sdf_n).
 #include "volume.h"
 
 namespace osn_b200 {
@@ -35,6 +42,8 @@ constexpr int kScanThreads = 1024;
 constexpr int kApplyThreads = 512;  // one thread per voxel of a block
 constexpr int kDigitBits = 4;
 constexpr int kDigits = 1 << kDigitBits;
+constexpr double kFixScale = 1099511627776.0;        // 2^40
+constexpr double kFixInv = 1.0 / 1099511627776.0;    // 2^-40
 
 // Per-thread cache of the last looked-up block, and the warp-cooperative
 // lookup for samples whose block differs from it: one leader per distinct key.
@@ -212,7 +221,7 @@ __global__ void __launch_bounds__(kApplyThreads, 2)
 update_apply_kernel(DevVolume v, UpdateScratch u) {
     __shared__ int s_cnt[kBlockVoxels];
     __shared__ int s_keep[kBlockVoxels];
-    __shared__ float s_acc[kBlockVoxels];
+    __shared__ unsigned long long s_acc[kBlockVoxels];
     __shared__ uint32_t s_thr[kBlockVoxels];
     __shared__ uint32_t s_hist[kBlockVoxels * kDigits];
     __shared__ int s_item;
@@ -233,7 +242,7 @@ update_apply_kernel(DevVolume v, UpdateScratch u) {
         const float w0 = v.weight[vox];
         const float t0 = v.tsdf[vox];
         s_cnt[t] = 0;
-        s_acc[t] = t0;
+        s_acc[t] = 0ull;
         __syncthreads();
 
         // Pass A: records per voxel.
@@ -289,12 +298,14 @@ update_apply_kernel(DevVolume v, UpdateScratch u) {
             const int kl = s_keep[lv];
             if (kl <= 0) continue;
             if (kl < s_cnt[lv] && rec.id > s_thr[lv]) continue;
-            atomicAdd(&s_acc[lv], __fmul_rn(rec.sdf_n, rec.w_in));
+            const double x = (double)__fmul_rn(rec.sdf_n, rec.w_in);
+            atomicAdd(&s_acc[lv], (unsigned long long)__double2ll_rn(x * kFixScale));
         }
         __syncthreads();
 
         if (keep > 0) {
-            v.tsdf[vox] = s_acc[t];
+            const double sum = (double)(long long)s_acc[t] * kFixInv;
+            v.tsdf[vox] = __double2float_rn((double)t0 + sum);
             v.weight[vox] = __fadd_rn(w0, (float)keep);
             const float dc = __fmul_rn(128.0f, (float)keep);
             v.r[vox] = __fadd_rn(v.r[vox], dc);
