@@ -154,6 +154,28 @@ int32_t osn_tsdf_cuda_allocate_probe_histogram(OsnTsdfCudaVolume* v, const float
  * out[3] blocks that needed ordered cap selection. */
 int32_t osn_tsdf_cuda_last_update_stats(const OsnTsdfCudaVolume* v, int64_t* out4);
 
+/* Largest batch of one update_voxels_noalloc call, counted in records:
+ * n_points * (2 * steps + 1) with steps = max(1, ceil(trunc / voxel)). */
+#define OSN_TSDF_NOALLOC_MAX_RECORDS (1 << 22)
+
+/* update_voxels that allocates no device memory. No counterpart in the
+ * reference. update_voxels may grow its scratch with cudaMalloc (after
+ * waiting for the stream) when a batch is larger than any before it; callers
+ * that cannot allow that -- code recording the integrate into a CUDA graph
+ * (no allocation during stream capture), serving loops that budget device
+ * memory up front, latency-critical threads that cannot absorb the implied
+ * synchronisation -- call this instead. Same results as update_voxels.
+ * Its scratch is one fixed 64 MiB array inside the library, held on every
+ * GPU where the library's code is loaded until the process exits, and shared
+ * by all calls: calls whose work overlaps on the GPU race and must be
+ * serialised. The first call on a device resolves the array's address and
+ * must come before any stream capture. Returns 0 (queued), 1 on bad
+ * arguments, 3 on a set-up or launch failure, 4 when n_points * (2*steps+1)
+ * exceeds OSN_TSDF_NOALLOC_MAX_RECORDS (nothing is queued; split the batch). */
+int32_t osn_tsdf_cuda_update_voxels_noalloc(OsnTsdfCudaVolume* v, const float* d_positions,
+                                            int32_t n_points, float cam_x, float cam_y,
+                                            float cam_z, float radius_m);
+
 /* Kernel timing. When enabled, every kernel launch of the volume is
  * bracketed by CUDA events on the volume's stream; kernel_times reads (and
  * waits for) the accumulated per-kernel milliseconds and launch counts.

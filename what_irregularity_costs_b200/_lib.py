@@ -67,6 +67,7 @@ _SIG = {
     "osn_tsdf_cuda_last_update_stats": (_I, [_P, _P]),
     "osn_tsdf_cuda_set_timing": (_I, [_P, _I]),
     "osn_tsdf_cuda_kernel_times": (_I, [_P, _P, _P, _I]),
+    "osn_tsdf_cuda_update_voxels_noalloc": (_I, [_P, _P, _I, _F, _F, _F, _F]),
 }
 
 _lib = None

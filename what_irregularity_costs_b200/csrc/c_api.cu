@@ -50,6 +50,10 @@ int32_t allocate_mode(OsnTsdfCudaVolume* v, const float* d_positions, int32_t n,
 
 }  // namespace
 
+osn_b200::Volume* osn_tsdf_b200_volume_of(OsnTsdfCudaVolume* v) {
+    return usable(v) ? &v->vol : nullptr;
+}
+
 extern "C" {
 
 OsnTsdfCudaVolume* osn_tsdf_cuda_create(float voxel_size_m, int32_t pool_capacity_blocks,

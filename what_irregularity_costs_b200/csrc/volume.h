@@ -70,6 +70,9 @@ public:
     // Stages (all asynchronous on stream()). Return a cudaError_t of the launch.
     cudaError_t allocate(const BatchArgs& a, int mode, unsigned long long* hist, int n_bins);
     cudaError_t update(const BatchArgs& a);
+    // update() with its control counters and records in caller-provided
+    // device memory instead of the volume's own (grown) buffer.
+    cudaError_t update_static_scratch(const BatchArgs& a, void* scratch);
     int32_t extract(float* posnor, uint8_t* rgb, int32_t cap, float min_w, float iso, bool host_out);
     cudaError_t reset();
 
@@ -146,3 +149,7 @@ enum AllocMode : int {
 };
 
 }  // namespace osn_b200
+
+// The Volume behind a C-ABI handle, or nullptr when the handle is NULL or invalid.
+struct OsnTsdfCudaVolume;
+osn_b200::Volume* osn_tsdf_b200_volume_of(OsnTsdfCudaVolume* v);

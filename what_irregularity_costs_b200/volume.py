@@ -117,6 +117,23 @@ class CudaVolume:
         self._batch(self.lib.osn_tsdf_cuda_update_voxels, positions, cam, radius_m, n,
                     "update_voxels")
 
+    def update_voxels_noalloc(self, positions, cam: Sequence[float], radius_m: float = 0.0,
+                              n=None) -> int:
+        """update_voxels with no device allocation (the library's fixed scratch array).
+
+        For callers that must not allocate during the call (graph capture,
+        fixed memory budgets). Returns the C ABI code: 0 queued, 4 when the
+        batch exceeds OSN_TSDF_NOALLOC_MAX_RECORDS records (nothing queued).
+        """
+        count = _count(positions, n)
+        self._keep.append(positions)
+        rc = self.lib.osn_tsdf_cuda_update_voxels_noalloc(
+            self.h, _addr(positions), count, float(cam[0]), float(cam[1]), float(cam[2]),
+            float(radius_m))
+        if rc not in (0, 4):
+            self._check(rc, "update_voxels_noalloc")
+        return rc
+
     def integrate(self, positions, cam: Sequence[float], radius_m: float = 0.0, n=None):
         self._batch(self.lib.osn_tsdf_cuda_integrate, positions, cam, radius_m, n, "integrate")
 
