@@ -322,7 +322,7 @@ def run_ours(args):
     vol.kernel_times()  # flush
     base = vol.kernel_times()
     vol.reset()
-    touched, accepted, records = [], [], []
+    touched, accepted, records, crossing = [], [], [], []
     for k in range(N_FRAMES):
         a, b = int(offsets[k]), int(offsets[k + 1])
         vol.integrate(d_all[a:b], cams[k])
@@ -330,6 +330,7 @@ def run_ours(args):
         touched.append(st["touched_blocks"])
         accepted.append(st["accepted_blocks"])
         records.append(st["records"])
+        crossing.append(st["crossing_blocks"])
     times = vol.kernel_times()
     vol.set_timing(False)
     per_kernel = {k: (times[k][0] - base[k][0], times[k][1] - base[k][1]) for k in KERNEL_NAMES}
@@ -338,7 +339,7 @@ def run_ours(args):
 
     peak, peak_kind = measured_peak()
     t_alloc = per_kernel["allocate"][0] / 1e3
-    t_update = sum(per_kernel[k][0] for k in ("update_count", "update_scan", "update_scatter",
+    t_update = sum(per_kernel[k][0] for k in ("update_stage", "update_crossing", "update_place",
                                                "update_apply")) / 1e3
     tile_bytes = sum(accepted) * 512 * 2 * 8          # tsdf + weight, read + write
     rgb_bytes = sum(accepted) * 512 * 2 * 12
@@ -346,8 +347,7 @@ def run_ours(args):
     # Algorithmic bytes per launch of each kernel (roofline).
     alg = {
         "update_apply": tile_bytes / N_FRAMES,
-        "update_count": 12 * n_points / N_FRAMES,
-        "update_scatter": 12 * n_points / N_FRAMES + 16 * sum(records) / N_FRAMES,
+        "update_stage": 12 * n_points / N_FRAMES,
         "allocate": 12 * n_points / N_FRAMES,
     }
     dom_ms, dom_n = per_kernel[dominant]
@@ -395,6 +395,8 @@ def run_ours(args):
             "blocks": blocks, "drops": int(drops), "status": status,
             "touched_blocks_per_frame": float(np.mean(touched)),
             "accepted_blocks_per_frame": float(np.mean(accepted)),
+            "crossing_blocks_per_frame": float(np.mean(crossing)),
+            "records_per_frame": float(np.mean(records)),
         }
         print(json.dumps(line))
     if dist is not None:

@@ -122,7 +122,9 @@ OsnTsdfCudaVolume* osn_tsdf_cuda_create_ex(float voxel_size_m, int32_t pool_capa
                                            int32_t storage);
 
 /* allocate_blocks then update_voxels on the same points, as the reference's
- * CPU integrate (cpp/src/volume.cpp:301-304). Return codes as allocate_blocks. */
+ * CPU integrate (cpp/src/volume.cpp:301-304), in one pass: blocks are
+ * allocated and contributions counted by the same walk. Results are those of
+ * the two separate calls. Return codes as allocate_blocks. */
 int32_t osn_tsdf_cuda_integrate(OsnTsdfCudaVolume* v, const float* d_positions, int32_t n_points,
                                 float cam_x, float cam_y, float cam_z, float radius_m);
 
@@ -165,7 +167,7 @@ int32_t osn_tsdf_cuda_last_update_stats(const OsnTsdfCudaVolume* v, int64_t* out
  * (no allocation during stream capture), serving loops that budget device
  * memory up front, latency-critical threads that cannot absorb the implied
  * synchronisation -- call this instead. Same results as update_voxels.
- * Its scratch is one fixed 64 MiB array inside the library, held on every
+ * Its scratch is one fixed 88 MiB array inside the library, held on every
  * GPU where the library's code is loaded until the process exits, and shared
  * by all calls: calls whose work overlaps on the GPU race and must be
  * serialised. The first call on a device resolves the array's address and
@@ -179,7 +181,8 @@ int32_t osn_tsdf_cuda_update_voxels_noalloc(OsnTsdfCudaVolume* v, const float* d
 /* Kernel timing. When enabled, every kernel launch of the volume is
  * bracketed by CUDA events on the volume's stream; kernel_times reads (and
  * waits for) the accumulated per-kernel milliseconds and launch counts.
- * Kernel ids: 0 allocate, 1 update-count, 2 update-scan, 3 update-scatter,
+ * Kernel ids: 0 allocate, 1 update-stage (allocate+stage in integrate),
+ * 2 update-crossing (ordered cap selection), 3 update-place,
  * 4 update-apply, 5 extract, 6 reset. Returns the number of ids written. */
 int32_t osn_tsdf_cuda_set_timing(OsnTsdfCudaVolume* v, int32_t enabled);
 int32_t osn_tsdf_cuda_kernel_times(OsnTsdfCudaVolume* v, double* ms, int64_t* launches,

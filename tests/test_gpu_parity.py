@@ -145,6 +145,23 @@ def test_pool_exhaustion(cuda):
     assert gpu.status() == 0
 
 
+def test_pool_exactly_full(cuda):
+    """The pool holds exactly the frame's blocks: the last insertions race with
+    lookups of the same keys while the pool fills. Every sample must still be
+    counted and binned the same way (no drops, voxels equal)."""
+    scene = scenes.RoomScene.make(2)
+    f = scenes.room_frame(scene, 0)
+    pts = scenes.frame_points(f)
+    probe = oracle.OracleVolume(0.02, 1 << 19, 0.08, 64.0)
+    probe.allocate(pts, f.cam)
+    blocks = probe.block_count()
+    gpu, ref = _pair(cuda, [(pts, f.cam)], 0.02, blocks, 0.08, 64.0)
+    assert gpu.block_count() == blocks and gpu.drop_count() == 0 == ref.drop_count()
+    assert gpu.status() == 0
+    assert_same_blocks(gpu, ref)
+    assert_same_voxels(gpu, ref)
+
+
 def test_radius_cutoff_and_offset_camera(cuda):
     """Far cutoff and a camera far from the origin (negative block coordinates)."""
     f = scenes.sphere_frame()

@@ -122,10 +122,11 @@ int32_t osn_tsdf_cuda_update_voxels(OsnTsdfCudaVolume* v, const float* d_positio
 
 int32_t osn_tsdf_cuda_integrate(OsnTsdfCudaVolume* v, const float* d_positions, int32_t n_points,
                                 float cam_x, float cam_y, float cam_z, float radius_m) {
-    const int32_t rc =
-        osn_tsdf_cuda_allocate_blocks(v, d_positions, n_points, cam_x, cam_y, cam_z, radius_m);
-    if (rc) return rc;
-    return osn_tsdf_cuda_update_voxels(v, d_positions, n_points, cam_x, cam_y, cam_z, radius_m);
+    if (!usable(v) || !d_positions || n_points <= 0 || !batch_fits(v, n_points)) return 1;
+    return v->vol.integrate(batch(d_positions, n_points, cam_x, cam_y, cam_z, radius_m)) ==
+                   cudaSuccess
+               ? 0
+               : 3;
 }
 
 int32_t osn_tsdf_cuda_extract_mesh(OsnTsdfCudaVolume* v, float* buffer_posnor, uint8_t* buffer_rgb,

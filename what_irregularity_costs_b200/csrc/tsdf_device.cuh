@@ -177,6 +177,113 @@ __device__ __forceinline__ int32_t find_block(const DevVolume& v, int32_t bx, in
     return -1;
 }
 
+// ---- insertion (volume.cpp:94-145, volume_cuda.cu:59-107) -------------------
+
+// Allocation modes: the production insert and the reference's measurement
+// variants (cpp/include/osn_tsdf/c_api.h:275-289), plus a probe histogram.
+enum AllocMode : int {
+    kAllocInsert = 0,       // production
+    kAllocCountingCas = 1,  // measurement: count CAS attempts into drop_count
+    kAllocNoCas = 2,        // measurement: probe, never insert
+    kAllocProbeHist = 3,    // measurement: insert and histogram probe depths
+    kAllocSlotIndex = 4,    // measurement: block index = slot
+    kLookupOnly = 5,        // no insertion: find_block (update after allocation)
+};
+
+struct InsertResult {
+    int32_t idx;      // >= 0 allocated or found, -1 dropped / absent
+    uint32_t probes;  // slots visited
+};
+
+// Wait, with an iteration bound, until a claimed slot's index is published
+// or its claim is rolled back (pool full). A timeout sets a status bit.
+__device__ __forceinline__ int32_t wait_published(const DevVolume& v, HashEntry* e, long long want) {
+    for (int it = 0; it < kSpinLimit; ++it) {
+        const int idx = ld_acquire_s32(&e->block_idx);
+        if (idx >= 0) return idx;
+        if (ld_relaxed_s64(&e->key) != want) return -1;
+        __nanosleep(64);
+    }
+    atomicOr(v.status, kStatusSpinTimeout);
+    return -1;
+}
+
+// Find or insert one block: CAS the key into the first empty slot of its
+// linear probe sequence, take a pool index from the counter, write the
+// coordinate, fence, publish the index (volume_cuda.cu:82-95). When the pool
+// is already full no slot is claimed; a claim that overflows the pool is
+// rolled back to kReleasedKey.
+template <int MODE>
+__device__ __forceinline__ InsertResult find_or_insert(const DevVolume& v, int32_t bx, int32_t by,
+                                                       int32_t bz, long long want) {
+    InsertResult res{-1, 0};
+    const uint32_t mask = (MODE == kAllocSlotIndex) ? (uint32_t)v.pool_capacity - 1u : v.hash_mask;
+    const uint32_t size = mask + 1;
+    const uint32_t start = hash_slot(bx, by, bz, mask);
+    for (uint32_t p = 0; p < size; ++p) {
+        const uint32_t slot = (start + p) & mask;
+        HashEntry* e = &v.table[slot];
+        ++res.probes;
+        const long long key = ld_relaxed_s64(&e->key);
+        if (key == want) {
+            if (MODE == kAllocNoCas) { res.idx = 0; return res; }
+            if (MODE == kAllocSlotIndex) { res.idx = (int32_t)slot; return res; }
+            res.idx = wait_published(v, e, want);
+            return res;
+        }
+        if (key == kEmptyKey) {
+            if (MODE == kAllocNoCas) return res;
+            if (MODE != kAllocSlotIndex && ld_acquire_s32(v.block_count) >= v.pool_capacity) {
+                // The pool is full, so no claim can succeed any more -- but the
+                // claim that filled it may have been this very key, made after
+                // we read the slot. Claimers fence between their CAS and their
+                // counter increment, so having seen the full count we see
+                // their key if it is there.
+                const long long again = ld_relaxed_s64(&e->key);
+                if (again == want) {
+                    res.idx = wait_published(v, e, want);
+                    return res;
+                }
+                if (again == kEmptyKey) return res;  // absent, and cannot be inserted
+                continue;                            // another key took the slot: probe on
+            }
+            if (MODE == kAllocCountingCas) atomicAdd(v.drop_count, 1ULL);
+            const long long prev = (long long)atomicCAS((unsigned long long*)&e->key,
+                                                        (unsigned long long)kEmptyKey,
+                                                        (unsigned long long)want);
+            if (prev == kEmptyKey) {
+                if (MODE == kAllocSlotIndex) {
+                    v.block_coord[slot] = BlockCoord{bx, by, bz};
+                    atomicAdd(v.block_count, 1);
+                    __threadfence();
+                    atomicExch(&e->block_idx, (int)slot);
+                    res.idx = (int32_t)slot;
+                    return res;
+                }
+                __threadfence();  // the claim is visible before the count that reflects it
+                const int32_t idx = atomicAdd(v.block_count, 1);
+                if (idx >= v.pool_capacity) {
+                    atomicSub(v.block_count, 1);
+                    atomicExch((unsigned long long*)&e->key, (unsigned long long)kReleasedKey);
+                    return res;
+                }
+                v.block_coord[idx] = BlockCoord{bx, by, bz};
+                __threadfence();  // coordinate visible before the index
+                atomicExch(&e->block_idx, idx);
+                res.idx = idx;
+                return res;
+            }
+            if (prev == want) {
+                if (MODE == kAllocSlotIndex) { res.idx = (int32_t)slot; return res; }
+                res.idx = wait_published(v, e, want);
+                return res;
+            }
+        }
+        // Another key, a rolled-back slot or a scratch sentinel: probe on.
+    }
+    return res;  // table full
+}
+
 __device__ __forceinline__ unsigned lanemask_lt() {
     unsigned m;
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));

@@ -12,15 +12,16 @@
 // with its scratch in one fixed array compiled into the library.
 //
 // The array is a file-scope __device__ variable of kNoAllocScratchBytes
-// (64 MiB + 256 bytes): the control counters, then room for
-// kNoAllocMaxRecords 16-byte records, i.e. batches with
-// n_points * (2 * steps + 1) <= 4,194,304 (a 640x480 frame at 9 band steps
-// per point fits). Every GPU on which the library's code is loaded holds the
-// array until the process exits. Every call shares it and it keeps the last
-// call's contents; the counters that must start at zero are cleared at the
-// start of each call. Two calls whose work overlaps on the GPU (two volumes
-// on different streams, say) race on the array and corrupt each other's
-// results: serialise them.
+// (88 MiB + 256 bytes): the control counters, room for kNoAllocMaxRecords
+// 16-byte records and for kNoAllocMaxSegments 24-byte segment entries, i.e.
+// batches with n_points * (2 * steps + 1) <= 4,194,304 (a 640x480 frame at 9
+// band steps per point fits). Every GPU on which the library's code is loaded
+// holds the array until the process exits. Every call shares it and it keeps
+// the last call's contents; the counters that must start at zero are cleared
+// at the start of each call. Two calls whose work overlaps on the GPU (two
+// volumes on different streams, say) race on the array and corrupt each
+// other's results: serialise them.
+#include <algorithm>
 #include <cstdio>
 #include <mutex>
 
@@ -33,8 +34,11 @@ namespace {
 
 constexpr size_t kNoAllocHeaderBytes = 256;  // UpdateControl, padded
 constexpr int64_t kNoAllocMaxRecords = OSN_TSDF_NOALLOC_MAX_RECORDS;
-constexpr size_t kNoAllocScratchBytes =
-    kNoAllocHeaderBytes + (size_t)kNoAllocMaxRecords * sizeof(Record);
+constexpr int64_t kNoAllocMaxSegments = (int64_t)1 << 20;
+constexpr size_t kNoAllocRecordBytes = (size_t)kNoAllocMaxRecords * sizeof(Record);
+constexpr size_t kNoAllocSegBytes = (size_t)kNoAllocMaxSegments * sizeof(int4);
+constexpr size_t kNoAllocScratchBytes = kNoAllocHeaderBytes + kNoAllocRecordBytes + kNoAllocSegBytes +
+                                        (size_t)kNoAllocMaxSegments * sizeof(int2);
 static_assert(sizeof(UpdateControl) <= kNoAllocHeaderBytes, "control block must fit the header");
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
@@ -68,30 +72,17 @@ void* scratch_address(int device) {
 }  // namespace
 
 cudaError_t Volume::update_static_scratch(const BatchArgs& a, void* scratch) {
+    unsigned char* base = static_cast<unsigned char*>(scratch);
     UpdateScratch u = us_;
-    u.ctl = reinterpret_cast<UpdateControl*>(scratch);
-    u.records = reinterpret_cast<Record*>(static_cast<unsigned char*>(scratch) + kNoAllocHeaderBytes);
+    u.ctl = reinterpret_cast<UpdateControl*>(base);
+    u.records = reinterpret_cast<Record*>(base + kNoAllocHeaderBytes);
     u.record_cap = kNoAllocMaxRecords;
-    // Only the control counters must start at zero; the records of the
-    // previous call are overwritten before they are read.
-    cudaError_t e = cudaMemsetAsync(u.ctl, 0, sizeof(UpdateControl), stream_);
-    if (e != cudaSuccess) return e;
-    mark_start(kKUpdateCount);
-    e = launch_update_count(dv_, a, u, stream_);
-    mark_end(kKUpdateCount);
-    if (e != cudaSuccess) return e;
-    mark_start(kKUpdateScan);
-    e = launch_update_scan(dv_, u, stream_);
-    mark_end(kKUpdateScan);
-    if (e != cudaSuccess) return e;
-    mark_start(kKUpdateScatter);
-    e = launch_update_scatter(dv_, a, u, stream_);
-    mark_end(kKUpdateScatter);
-    if (e != cudaSuccess) return e;
-    mark_start(kKUpdateApply);
-    e = launch_update_apply(dv_, u, sm_count_ * apply_ctas_per_sm_, stream_);
-    mark_end(kKUpdateApply);
-    return e;
+    u.segs = reinterpret_cast<int4*>(base + kNoAllocHeaderBytes + kNoAllocRecordBytes);
+    u.seg_list = reinterpret_cast<int2*>(base + kNoAllocHeaderBytes + kNoAllocRecordBytes + kNoAllocSegBytes);
+    u.seg_cap = kNoAllocMaxSegments;
+    // Only the control counters must start at zero (run_update clears them);
+    // the records of the previous call are overwritten before they are read.
+    return run_update(a, u, false);
 }
 
 }  // namespace osn_b200
@@ -103,7 +94,8 @@ extern "C" int32_t osn_tsdf_cuda_update_voxels_noalloc(OsnTsdfCudaVolume* v,
     osn_b200::Volume* vol = osn_tsdf_b200_volume_of(v);
     if (!vol || !d_positions || n_points <= 0) return 1;
     const int64_t records = (int64_t)n_points * (2 * (int64_t)vol->dev().steps + 1);
-    if (records > osn_b200::kNoAllocMaxRecords) {
+    const int64_t segments = std::min<int64_t>(records, (int64_t)((n_points + 255) / 256) * 512);
+    if (records > osn_b200::kNoAllocMaxRecords || segments > osn_b200::kNoAllocMaxSegments) {
         std::fprintf(stderr,
                      "[osn_tsdf_b200] update_voxels_noalloc: batch of %d points needs %lld records, "
                      "above the fixed maximum of %lld (n_points * (2*steps+1)); split the batch\n",

@@ -52,6 +52,7 @@ bool Volume::alloc_device(uint32_t hash_slots) {
     int dev = 0;
     OSN_TRY(cudaGetDevice(&dev));
     OSN_TRY(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, dev));
+    OSN_TRY(prepare_update_kernels());
     OSN_TRY(cudaStreamCreate(&stream_));
     OSN_TRY(cudaMalloc(&dv_.table, ((size_t)size + kScratchSlots) * sizeof(HashEntry)));
     OSN_TRY(cudaMalloc(&dv_.block_count, sizeof(int32_t)));
@@ -64,8 +65,11 @@ bool Volume::alloc_device(uint32_t hash_slots) {
     OSN_TRY(cudaMalloc(&dv_.g, n_vox * sizeof(float)));
     OSN_TRY(cudaMalloc(&dv_.b, n_vox * sizeof(float)));
     OSN_TRY(cudaMalloc(&us_.blk_cnt, (size_t)dv_.pool_capacity * sizeof(int32_t)));
-    OSN_TRY(cudaMalloc(&us_.blk_bin, (size_t)dv_.pool_capacity * sizeof(int2)));
+    OSN_TRY(cudaMalloc(&us_.blk_nseg, (size_t)dv_.pool_capacity * sizeof(int32_t)));
+    OSN_TRY(cudaMalloc(&us_.blk_cur, (size_t)dv_.pool_capacity * sizeof(int32_t)));
+    OSN_TRY(cudaMalloc(&us_.blk_info, (size_t)dv_.pool_capacity * sizeof(int4)));
     OSN_TRY(cudaMalloc(&us_.touched, (size_t)dv_.pool_capacity * sizeof(int32_t)));
+    OSN_TRY(cudaMalloc(&us_.cross_list, (size_t)dv_.pool_capacity * sizeof(int32_t)));
     OSN_TRY(cudaMalloc(&us_.ctl, sizeof(UpdateControl)));
     OSN_TRY(cudaMalloc(&mesh_ctl_, 2 * sizeof(int32_t)));
     OSN_TRY(cudaMallocHost(&host_small_, 8 * sizeof(int64_t)));
@@ -83,11 +87,16 @@ bool Volume::alloc_device(uint32_t hash_slots) {
     OSN_TRY(cudaMemsetAsync(dv_.g, 0, n_vox * sizeof(float), stream_));
     OSN_TRY(cudaMemsetAsync(dv_.b, 0, n_vox * sizeof(float), stream_));
     OSN_TRY(cudaMemsetAsync(us_.blk_cnt, 0, (size_t)dv_.pool_capacity * sizeof(int32_t), stream_));
+    OSN_TRY(cudaMemsetAsync(us_.blk_nseg, 0, (size_t)dv_.pool_capacity * sizeof(int32_t), stream_));
+    OSN_TRY(cudaMemsetAsync(us_.blk_cur, 0, (size_t)dv_.pool_capacity * sizeof(int32_t), stream_));
     OSN_TRY(cudaMemsetAsync(us_.ctl, 0, sizeof(UpdateControl), stream_));
     OSN_TRY(cudaStreamSynchronize(stream_));
 
-    // Persistent apply grid: two 512-thread CTAs per SM (its launch bounds).
-    apply_ctas_per_sm_ = 2;
+    // Persistent grids, as many CTAs per SM as shared memory allows.
+    int per_sm = 0;
+    OSN_TRY(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+    apply_ctas_per_sm_ = std::max(1, per_sm / (int)(apply_smem_bytes() + 1024));
+    cross_ctas_per_sm_ = 2;
     return true;
 }
 
@@ -104,8 +113,13 @@ Volume::~Volume() {
     cudaFree(dv_.g);
     cudaFree(dv_.b);
     cudaFree(us_.blk_cnt);
-    cudaFree(us_.blk_bin);
+    cudaFree(us_.blk_nseg);
+    cudaFree(us_.blk_cur);
+    cudaFree(us_.blk_info);
+    cudaFree(us_.segs);
+    cudaFree(us_.seg_list);
     cudaFree(us_.touched);
+    cudaFree(us_.cross_list);
     cudaFree(us_.ctl);
     cudaFree(us_.records);
     cudaFree(mesh_posnor_);
@@ -178,40 +192,70 @@ cudaError_t Volume::allocate(const BatchArgs& a, int mode, unsigned long long* h
     return e;
 }
 
-bool Volume::ensure_records(int64_t n) {
-    if (n <= us_.record_cap) return true;
-    // Grows only; waits for in-flight work that may still read the old bins.
+bool Volume::ensure_records(int64_t n_records, int64_t n_segs) {
+    if (n_records <= us_.record_cap && n_segs <= us_.seg_cap) return true;
+    // Grows only; waits for in-flight work that may still read the old buffers.
     cudaStreamSynchronize(stream_);
-    cudaFree(us_.records);
-    us_.records = nullptr;
-    us_.record_cap = 0;
-    if (cudaMalloc(&us_.records, (size_t)n * sizeof(Record)) != cudaSuccess) return false;
-    us_.record_cap = n;
+    if (n_records > us_.record_cap) {
+        cudaFree(us_.records);
+        us_.records = nullptr;
+        us_.record_cap = 0;
+        if (cudaMalloc(&us_.records, (size_t)n_records * sizeof(Record)) != cudaSuccess) return false;
+        us_.record_cap = n_records;
+    }
+    if (n_segs > us_.seg_cap) {
+        cudaFree(us_.segs);
+        cudaFree(us_.seg_list);
+        us_.segs = nullptr;
+        us_.seg_list = nullptr;
+        us_.seg_cap = 0;
+        if (cudaMalloc(&us_.segs, (size_t)n_segs * sizeof(int4)) != cudaSuccess) return false;
+        if (cudaMalloc(&us_.seg_list, (size_t)n_segs * sizeof(int2)) != cudaSuccess) return false;
+        us_.seg_cap = n_segs;
+    }
     return true;
 }
 
-cudaError_t Volume::update(const BatchArgs& a) {
-    // Each point contributes at most one record per band step.
-    const int64_t need = (int64_t)a.n * (2 * dv_.steps + 1);
-    if (!ensure_records(need)) return cudaErrorMemoryAllocation;
-    cudaError_t e = cudaMemsetAsync(us_.ctl, 0, sizeof(UpdateControl), stream_);
+cudaError_t Volume::run_update(const BatchArgs& a, const UpdateScratch& u, bool insert) {
+    cudaError_t e = cudaMemsetAsync(u.ctl, 0, sizeof(UpdateControl), stream_);
     if (e != cudaSuccess) return e;
-    mark_start(kKUpdateCount);
-    e = launch_update_count(dv_, a, us_, stream_);
-    mark_end(kKUpdateCount);
+    mark_start(kKUpdateStage);
+    e = launch_update_stage(dv_, a, u, insert, stream_);
+    mark_end(kKUpdateStage);
     if (e != cudaSuccess) return e;
-    mark_start(kKUpdateScan);
-    e = launch_update_scan(dv_, us_, stream_);
-    mark_end(kKUpdateScan);
-    if (e != cudaSuccess) return e;
-    mark_start(kKUpdateScatter);
-    e = launch_update_scatter(dv_, a, us_, stream_);
-    mark_end(kKUpdateScatter);
+    mark_start(kKUpdatePlace);
+    e = launch_update_place(u, sm_count_ * 4, stream_);
+    mark_end(kKUpdatePlace);
     if (e != cudaSuccess) return e;
     mark_start(kKUpdateApply);
-    e = launch_update_apply(dv_, us_, sm_count_ * apply_ctas_per_sm_, stream_);
+    e = launch_update_apply(dv_, u, sm_count_ * apply_ctas_per_sm_, stream_);
     mark_end(kKUpdateApply);
+    if (e != cudaSuccess) return e;
+    mark_start(kKUpdateCrossing);
+    e = launch_update_crossing(dv_, u, sm_count_ * cross_ctas_per_sm_, stream_);
+    mark_end(kKUpdateCrossing);
     return e;
+}
+
+// Scratch a batch of n points can need: one record per band sample, and one
+// segment per (walk CTA of 256 points, block), at most 512 per CTA.
+static void batch_scratch(int32_t n, int32_t steps, int64_t* records, int64_t* segs) {
+    *records = (int64_t)n * (2 * steps + 1);
+    *segs = std::min<int64_t>(*records, (int64_t)((n + 255) / 256) * 512);
+}
+
+cudaError_t Volume::update(const BatchArgs& a) {
+    int64_t rec = 0, seg = 0;
+    batch_scratch(a.n, dv_.steps, &rec, &seg);
+    if (!ensure_records(rec, seg)) return cudaErrorMemoryAllocation;
+    return run_update(a, us_, false);
+}
+
+cudaError_t Volume::integrate(const BatchArgs& a) {
+    int64_t rec = 0, seg = 0;
+    batch_scratch(a.n, dv_.steps, &rec, &seg);
+    if (!ensure_records(rec, seg)) return cudaErrorMemoryAllocation;
+    return run_update(a, us_, true);
 }
 
 bool Volume::ensure_mesh(int32_t cap, bool rgb) {
@@ -278,6 +322,10 @@ cudaError_t Volume::reset() {
     if (e == cudaSuccess) e = cudaMemsetAsync(dv_.status, 0, sizeof(uint32_t), stream_);
     if (e == cudaSuccess)
         e = cudaMemsetAsync(us_.blk_cnt, 0, (size_t)dv_.pool_capacity * sizeof(int32_t), stream_);
+    if (e == cudaSuccess)
+        e = cudaMemsetAsync(us_.blk_nseg, 0, (size_t)dv_.pool_capacity * sizeof(int32_t), stream_);
+    if (e == cudaSuccess)
+        e = cudaMemsetAsync(us_.blk_cur, 0, (size_t)dv_.pool_capacity * sizeof(int32_t), stream_);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
     return e;
 }

@@ -12,11 +12,11 @@ namespace osn_b200 {
 
 // Kernel ids for the timing table (documented in include/osn_tsdf_b200.h).
 enum KernelId : int {
-    kKAllocate = 0,
-    kKUpdateCount = 1,
-    kKUpdateScan = 2,
-    kKUpdateScatter = 3,
-    kKUpdateApply = 4,
+    kKAllocate = 0,        // allocate-only walk
+    kKUpdateStage = 1,     // count-and-stage walk (fused with allocation in integrate)
+    kKUpdateCrossing = 2,  // ordered cap selection for deferred blocks
+    kKUpdatePlace = 3,     // file segment descriptors under their blocks
+    kKUpdateApply = 4,     // tile read-modify-write
     kKExtract = 5,
     kKReset = 6,
     kNumKernelIds = 7,
@@ -25,11 +25,15 @@ enum KernelId : int {
 // Counters an update pass keeps on the device (one small struct, cleared by
 // one memset at the start of every update).
 struct UpdateControl {
-    int32_t n_touched;        // blocks that received at least one record
-    int32_t n_records;        // records binned
-    int32_t work;             // apply-kernel work cursor
-    int32_t n_accepted;       // blocks that accepted at least one contribution
-    int32_t n_crossing;       // blocks that needed ordered cap selection
+    int32_t n_touched;   // blocks that received at least one record
+    int32_t n_records;   // records staged
+    int32_t work;        // apply-kernel work cursor
+    int32_t n_accepted;  // blocks that accepted at least one contribution
+    int32_t n_crossing;  // blocks that needed ordered cap selection
+    int32_t work2;       // crossing-kernel work cursor
+    int32_t cta_done;    // stage-kernel CTAs finished (the last one scans)
+    int32_t n_segs;      // segment descriptors published
+    int32_t n_deferred;  // blocks handed to the crossing kernel
     int32_t pad[3];
 };
 
@@ -43,12 +47,18 @@ struct __align__(16) Record {
 static_assert(sizeof(Record) == 16, "record must stay one 128-bit vector");
 
 struct UpdateScratch {
-    int32_t* blk_cnt = nullptr;   // [pool] records per block; back to 0 after every update
-    int2* blk_bin = nullptr;      // [pool] (offset, length) of each touched block's bin
-    int32_t* touched = nullptr;   // [pool] touched block indices
+    int32_t* blk_cnt = nullptr;     // [pool] records per block; back to 0 after every update
+    int32_t* blk_nseg = nullptr;    // [pool] segments per block; back to 0 after every update
+    int32_t* blk_cur = nullptr;     // [pool] segment filing cursor; back to 0 after every update
+    int4* blk_info = nullptr;       // [pool] (first segment slot, segments, records, -)
+    int32_t* touched = nullptr;     // [pool] touched block indices
+    int32_t* cross_list = nullptr;  // [pool] blocks deferred to ordered selection
     UpdateControl* ctl = nullptr;
-    Record* records = nullptr;
+    Record* records = nullptr;      // staged records, grouped per (walk CTA, block)
     int64_t record_cap = 0;
+    int4* segs = nullptr;           // segment descriptors (block, offset, length, -)
+    int2* seg_list = nullptr;       // descriptors filed per block: (offset, length)
+    int64_t seg_cap = 0;
 };
 
 class Volume {
@@ -70,6 +80,8 @@ public:
     // Stages (all asynchronous on stream()). Return a cudaError_t of the launch.
     cudaError_t allocate(const BatchArgs& a, int mode, unsigned long long* hist, int n_bins);
     cudaError_t update(const BatchArgs& a);
+    // allocate + update in one pass over the points (same results).
+    cudaError_t integrate(const BatchArgs& a);
     // update() with its control counters and records in caller-provided
     // device memory instead of the volume's own (grown) buffer.
     cudaError_t update_static_scratch(const BatchArgs& a, void* scratch);
@@ -90,7 +102,8 @@ public:
 
 private:
     bool alloc_device(uint32_t hash_slots);
-    bool ensure_records(int64_t n);
+    cudaError_t run_update(const BatchArgs& a, const UpdateScratch& u, bool insert);
+    bool ensure_records(int64_t n_records, int64_t n_segs);
     bool ensure_mesh(int32_t cap, bool rgb);
 
     bool ok_ = false;
@@ -99,6 +112,7 @@ private:
     UpdateScratch us_{};
     int sm_count_ = 148;
     int apply_ctas_per_sm_ = 2;
+    int cross_ctas_per_sm_ = 2;
 
     // Extraction scratch (device output for the host-copy path, counters).
     float* mesh_posnor_ = nullptr;
@@ -130,23 +144,17 @@ cudaError_t launch_reset_voxels(const DevVolume& v, int32_t n_blocks, cudaStream
 cudaError_t launch_extract(const DevVolume& v, int32_t n_blocks, float min_w, float iso,
                            float* posnor, uint8_t* rgb, int32_t cap, int32_t* ctl, cudaStream_t s);
 
-// The update pipeline: count -> scan -> scatter -> apply.
-cudaError_t launch_update_count(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
-                                cudaStream_t s);
-cudaError_t launch_update_scan(const DevVolume& v, const UpdateScratch& u, cudaStream_t s);
-cudaError_t launch_update_scatter(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
-                                  cudaStream_t s);
+// The update pipeline: stage (+ per-block segment ranges) -> place -> apply -> crossing.
+cudaError_t launch_update_stage(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
+                                bool insert, cudaStream_t s);
+cudaError_t launch_update_place(const UpdateScratch& u, int n_ctas, cudaStream_t s);
 cudaError_t launch_update_apply(const DevVolume& v, const UpdateScratch& u, int n_ctas,
                                 cudaStream_t s);
-
-// Allocation modes.
-enum AllocMode : int {
-    kAllocInsert = 0,       // production
-    kAllocCountingCas = 1,  // measurement: count CAS attempts into drop_count
-    kAllocNoCas = 2,        // measurement: probe, never insert
-    kAllocProbeHist = 3,    // measurement: insert and histogram probe depths
-    kAllocSlotIndex = 4,    // measurement: block index = slot
-};
+cudaError_t launch_update_crossing(const DevVolume& v, const UpdateScratch& u, int n_ctas,
+                                   cudaStream_t s);
+// One-time kernel attributes (dynamic shared memory of apply and crossing).
+cudaError_t prepare_update_kernels();
+size_t apply_smem_bytes();
 
 }  // namespace osn_b200
 
