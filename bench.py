@@ -339,7 +339,7 @@ def run_ours(args):
 
     peak, peak_kind = measured_peak()
     t_alloc = per_kernel["allocate"][0] / 1e3
-    t_update = sum(per_kernel[k][0] for k in ("update_stage", "update_crossing", "update_place",
+    t_update = sum(per_kernel[k][0] for k in ("update_stage", "update_crossing", "update_bin",
                                                "update_apply")) / 1e3
     tile_bytes = sum(accepted) * 512 * 2 * 8          # tsdf + weight, read + write
     rgb_bytes = sum(accepted) * 512 * 2 * 12

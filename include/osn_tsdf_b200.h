@@ -158,7 +158,7 @@ int32_t osn_tsdf_cuda_last_update_stats(const OsnTsdfCudaVolume* v, int64_t* out
 
 /* Largest batch of one update_voxels_noalloc call, counted in records:
  * n_points * (2 * steps + 1) with steps = max(1, ceil(trunc / voxel)). */
-#define OSN_TSDF_NOALLOC_MAX_RECORDS (1 << 22)
+#define OSN_TSDF_NOALLOC_MAX_RECORDS (1 << 21)
 
 /* update_voxels that allocates no device memory. No counterpart in the
  * reference. update_voxels may grow its scratch with cudaMalloc (after
@@ -167,7 +167,7 @@ int32_t osn_tsdf_cuda_last_update_stats(const OsnTsdfCudaVolume* v, int64_t* out
  * (no allocation during stream capture), serving loops that budget device
  * memory up front, latency-critical threads that cannot absorb the implied
  * synchronisation -- call this instead. Same results as update_voxels.
- * Its scratch is one fixed 88 MiB array inside the library, held on every
+ * Its scratch is one fixed 72 MiB array inside the library, held on every
  * GPU where the library's code is loaded until the process exits, and shared
  * by all calls: calls whose work overlaps on the GPU race and must be
  * serialised. The first call on a device resolves the array's address and
@@ -182,7 +182,7 @@ int32_t osn_tsdf_cuda_update_voxels_noalloc(OsnTsdfCudaVolume* v, const float* d
  * bracketed by CUDA events on the volume's stream; kernel_times reads (and
  * waits for) the accumulated per-kernel milliseconds and launch counts.
  * Kernel ids: 0 allocate, 1 update-stage (allocate+stage in integrate),
- * 2 update-crossing (ordered cap selection), 3 update-place,
+ * 2 update-crossing (ordered cap selection), 3 update-bin,
  * 4 update-apply, 5 extract, 6 reset. Returns the number of ids written. */
 int32_t osn_tsdf_cuda_set_timing(OsnTsdfCudaVolume* v, int32_t enabled);
 int32_t osn_tsdf_cuda_kernel_times(OsnTsdfCudaVolume* v, double* ms, int64_t* launches,

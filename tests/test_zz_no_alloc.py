@@ -20,7 +20,7 @@ from what_irregularity_costs_b200 import CudaVolume, scenes
 
 pytestmark = pytest.mark.gpu
 
-MAX_RECORDS = 1 << 22  # OSN_TSDF_NOALLOC_MAX_RECORDS in include/osn_tsdf_b200.h
+MAX_RECORDS = 1 << 21  # OSN_TSDF_NOALLOC_MAX_RECORDS in include/osn_tsdf_b200.h
 
 
 def test_noalloc_update_matches_update_voxels_twice(cuda):
@@ -28,7 +28,8 @@ def test_noalloc_update_matches_update_voxels_twice(cuda):
     A cap of 6 makes many voxels cross the cap inside a frame, so the ordered
     selection runs on the shared scratch as well."""
     scene = scenes.RoomScene.make(1)
-    frames = [scenes.room_frame(scene, k) for k in (0, 1)]
+    K = scenes.ROOM_K.scaled(480, 360)  # fits the fixed scratch in one call
+    frames = [scenes.room_frame(scene, k, K) for k in (0, 1)]
     with CudaVolume(0.02, 1 << 19, 0.08, 6.0) as regular, \
             CudaVolume(0.02, 1 << 19, 0.08, 6.0) as fixed:
         for f in frames:

@@ -1,4 +1,4 @@
-// Update, second half: apply the binned contributions to the block tiles.
+// Update, second half: apply the staged contributions to the block tiles.
 //
 // Reference: cpp/src/volume.cpp:282-295 and cpp/src/volume_cuda.cu:325-335
 // (per sample: cap check, then atomic adds of weight, w*sdf and w*colour).
@@ -12,21 +12,27 @@
 //
 // The count-and-stage walk (walk_kernels.cu) has staged every contribution
 // that can still be accepted, in segments of consecutive records, one
-// segment per (walk CTA, block), and given each touched block its range of
-// segment slots. Here:
+// segment per (walk CTA, block), and has given each touched block the offset
+// and length of its bin. Here:
 //
-//   place     files each segment descriptor under its block (one thread per
-//             segment);
-//   apply     one 128-thread CTA per touched block (persistent, work-queued),
-//             4 voxels per thread, 128-bit tile loads and stores. One pass
-//             over the block's segments counts each voxel's records and sums
-//             their values; a voxel accepts all of them when w0 + n - 1 < cap.
-//             A block in which some voxel would cross the cap inside this
-//             batch is deferred, untouched, to
+//   bin       one warp per segment copies its records into the block's
+//             contiguous bin (L2-resident traffic);
+//   apply     one 128-thread CTA per touched block (persistent, work-queued,
+//             many per SM), 4 voxels per thread; blocks with more than 2048
+//             records go to a 1024-thread CTA instead (one per SM), so the
+//             largest blocks of a frame (~20k records) do not form a tail. The block's five 2 KB tiles
+//             are staged into shared memory by cp.async.bulk while the CTA
+//             makes one pass over the bin: per-voxel record counts and sums,
+//             combined per warp with __match_any_sync before the shared
+//             atomics. A voxel accepts all of its records when w0 + n - 1 <
+//             cap. Voxels that cross the cap inside the batch are resolved in
+//             the CTA: their records are grouped per voxel in shared memory
+//             and a warp counts each record's rank by id among its voxel's
+//             records; the `keep` lowest are accepted. Blocks with more such
+//             records than fit are deferred to
 //   crossing  one 256-thread CTA per deferred block: an exact radix select
 //             (4-bit digits over the record ids) finds the id of each
-//             crossing voxel's last accepted record, then the block is
-//             applied with that threshold.
+//             crossing voxel's last accepted record.
 //
 // Sums are accumulated in 64-bit fixed point (2^-40 resolution, exact for
 // |value| >= 2^-17) and added to the stored sum with one rounding, so results
@@ -39,11 +45,17 @@
 namespace osn_b200 {
 namespace {
 
-constexpr int kCrossThreads = 256;   // two voxels per thread
+constexpr int kApplyThreads = 128;  // 4 voxels per thread
+constexpr int kBigThreads = 1024;   // big blocks: one CTA per SM
+constexpr int kBigRecords = 2048;   // blocks above this go to the big-block apply
+constexpr int kCrossThreads = 256;  // deferred blocks: two voxels per thread
+constexpr int kCrossCap = 1024;     // crossing records resolved inside apply
+constexpr int kBigCrossCap = 16384; // crossing records resolved inside the big-block apply
+constexpr int kCrossList = 4096;    // crossing records the deferred kernel holds in shared memory
 constexpr int kDigitBits = 4;
 constexpr int kDigits = 1 << kDigitBits;
-constexpr double kFixScale = 1099511627776.0;        // 2^40
-constexpr double kFixInv = 1.0 / 1099511627776.0;    // 2^-40
+constexpr double kFixScale = 1099511627776.0;      // 2^40
+constexpr double kFixInv = 1.0 / 1099511627776.0;  // 2^-40
 
 // Contributions a voxel accepts given its weight w0 before the batch and n
 // unit-weight records: the j-th record (0-based, canonical order) is accepted
@@ -56,73 +68,86 @@ __device__ __forceinline__ int accept_count(float w0, float cap, int n) {
     return room >= (double)n ? n : (int)room;
 }
 
-__device__ __forceinline__ unsigned long long to_fix(float sdf_n, float w_in) {
-    return (unsigned long long)__double2ll_rn((double)__fmul_rn(sdf_n, w_in) * kFixScale);
+__device__ __forceinline__ unsigned long long to_fix(float x) {
+    return (unsigned long long)__double2ll_rn((double)x * kFixScale);
 }
 
 __device__ __forceinline__ float add_fix(float t0, unsigned long long acc) {
     return __double2float_rn((double)t0 + (double)(long long)acc * kFixInv);
 }
 
-// Visit every record of a block, warp w taking segments w, w + W, ...
-template <int NTHREADS, class F>
-__device__ __forceinline__ void for_block_records(const UpdateScratch& u, const int4& info, F&& f) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int g = warp; g < info.y; g += NTHREADS / 32) {
-        const int2 sg = u.seg_list[info.x + g];
-        for (int k = lane; k < sg.y; k += 32) f(u.records[sg.x + k]);
-    }
-}
+// ---- bin -----------------------------------------------------------------
 
 __global__ void __launch_bounds__(256)
-update_place_kernel(UpdateScratch u) {
+update_bin_kernel(UpdateScratch u) {
     const int n = (int)min((long long)u.ctl->n_segs, (long long)u.seg_cap);
-    for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < n; d += gridDim.x * blockDim.x) {
-        const int4 sg = u.segs[d];
-        const int4 info = u.blk_info[sg.x];
-        const int k = atomicAdd(&u.blk_cur[sg.x], 1);
-        if (k < info.y) u.seg_list[info.x + k] = make_int2(sg.y, sg.z);
+    const int lane = threadIdx.x & 31;
+    const int warps = gridDim.x * (blockDim.x >> 5);
+    for (int d = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); d < n; d += warps) {
+        const int4 sg = u.segs[d];  // (block, staging offset, length, -)
+        int at = 0;
+        if (lane == 0) at = u.blk_info[sg.x].x + atomicAdd(&u.blk_cur[sg.x], sg.z);
+        at = __shfl_sync(0xffffffffu, at, 0);
+        const int4* src = reinterpret_cast<const int4*>(u.records + sg.y);
+        int4* dst = reinterpret_cast<int4*>(u.bins + at);
+        for (int k = lane; k < sg.z; k += 32) dst[k] = src[k];
     }
 }
 
-// ---- apply: warp-specialised, bulk-copy staged --------------------------
-//
-// Warp 0 is the producer: it takes the next touched block from the work
-// cursor, loads the block's segment descriptors, and issues cp.async.bulk
-// copies of the block's five 2 KB tiles (weight, tsdf, r, g, b) and of every
-// record segment into one of kStages shared-memory stages, completing on the
-// stage's "full" mbarrier. Warps 1-4 are consumers (4 voxels per thread):
-// they wait for a full stage, apply it, and release it on its "empty"
-// mbarrier, so the copies of the next blocks overlap the current one.
-// Blocks with more records or segments than a stage holds are applied from
-// global memory by the same consumers.
-//
-// Voxels that cross the cap inside the batch are resolved in the CTA: their
-// records are grouped per voxel in shared memory and each record's rank by
-// id among its voxel's records is counted by a warp; the `keep` lowest-ranked
-// are accepted. Blocks whose crossing records exceed kCrossCap are deferred
-// to update_crossing_kernel.
-constexpr int kConsumerWarps = 4;
-constexpr int kConsumers = 32 * kConsumerWarps;
-constexpr int kApplyCta = kConsumers + 32;
-constexpr int kStages = 3;
-constexpr int kStageRecords = 1024;
-constexpr int kStageSegs = 256;  // 8 descriptors per producer lane
-constexpr int kCrossCap = 2048;
-constexpr int kModeDone = 0, kModeShared = 1, kModeGlobal = 2;
-constexpr int kConsumerBar = 1;
+// ---- apply ---------------------------------------------------------------
 
-struct __align__(128) ApplyStage {
-    float tile[5][kBlockVoxels];  // weight, tsdf, r, g, b
-    Record rec[kStageRecords];
-    int4 info;                    // (first segment slot, segments, records, block)
-    int mode;
-};
+// One pass over a bin: per-voxel record counts and fixed-point sums in
+// shared memory. Four records per thread are loaded before any is used, and
+// lanes holding the same voxel combine before the shared atomics.
+template <int NT>
+__device__ __forceinline__ void accumulate_bin(const Record* recs, int nrec, int* cnt,
+                                               unsigned long long* sum) {
+    constexpr int kU = 4;
+    const int t = threadIdx.x, lane = t & 31;
+    for (int k0 = 0; k0 < nrec; k0 += NT * kU) {
+        Record rec[kU];
+#pragma unroll
+        for (int q = 0; q < kU; ++q) {
+            const int k = k0 + q * NT + t;
+            if (k < nrec) rec[q] = recs[k];
+        }
+#pragma unroll
+        for (int q = 0; q < kU; ++q) {
+            const bool ok = k0 + q * NT + t < nrec;
+            const uint32_t lv = ok ? (rec[q].lv & 511u) : 0u;
+            const unsigned long long fx = ok ? to_fix(__fmul_rn(rec[q].sdf_n, rec[q].w_in)) : 0ull;
+            const unsigned m = __ballot_sync(0xffffffffu, ok);
+            if (ok) {
+                const unsigned grp = __match_any_sync(m, lv);
+                unsigned long long acc = 0ull;
+                for (unsigned g = grp; g; g &= g - 1) acc += __shfl_sync(grp, fx, __ffs(g) - 1);
+                if (lane == __ffs(grp) - 1) {
+                    atomicAdd(&cnt[lv], __popc(grp));
+                    atomicAdd(&sum[lv], acc);
+                }
+            }
+        }
+    }
+}
 
-struct ApplySmem {
-    ApplyStage st[kStages];
-    uint64_t full[kStages];
-    uint64_t empty[kStages];
+// A warp per crossing voxel: rank each of the voxel's records by id among
+// them; the `keep` smallest ids are accepted and their values summed.
+__device__ __forceinline__ unsigned long long ranked_sum(const uint32_t* cid, const float* cval,
+                                                         int beg, int n, int keep, int lane) {
+    unsigned long long acc = 0ull;
+    for (int e = lane; e < n; e += 32) {
+        const uint32_t ide = cid[beg + e];
+        int rank = 0;
+        for (int f = 0; f < n; ++f) rank += cid[beg + f] < ide ? 1 : 0;
+        if (rank < keep) acc += to_fix(cval[beg + e]);
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    return acc;
+}
+
+struct __align__(128) ApplySmem {
+    float tile[5][kBlockVoxels];  // weight, tsdf, r, g, b (bulk-copy destination)
+    uint64_t bar;
     int cnt[kBlockVoxels];
     unsigned long long sum[kBlockVoxels];
     short ci[kBlockVoxels];  // crossing index of a voxel, or -1
@@ -131,177 +156,76 @@ struct ApplySmem {
     int ccur[kBlockVoxels];
     uint32_t cid[kCrossCap];
     float cval[kCrossCap];
-    int flags, ncv, ncrec, warp_tot[kConsumerWarps];
+    int item, flags, ncv, warp_tot[kApplyThreads / 32];
 };
 
-// Records of a block for the consumers: from the stage, or from global
-// memory through the block's segments (consumer warps take segments in turn).
-template <class F>
-__device__ __forceinline__ void consumer_records(const UpdateScratch& u, const ApplyStage& st,
-                                                 int c, F&& f) {
-    if (st.mode == kModeShared) {
-        for (int k = c; k < st.info.z; k += kConsumers) f(st.rec[k]);
-    } else {
-        const int warp = c >> 5, lane = c & 31;
-        for (int g = warp; g < st.info.y; g += kConsumerWarps) {
-            const int2 sg = u.seg_list[st.info.x + g];
-            for (int k = lane; k < sg.y; k += 32) f(u.records[sg.x + k]);
-        }
-    }
-}
-
-__global__ void __launch_bounds__(kApplyCta)
+__global__ void __launch_bounds__(kApplyThreads)
 update_apply_kernel(DevVolume v, UpdateScratch u) {
     extern __shared__ __align__(128) unsigned char apply_smem[];
     ApplySmem& S = *reinterpret_cast<ApplySmem*>(apply_smem);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const int n_touched = u.ctl->n_touched;
-
-    if (threadIdx.x == 0) {
-        for (int k = 0; k < kStages; ++k) {
-            mbar_init(&S.full[k], 1);
-            mbar_init(&S.empty[k], kConsumerWarps);
-        }
+    if (t == 0) {
+        mbar_init(&S.bar, 1);
         mbar_fence_init();
         S.flags = 0;
         S.ncv = 0;
     }
-    for (int k = threadIdx.x; k < kBlockVoxels; k += kApplyCta) {
-        S.cnt[k] = 0;
-        S.sum[k] = 0ull;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        S.cnt[4 * t + q] = 0;
+        S.sum[4 * t + q] = 0ull;
     }
     __syncthreads();
 
-    if (warp == 0) {
-        // ---- producer ----
-        float* const arrays[5] = {v.weight, v.tsdf, v.r, v.g, v.b};
-        int issued[kStages];  // last use of each stage this warp filled, -1 none
-#pragma unroll
-        for (int k = 0; k < kStages; ++k) issued[k] = -1;
-        for (int it = 0;; ++it) {
-            const int s = it % kStages;
-            const uint32_t use = (uint32_t)(it / kStages);
-            if (use > 0 && !mbar_wait(&S.empty[s], (use - 1) & 1u, kSpinLimit)) {
-                if (lane == 0) atomicOr(v.status, kStatusSpinTimeout);
-                break;
-            }
-            int item = 0;
-            if (lane == 0) item = atomicAdd(&u.ctl->work, 1);
-            item = __shfl_sync(0xffffffffu, item, 0);
-            ApplyStage& st = S.st[s];
-            issued[s] = (int)use;
-            if (item >= n_touched) {
-                if (lane == 0) {
-                    st.mode = kModeDone;
-                    mbar_arrive(&S.full[s]);
-                }
-                break;
-            }
-            int bi = 0;
-            int4 info = make_int4(0, 0, 0, 0);
-            if (lane == 0) {
-                bi = u.touched[item];
-                info = u.blk_info[bi];
-            }
-            bi = __shfl_sync(0xffffffffu, bi, 0);
-            info.x = __shfl_sync(0xffffffffu, info.x, 0);
-            info.y = __shfl_sync(0xffffffffu, info.y, 0);
-            info.z = __shfl_sync(0xffffffffu, info.z, 0);
-            info.w = bi;
-            if (info.z > kStageRecords || info.y > kStageSegs) {
-                if (lane == 0) {
-                    st.info = info;
-                    st.mode = kModeGlobal;
-                    mbar_arrive(&S.full[s]);
-                }
-                continue;
-            }
-            int2 sg[kStageSegs / 32];
-            int mine = 0;
-#pragma unroll
-            for (int q = 0; q < kStageSegs / 32; ++q) {
-                const int d = lane + 32 * q;
-                sg[q] = d < info.y ? u.seg_list[info.x + d] : make_int2(0, 0);
-                mine += sg[q].y;
-            }
-            int incl = mine;
-            for (int o = 1; o < 32; o <<= 1) {
-                const int y = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += y;
-            }
-            if (lane == 0) {
-                st.info = info;
-                st.mode = kModeShared;
-                mbar_arrive_expect_tx(&S.full[s], 5u * kBlockVoxels * 4u + (uint32_t)info.z * 16u);
-            }
-            __syncwarp();
-            if (lane < 5)
-                bulk_load(st.tile[lane], arrays[lane] + (size_t)bi * kBlockVoxels, kBlockVoxels * 4,
-                          &S.full[s]);
-            int off = incl - mine;
-#pragma unroll
-            for (int q = 0; q < kStageSegs / 32; ++q) {
-                if (sg[q].y > 0) {
-                    bulk_load(&st.rec[off], u.records + sg[q].x, (uint32_t)sg[q].y * 16u, &S.full[s]);
-                    off += sg[q].y;
-                }
-            }
+    float* const arrays[5] = {v.weight, v.tsdf, v.r, v.g, v.b};
+    uint32_t round = 0;  // copies issued so far: the barrier phase to wait for
+    for (;;) {
+        if (t == 0) S.item = atomicAdd(&u.ctl->work, 1);
+        __syncthreads();
+        const int item = S.item;
+        if (item >= n_touched) break;
+        const int32_t bi = u.touched[item];
+        const int4 info = u.blk_info[bi];  // (bin offset, records, -, -)
+        if (info.y > kBigRecords) {
+            if (t == 0) u.big_list[atomicAdd(&u.ctl->n_big, 1)] = bi;
+            __syncthreads();  // everyone has read S.item before it is reused
+            continue;         // no copy was issued for this block
         }
-        // Never leave with copies in flight: wait (bounded) until the last
-        // fill of every stage has landed. Stages the consumers already used
-        // return at once.
-#pragma unroll
-        for (int k = 0; k < kStages; ++k)
-            if (issued[k] >= 0 && !mbar_wait(&S.full[k], (uint32_t)issued[k] & 1u, kSpinLimit) &&
-                lane == 0)
-                atomicOr(v.status, kStatusSpinTimeout);
-        return;
-    }
-
-    // ---- consumers ----
-    const int c = threadIdx.x - 32;
-    const int cw = c >> 5;
-    for (int it = 0;; ++it) {
-        const int s = it % kStages;
-        const uint32_t use = (uint32_t)(it / kStages);
-        if (!mbar_wait(&S.full[s], use & 1u, kSpinLimit)) {
-            if (c == 0) atomicOr(v.status, kStatusSpinTimeout);
-            break;
+        if (t == 0) {
+            // The previous block's tiles were last read before the barrier
+            // above; order those reads before the copies overwrite them.
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            mbar_arrive_expect_tx(&S.bar, 5u * kBlockVoxels * 4u);
+            for (int k = 0; k < 5; ++k)
+                bulk_load(S.tile[k], arrays[k] + (size_t)bi * kBlockVoxels, kBlockVoxels * 4, &S.bar);
         }
-        const ApplyStage& st = S.st[s];
-        const int mode = st.mode;
-        if (mode == kModeDone) break;
-        const int4 info = st.info;
-        const int32_t bi = info.w;
-        const size_t v4 = (size_t)bi * (kBlockVoxels / 4) + c;
-        float4 w0, t0;
-        if (mode == kModeShared) {
-            w0 = reinterpret_cast<const float4*>(st.tile[0])[c];
-            t0 = reinterpret_cast<const float4*>(st.tile[1])[c];
-        } else {
-            w0 = reinterpret_cast<const float4*>(v.weight)[v4];
-            t0 = reinterpret_cast<const float4*>(v.tsdf)[v4];
+        const Record* recs = u.bins + info.x;
+        const int nrec = info.y;
+
+        accumulate_bin<kApplyThreads>(recs, nrec, S.cnt, S.sum);
+        const bool landed = mbar_wait(&S.bar, round & 1u, kSpinLimit);
+        if (__syncthreads_or(!landed)) {
+            if (t == 0) atomicOr(v.status, kStatusSpinTimeout);
+            mbar_wait(&S.bar, round & 1u, kSpinLimit);  // the copies must land before exit
+            return;
         }
+        ++round;
 
-        consumer_records(u, st, c, [&](const Record& rec) {
-            const uint32_t lv = rec.lv & 511u;
-            atomicAdd(&S.cnt[lv], 1);
-            atomicAdd(&S.sum[lv], to_fix(rec.sdf_n, rec.w_in));
-        });
-        named_sync(kConsumerBar, kConsumers);
-
+        const float4 w0 = reinterpret_cast<const float4*>(S.tile[0])[t];
+        const float4 t0 = reinterpret_cast<const float4*>(S.tile[1])[t];
         const float w0a[4] = {w0.x, w0.y, w0.z, w0.w};
         int keep[4];
         int flags = 0;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-            const int n = S.cnt[4 * c + q];
+            const int n = S.cnt[4 * t + q];
             keep[q] = accept_count(w0a[q], v.weight_cap, n);
             if (keep[q] > 0) flags |= 1;
             if (keep[q] > 0 && keep[q] < n) flags |= 2;
         }
         if (flags) atomicOr(&S.flags, flags);
-        named_sync(kConsumerBar, kConsumers);
+        __syncthreads();
         const int block_flags = S.flags;
         bool deferred = false;
 
@@ -309,7 +233,7 @@ update_apply_kernel(DevVolume v, UpdateScratch u) {
             // Ordered selection for the voxels crossing the cap.
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                const int lv = 4 * c + q;
+                const int lv = 4 * t + q;
                 short ci = -1;
                 if (keep[q] > 0 && keep[q] < S.cnt[lv]) {
                     ci = (short)atomicAdd(&S.ncv, 1);
@@ -317,73 +241,62 @@ update_apply_kernel(DevVolume v, UpdateScratch u) {
                 }
                 S.ci[lv] = ci;
             }
-            named_sync(kConsumerBar, kConsumers);
+            __syncthreads();
             const int ncv = S.ncv;
             int local[4], mine = 0;
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                const int ci = 4 * c + q;
+                const int ci = 4 * t + q;
                 local[q] = ci < ncv ? S.cnt[S.cl[ci]] : 0;
                 mine += local[q];
             }
             int incl = mine;
             for (int o = 1; o < 32; o <<= 1) {
                 const int y = __shfl_up_sync(0xffffffffu, incl, o);
-                if ((c & 31) >= o) incl += y;
+                if (lane >= o) incl += y;
             }
-            if ((c & 31) == 31) S.warp_tot[cw] = incl;
-            named_sync(kConsumerBar, kConsumers);
+            if (lane == 31) S.warp_tot[warp] = incl;
+            __syncthreads();
             int before = 0, total = 0;
 #pragma unroll
-            for (int w = 0; w < kConsumerWarps; ++w) {
-                if (w < cw) before += S.warp_tot[w];
+            for (int w = 0; w < kApplyThreads / 32; ++w) {
+                if (w < warp) before += S.warp_tot[w];
                 total += S.warp_tot[w];
             }
-            int run = before + incl - mine;
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int ci = 4 * c + q;
-                if (ci < ncv) {
-                    S.cstart[ci] = run;
-                    S.ccur[ci] = 0;
-                }
-                run += local[q];
-            }
-            if (c == 0) atomicAdd(&u.ctl->n_crossing, 1);
+            if (t == 0) atomicAdd(&u.ctl->n_crossing, 1);
             if (total > kCrossCap) {
                 deferred = true;
-                if (c == 0) u.cross_list[atomicAdd(&u.ctl->n_deferred, 1)] = bi;
+                if (t == 0) u.cross_list[atomicAdd(&u.ctl->n_deferred, 1)] = bi;
             } else {
-                named_sync(kConsumerBar, kConsumers);
-                consumer_records(u, st, c, [&](const Record& rec) {
+                int run = before + incl - mine;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int ci = 4 * t + q;
+                    if (ci < ncv) {
+                        S.cstart[ci] = run;
+                        S.ccur[ci] = 0;
+                    }
+                    run += local[q];
+                }
+                __syncthreads();
+                for (int k = t; k < nrec; k += kApplyThreads) {
+                    const Record rec = recs[k];
                     const int ci = S.ci[rec.lv & 511u];
-                    if (ci < 0) return;
+                    if (ci < 0) continue;
                     const int pos = S.cstart[ci] + atomicAdd(&S.ccur[ci], 1);
                     S.cid[pos] = rec.id;
                     S.cval[pos] = __fmul_rn(rec.sdf_n, rec.w_in);
-                });
-                named_sync(kConsumerBar, kConsumers);
-                const int lane_c = c & 31;
-                for (int ci = cw; ci < ncv; ci += kConsumerWarps) {
+                }
+                __syncthreads();
+                for (int ci = warp; ci < ncv; ci += kApplyThreads / 32) {
                     const int lv = S.cl[ci];
                     const int n = S.cnt[lv];
-                    const int beg = S.cstart[ci];
-                    const float wv = mode == kModeShared ? st.tile[0][lv]
-                                                         : v.weight[(size_t)bi * kBlockVoxels + lv];
-                    const int k = accept_count(wv, v.weight_cap, n);
-                    unsigned long long acc = 0ull;
-                    for (int e = lane_c; e < n; e += 32) {
-                        const uint32_t ide = S.cid[beg + e];
-                        int rank = 0;
-                        for (int f = 0; f < n; ++f) rank += S.cid[beg + f] < ide ? 1 : 0;
-                        if (rank < k)
-                            acc += (unsigned long long)__double2ll_rn((double)S.cval[beg + e] * kFixScale);
-                    }
-                    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-                    if (lane_c == 0) S.sum[lv] = acc;
+                    const int k = accept_count(S.tile[0][lv], v.weight_cap, n);
+                    const unsigned long long acc = ranked_sum(S.cid, S.cval, S.cstart[ci], n, k, lane);
+                    if (lane == 0) S.sum[lv] = acc;
                 }
             }
-            named_sync(kConsumerBar, kConsumers);
+            __syncthreads();
         }
 
         if (!deferred && (block_flags & 1)) {
@@ -391,54 +304,192 @@ update_apply_kernel(DevVolume v, UpdateScratch u) {
             float tn[4], wn[4], dc[4];
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                tn[q] = keep[q] > 0 ? add_fix(t0a[q], S.sum[4 * c + q]) : t0a[q];
+                tn[q] = keep[q] > 0 ? add_fix(t0a[q], S.sum[4 * t + q]) : t0a[q];
                 wn[q] = __fadd_rn(w0a[q], (float)keep[q]);
                 dc[q] = __fmul_rn(128.0f, (float)keep[q]);
             }
+            const size_t v4 = (size_t)bi * (kBlockVoxels / 4) + t;
             reinterpret_cast<float4*>(v.tsdf)[v4] = make_float4(tn[0], tn[1], tn[2], tn[3]);
             reinterpret_cast<float4*>(v.weight)[v4] = make_float4(wn[0], wn[1], wn[2], wn[3]);
-            float* rgb[3] = {v.r, v.g, v.b};
 #pragma unroll
             for (int ch = 0; ch < 3; ++ch) {
-                float4 x = mode == kModeShared ? reinterpret_cast<const float4*>(st.tile[2 + ch])[c]
-                                               : reinterpret_cast<const float4*>(rgb[ch])[v4];
+                float4 x = reinterpret_cast<const float4*>(S.tile[2 + ch])[t];
                 x.x = __fadd_rn(x.x, dc[0]);
                 x.y = __fadd_rn(x.y, dc[1]);
                 x.z = __fadd_rn(x.z, dc[2]);
                 x.w = __fadd_rn(x.w, dc[3]);
-                reinterpret_cast<float4*>(rgb[ch])[v4] = x;
+                reinterpret_cast<float4*>(arrays[2 + ch])[v4] = x;
             }
-            if (c == 0) atomicAdd(&u.ctl->n_accepted, 1);
+            if (t == 0) atomicAdd(&u.ctl->n_accepted, 1);
         }
-        if (c == 0 && !deferred) u.blk_cur[bi] = 0;  // done with its segments
-        named_sync(kConsumerBar, kConsumers);
-        if ((c & 31) == 0) mbar_arrive(&S.empty[s]);
+        if (t == 0 && !deferred) u.blk_cur[bi] = 0;  // done with its bin
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-            S.cnt[4 * c + q] = 0;
-            S.sum[4 * c + q] = 0ull;
+            S.cnt[4 * t + q] = 0;
+            S.sum[4 * t + q] = 0ull;
         }
-        if (c == 0) {
+        __syncthreads();
+        if (t == 0) {
             S.flags = 0;
             S.ncv = 0;
         }
-        named_sync(kConsumerBar, kConsumers);
     }
 }
 
-// Blocks with voxels that cross the cap inside this batch. The records of
-// the crossing voxels are compacted into shared memory once (when they fit),
-// and the radix select runs only over the id bits that differ within the
-// block: a 640x480 frame's block spans ids of a few hundred rows, ~20 bits,
-// i.e. 5 four-bit passes. Histograms are kept for crossing voxels only.
-constexpr int kCrossList = 4096;
+// ---- apply, big blocks ----------------------------------------------------
+//
+// Blocks with more than kBigRecords records: one 1024-thread CTA per SM
+// (persistent over the big list), so a 20k-record block is one pass of ~20
+// records per thread. Threads 0-511 own one voxel each. Crossing voxels are
+// resolved in the CTA as in the regular apply, with room for kBigCrossCap
+// records.
+struct BigSmem {
+    int cnt[kBlockVoxels];
+    unsigned long long sum[kBlockVoxels];
+    short ci[kBlockVoxels];
+    short cl[kBlockVoxels];
+    int cstart[kBlockVoxels];
+    int ccur[kBlockVoxels];
+    uint32_t cid[kBigCrossCap];
+    float cval[kBigCrossCap];
+    int item, flags, ncv, warp_tot[kBigThreads / 32];
+};
 
+__global__ void __launch_bounds__(kBigThreads, 1)
+update_apply_big_kernel(DevVolume v, UpdateScratch u) {
+    extern __shared__ __align__(16) unsigned char big_smem[];
+    BigSmem& S = *reinterpret_cast<BigSmem*>(big_smem);
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int n_items = u.ctl->n_big;
+    if (n_items == 0) return;
+    for (int k = t; k < kBlockVoxels; k += kBigThreads) {
+        S.cnt[k] = 0;
+        S.sum[k] = 0ull;
+    }
+    if (t == 0) {
+        S.flags = 0;
+        S.ncv = 0;
+    }
+    for (;;) {
+        if (t == 0) S.item = atomicAdd(&u.ctl->work3, 1);
+        __syncthreads();
+        const int item = S.item;
+        if (item >= n_items) break;
+        const int32_t bi = u.big_list[item];
+        const int4 info = u.blk_info[bi];
+        const Record* recs = u.bins + info.x;
+        const int nrec = info.y;
+        const bool owner = t < kBlockVoxels;
+        const size_t vox = (size_t)bi * kBlockVoxels + t;
+        const float w0 = owner ? v.weight[vox] : 0.0f;
+
+        accumulate_bin<kBigThreads>(recs, nrec, S.cnt, S.sum);
+        __syncthreads();
+
+        const int n = owner ? S.cnt[t] : 0;
+        const int keep = owner ? accept_count(w0, v.weight_cap, n) : 0;
+        const bool crossing = keep > 0 && keep < n;
+        if (keep > 0) atomicOr(&S.flags, crossing ? 3 : 1);
+        __syncthreads();
+        const int block_flags = S.flags;
+        bool deferred = false;
+
+        if (block_flags & 2) {
+            if (owner) {
+                short ci = -1;
+                if (crossing) {
+                    ci = (short)atomicAdd(&S.ncv, 1);
+                    S.cl[ci] = (short)t;
+                }
+                S.ci[t] = ci;
+            }
+            __syncthreads();
+            const int ncv = S.ncv;
+            const int mine = t < ncv ? S.cnt[S.cl[t]] : 0;
+            int incl = mine;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            if (lane == 31) S.warp_tot[warp] = incl;
+            __syncthreads();
+            if (warp == 0) {
+                int w = S.warp_tot[lane];
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, w, o);
+                    if (lane >= o) w += y;
+                }
+                S.warp_tot[lane] = w;  // inclusive per warp
+            }
+            __syncthreads();
+            const int total = S.warp_tot[kBigThreads / 32 - 1];
+            if (t == 0) atomicAdd(&u.ctl->n_crossing, 1);
+            if (total > kBigCrossCap) {
+                deferred = true;
+                if (t == 0) u.cross_list[atomicAdd(&u.ctl->n_deferred, 1)] = bi;
+            } else {
+                if (t < ncv) {
+                    S.cstart[t] = (warp ? S.warp_tot[warp - 1] : 0) + incl - mine;
+                    S.ccur[t] = 0;
+                }
+                __syncthreads();
+                for (int k = t; k < nrec; k += kBigThreads) {
+                    const Record rec = recs[k];
+                    const int ci = S.ci[rec.lv & 511u];
+                    if (ci < 0) continue;
+                    const int pos = S.cstart[ci] + atomicAdd(&S.ccur[ci], 1);
+                    S.cid[pos] = rec.id;
+                    S.cval[pos] = __fmul_rn(rec.sdf_n, rec.w_in);
+                }
+                __syncthreads();
+                for (int ci = warp; ci < ncv; ci += kBigThreads / 32) {
+                    const int lv = S.cl[ci];
+                    const int nv = S.cnt[lv];
+                    const int kv = accept_count(v.weight[(size_t)bi * kBlockVoxels + lv], v.weight_cap, nv);
+                    const unsigned long long acc = ranked_sum(S.cid, S.cval, S.cstart[ci], nv, kv, lane);
+                    if (lane == 0) S.sum[lv] = acc;
+                }
+            }
+            __syncthreads();
+        }
+
+        if (!deferred && keep > 0) {
+            v.tsdf[vox] = add_fix(v.tsdf[vox], S.sum[t]);
+            v.weight[vox] = __fadd_rn(w0, (float)keep);
+            const float dc = __fmul_rn(128.0f, (float)keep);
+            v.r[vox] = __fadd_rn(v.r[vox], dc);
+            v.g[vox] = __fadd_rn(v.g[vox], dc);
+            v.b[vox] = __fadd_rn(v.b[vox], dc);
+        }
+        if (t == 0) {
+            if (!deferred && (block_flags & 1)) atomicAdd(&u.ctl->n_accepted, 1);
+            if (!deferred) u.blk_cur[bi] = 0;  // done with its bin
+        }
+        if (owner) {
+            S.cnt[t] = 0;
+            S.sum[t] = 0ull;
+        }
+        __syncthreads();
+        if (t == 0) {
+            S.flags = 0;
+            S.ncv = 0;
+        }
+    }
+}
+
+// ---- crossing (deferred blocks) -------------------------------------------
+
+// The records of the crossing voxels are compacted into shared memory once
+// (when they fit), and the radix select runs only over the id bits that
+// differ within the block: a 640x480 frame's block spans ids of a few
+// hundred rows, ~20 bits, i.e. 5 four-bit passes. Histograms are kept for
+// crossing voxels only.
 struct CrossSmem {
     int cnt[kBlockVoxels];
     unsigned long long sum[kBlockVoxels];
     int keep[kBlockVoxels];
-    short ci[kBlockVoxels];      // crossing index of a voxel, or -1
-    short lv[kBlockVoxels];      // voxel of a crossing index
+    short ci[kBlockVoxels];  // crossing index of a voxel, or -1
+    short lv[kBlockVoxels];  // voxel of a crossing index
     uint32_t prefix[kBlockVoxels];
     int rank[kBlockVoxels];
     uint32_t hist[kBlockVoxels * kDigits];
@@ -451,148 +502,144 @@ struct CrossSmem {
 
 __global__ void __launch_bounds__(kCrossThreads, 2)
 update_crossing_kernel(DevVolume v, UpdateScratch u) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    CrossSmem& S = *reinterpret_cast<CrossSmem*>(smem_raw);
-    int* s_cnt = S.cnt;
-    unsigned long long* s_sum = S.sum;
-    int* s_keep = S.keep;
-    short* s_ci = S.ci;
-    short* s_lv = S.lv;
-    uint32_t* s_prefix = S.prefix;
-    int* s_rank = S.rank;
-    uint32_t* s_hist = S.hist;
-    uint32_t* s_id = S.id;
-    float* s_val = S.val;
-    unsigned short* s_lci = S.lci;
-    int& s_item = S.item;
-    int& s_ncv = S.ncv;
-    int& s_nlist = S.nlist;
-    unsigned int& s_minid = S.minid;
-    unsigned int& s_maxid = S.maxid;
-
+    extern __shared__ __align__(16) unsigned char cross_smem[];
+    CrossSmem& S = *reinterpret_cast<CrossSmem*>(cross_smem);
     const int t = threadIdx.x;
     const int n_items = u.ctl->n_deferred;
     for (;;) {
         if (t == 0) {
-            s_item = atomicAdd(&u.ctl->work2, 1);
-            s_ncv = 0;
-            s_nlist = 0;
-            s_minid = 0xffffffffu;
-            s_maxid = 0u;
+            S.item = atomicAdd(&u.ctl->work2, 1);
+            S.ncv = 0;
+            S.nlist = 0;
+            S.minid = 0xffffffffu;
+            S.maxid = 0u;
         }
         for (int k = t; k < kBlockVoxels; k += kCrossThreads) {
-            s_cnt[k] = 0;
-            s_sum[k] = 0ull;
+            S.cnt[k] = 0;
+            S.sum[k] = 0ull;
         }
         __syncthreads();
-        const int item = s_item;
+        const int item = S.item;
         if (item >= n_items) break;
         const int32_t bi = u.cross_list[item];
         const int4 info = u.blk_info[bi];
+        const Record* recs = u.bins + info.x;
+        const int nrec = info.y;
 
-        for_block_records<kCrossThreads>(u, info, [&](const Record& rec) {
+        for (int k = t; k < nrec; k += kCrossThreads) {
+            const Record rec = recs[k];
             const uint32_t lv = rec.lv & 511u;
-            atomicAdd(&s_cnt[lv], 1);
-            atomicAdd(&s_sum[lv], to_fix(rec.sdf_n, rec.w_in));
-        });
+            atomicAdd(&S.cnt[lv], 1);
+            atomicAdd(&S.sum[lv], to_fix(__fmul_rn(rec.sdf_n, rec.w_in)));
+        }
         __syncthreads();
 
         for (int k = t; k < kBlockVoxels; k += kCrossThreads) {
             const float w0 = v.weight[(size_t)bi * kBlockVoxels + k];
-            const int n = s_cnt[k];
+            const int n = S.cnt[k];
             const int keep = accept_count(w0, v.weight_cap, n);
-            s_keep[k] = keep;
+            S.keep[k] = keep;
             short ci = -1;
             if (keep > 0 && keep < n) {
-                ci = (short)atomicAdd(&s_ncv, 1);
-                s_lv[ci] = (short)k;
-                s_rank[ci] = keep;
-                s_sum[k] = 0ull;  // re-summed over the accepted records below
+                ci = (short)atomicAdd(&S.ncv, 1);
+                S.lv[ci] = (short)k;
+                S.rank[ci] = keep;
+                S.sum[k] = 0ull;  // re-summed over the accepted records below
             }
-            s_ci[k] = ci;
+            S.ci[k] = ci;
         }
         __syncthreads();
 
         // Compact the crossing voxels' records.
-        for_block_records<kCrossThreads>(u, info, [&](const Record& rec) {
-            const int ci = s_ci[rec.lv & 511u];
-            if (ci < 0) return;
-            atomicMin(&s_minid, rec.id);
-            atomicMax(&s_maxid, rec.id);
-            const int slot = atomicAdd(&s_nlist, 1);
+        for (int k = t; k < nrec; k += kCrossThreads) {
+            const Record rec = recs[k];
+            const int ci = S.ci[rec.lv & 511u];
+            if (ci < 0) continue;
+            atomicMin(&S.minid, rec.id);
+            atomicMax(&S.maxid, rec.id);
+            const int slot = atomicAdd(&S.nlist, 1);
             if (slot < kCrossList) {
-                s_id[slot] = rec.id;
-                s_val[slot] = __fmul_rn(rec.sdf_n, rec.w_in);
-                s_lci[slot] = (unsigned short)ci;
+                S.id[slot] = rec.id;
+                S.val[slot] = __fmul_rn(rec.sdf_n, rec.w_in);
+                S.lci[slot] = (unsigned short)ci;
             }
-        });
+        }
         __syncthreads();
-        const int ncv = s_ncv;
-        const bool spill = s_nlist > kCrossList;  // too many: read them from the segments
-        const int n_list = s_nlist;
-        const uint32_t diff = s_minid ^ s_maxid;
+        const int ncv = S.ncv;
+        const bool spill = S.nlist > kCrossList;  // too many: read them from the bin
+        const int n_scan = spill ? nrec : S.nlist;
+        const uint32_t diff = S.minid ^ S.maxid;
         const int hi_bit = diff ? 31 - __clz(diff) : 0;
         const int top = (hi_bit / kDigitBits) * kDigitBits;
-        const uint32_t common = top + kDigitBits >= 32 ? 0u : (s_minid >> (top + kDigitBits)) << (top + kDigitBits);
-        for (int c = t; c < ncv; c += kCrossThreads) s_prefix[c] = common;
+        const uint32_t common =
+            top + kDigitBits >= 32 ? 0u : (S.minid >> (top + kDigitBits)) << (top + kDigitBits);
+        for (int c = t; c < ncv; c += kCrossThreads) S.prefix[c] = common;
 
         // Radix select over the differing bits, most significant digit first:
-        // afterwards s_prefix[c] is the id of crossing voxel c's keep-th
+        // afterwards prefix[c] is the id of crossing voxel c's keep-th
         // smallest record, i.e. its last accepted one.
         for (int shift = top; shift >= 0; shift -= kDigitBits) {
-            for (int k = t; k < ncv * kDigits; k += kCrossThreads) s_hist[k] = 0u;
+            for (int k = t; k < ncv * kDigits; k += kCrossThreads) S.hist[k] = 0u;
             __syncthreads();
-            auto count_digit = [&](uint32_t id, int ci) {
+            for (int k = t; k < n_scan; k += kCrossThreads) {
+                uint32_t id;
+                int ci;
+                if (spill) {
+                    const Record rec = recs[k];
+                    ci = S.ci[rec.lv & 511u];
+                    if (ci < 0) continue;
+                    id = rec.id;
+                } else {
+                    id = S.id[k];
+                    ci = S.lci[k];
+                }
                 if (((uint64_t)id >> (shift + kDigitBits)) !=
-                    ((uint64_t)s_prefix[ci] >> (shift + kDigitBits)))
-                    return;
-                atomicAdd(&s_hist[ci * kDigits + ((id >> shift) & (kDigits - 1))], 1u);
-            };
-            if (spill) {
-                for_block_records<kCrossThreads>(u, info, [&](const Record& rec) {
-                    const int ci = s_ci[rec.lv & 511u];
-                    if (ci >= 0) count_digit(rec.id, ci);
-                });
-            } else {
-                for (int k = t; k < n_list; k += kCrossThreads) count_digit(s_id[k], s_lci[k]);
+                    ((uint64_t)S.prefix[ci] >> (shift + kDigitBits)))
+                    continue;
+                atomicAdd(&S.hist[ci * kDigits + ((id >> shift) & (kDigits - 1))], 1u);
             }
             __syncthreads();
             for (int c = t; c < ncv; c += kCrossThreads) {
                 int acc = 0, d = 0;
-                const int rank = s_rank[c];
+                const int rank = S.rank[c];
                 for (; d < kDigits - 1; ++d) {
-                    const int h = (int)s_hist[c * kDigits + d];
+                    const int h = (int)S.hist[c * kDigits + d];
                     if (acc + h >= rank) break;
                     acc += h;
                 }
-                s_rank[c] = rank - acc;
-                s_prefix[c] |= (uint32_t)d << shift;
+                S.rank[c] = rank - acc;
+                S.prefix[c] |= (uint32_t)d << shift;
             }
             __syncthreads();
         }
 
         // Sum the accepted records of the crossing voxels.
-        auto add_accepted = [&](uint32_t id, int ci, float val) {
-            if (id <= s_prefix[ci])
-                atomicAdd(&s_sum[s_lv[ci]], (unsigned long long)__double2ll_rn((double)val * kFixScale));
-        };
-        if (spill) {
-            for_block_records<kCrossThreads>(u, info, [&](const Record& rec) {
-                const int ci = s_ci[rec.lv & 511u];
-                if (ci >= 0) add_accepted(rec.id, ci, __fmul_rn(rec.sdf_n, rec.w_in));
-            });
-        } else {
-            for (int k = t; k < n_list; k += kCrossThreads) add_accepted(s_id[k], s_lci[k], s_val[k]);
+        for (int k = t; k < n_scan; k += kCrossThreads) {
+            uint32_t id;
+            int ci;
+            float val;
+            if (spill) {
+                const Record rec = recs[k];
+                ci = S.ci[rec.lv & 511u];
+                if (ci < 0) continue;
+                id = rec.id;
+                val = __fmul_rn(rec.sdf_n, rec.w_in);
+            } else {
+                id = S.id[k];
+                ci = S.lci[k];
+                val = S.val[k];
+            }
+            if (id <= S.prefix[ci]) atomicAdd(&S.sum[S.lv[ci]], to_fix(val));
         }
         __syncthreads();
 
         int any = 0;
         for (int k = t; k < kBlockVoxels; k += kCrossThreads) {
-            const int keep = s_keep[k];
+            const int keep = S.keep[k];
             if (keep <= 0) continue;
             any = 1;
             const size_t vox = (size_t)bi * kBlockVoxels + k;
-            v.tsdf[vox] = add_fix(v.tsdf[vox], s_sum[k]);
+            v.tsdf[vox] = add_fix(v.tsdf[vox], S.sum[k]);
             v.weight[vox] = __fadd_rn(v.weight[vox], (float)keep);
             const float dc = __fmul_rn(128.0f, (float)keep);
             v.r[vox] = __fadd_rn(v.r[vox], dc);
@@ -602,21 +649,33 @@ update_crossing_kernel(DevVolume v, UpdateScratch u) {
         const int any_keep = __syncthreads_or(any);
         if (t == 0) {
             if (any_keep) atomicAdd(&u.ctl->n_accepted, 1);
-            u.blk_cur[bi] = 0;  // done with its segments
+            u.blk_cur[bi] = 0;  // done with its bin
         }
     }
 }
 
 }  // namespace
 
-cudaError_t launch_update_apply(const DevVolume& v, const UpdateScratch& u, int n_ctas,
-                                cudaStream_t s) {
-    update_apply_kernel<<<n_ctas, kApplyCta, sizeof(ApplySmem), s>>>(v, u);
+cudaError_t launch_update_bin(const UpdateScratch& u, int n_ctas, cudaStream_t s) {
+    update_bin_kernel<<<n_ctas, 256, 0, s>>>(u);
     return cudaGetLastError();
 }
 
-cudaError_t launch_update_place(const UpdateScratch& u, int n_ctas, cudaStream_t s) {
-    update_place_kernel<<<n_ctas, 256, 0, s>>>(u);
+cudaError_t launch_update_apply(const DevVolume& v, const UpdateScratch& u, int n_ctas,
+                                cudaStream_t s) {
+    update_apply_kernel<<<n_ctas, kApplyThreads, sizeof(ApplySmem), s>>>(v, u);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_update_apply_big(const DevVolume& v, const UpdateScratch& u, int n_ctas,
+                                    cudaStream_t s) {
+    update_apply_big_kernel<<<n_ctas, kBigThreads, sizeof(BigSmem), s>>>(v, u);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_update_crossing(const DevVolume& v, const UpdateScratch& u, int n_ctas,
+                                   cudaStream_t s) {
+    update_crossing_kernel<<<n_ctas, kCrossThreads, sizeof(CrossSmem), s>>>(v, u);
     return cudaGetLastError();
 }
 
@@ -625,16 +684,13 @@ cudaError_t prepare_update_kernels() {
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)sizeof(CrossSmem));
     if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(update_apply_big_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(BigSmem));
+    if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(update_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)sizeof(ApplySmem));
 }
 
 size_t apply_smem_bytes() { return sizeof(ApplySmem); }
-
-cudaError_t launch_update_crossing(const DevVolume& v, const UpdateScratch& u, int n_ctas,
-                                   cudaStream_t s) {
-    update_crossing_kernel<<<n_ctas, kCrossThreads, sizeof(CrossSmem), s>>>(v, u);
-    return cudaGetLastError();
-}
 
 }  // namespace osn_b200

@@ -12,15 +12,16 @@
 // with its scratch in one fixed array compiled into the library.
 //
 // The array is a file-scope __device__ variable of kNoAllocScratchBytes
-// (88 MiB + 256 bytes): the control counters, room for kNoAllocMaxRecords
-// 16-byte records and for kNoAllocMaxSegments 24-byte segment entries, i.e.
-// batches with n_points * (2 * steps + 1) <= 4,194,304 (a 640x480 frame at 9
-// band steps per point fits). Every GPU on which the library's code is loaded
-// holds the array until the process exits. Every call shares it and it keeps
-// the last call's contents; the counters that must start at zero are cleared
-// at the start of each call. Two calls whose work overlaps on the GPU (two
-// volumes on different streams, say) race on the array and corrupt each
-// other's results: serialise them.
+// (72 MiB + 256 bytes): the control counters, the staging area and the bins
+// for kNoAllocMaxRecords 16-byte records each, and kNoAllocMaxSegments
+// 16-byte segment descriptors, i.e. batches with
+// n_points * (2 * steps + 1) <= 2,097,152 (a 480x360 frame at 9 band steps
+// per point fits; a 640x480 frame must be split in two). Every GPU on which
+// the library's code is loaded holds the array until the process exits.
+// Every call shares it and it keeps the last call's contents; the counters
+// that must start at zero are cleared at the start of each call. Two calls
+// whose work overlaps on the GPU (two volumes on different streams, say)
+// race on the array and corrupt each other's results: serialise them.
 #include <algorithm>
 #include <cstdio>
 #include <mutex>
@@ -34,11 +35,10 @@ namespace {
 
 constexpr size_t kNoAllocHeaderBytes = 256;  // UpdateControl, padded
 constexpr int64_t kNoAllocMaxRecords = OSN_TSDF_NOALLOC_MAX_RECORDS;
-constexpr int64_t kNoAllocMaxSegments = (int64_t)1 << 20;
+constexpr int64_t kNoAllocMaxSegments = (int64_t)1 << 19;
 constexpr size_t kNoAllocRecordBytes = (size_t)kNoAllocMaxRecords * sizeof(Record);
-constexpr size_t kNoAllocSegBytes = (size_t)kNoAllocMaxSegments * sizeof(int4);
-constexpr size_t kNoAllocScratchBytes = kNoAllocHeaderBytes + kNoAllocRecordBytes + kNoAllocSegBytes +
-                                        (size_t)kNoAllocMaxSegments * sizeof(int2);
+constexpr size_t kNoAllocScratchBytes =
+    kNoAllocHeaderBytes + 2 * kNoAllocRecordBytes + (size_t)kNoAllocMaxSegments * sizeof(int4);
 static_assert(sizeof(UpdateControl) <= kNoAllocHeaderBytes, "control block must fit the header");
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
@@ -76,9 +76,9 @@ cudaError_t Volume::update_static_scratch(const BatchArgs& a, void* scratch) {
     UpdateScratch u = us_;
     u.ctl = reinterpret_cast<UpdateControl*>(base);
     u.records = reinterpret_cast<Record*>(base + kNoAllocHeaderBytes);
+    u.bins = reinterpret_cast<Record*>(base + kNoAllocHeaderBytes + kNoAllocRecordBytes);
     u.record_cap = kNoAllocMaxRecords;
-    u.segs = reinterpret_cast<int4*>(base + kNoAllocHeaderBytes + kNoAllocRecordBytes);
-    u.seg_list = reinterpret_cast<int2*>(base + kNoAllocHeaderBytes + kNoAllocRecordBytes + kNoAllocSegBytes);
+    u.segs = reinterpret_cast<int4*>(base + kNoAllocHeaderBytes + 2 * kNoAllocRecordBytes);
     u.seg_cap = kNoAllocMaxSegments;
     // Only the control counters must start at zero (run_update clears them);
     // the records of the previous call are overwritten before they are read.

@@ -65,11 +65,11 @@ bool Volume::alloc_device(uint32_t hash_slots) {
     OSN_TRY(cudaMalloc(&dv_.g, n_vox * sizeof(float)));
     OSN_TRY(cudaMalloc(&dv_.b, n_vox * sizeof(float)));
     OSN_TRY(cudaMalloc(&us_.blk_cnt, (size_t)dv_.pool_capacity * sizeof(int32_t)));
-    OSN_TRY(cudaMalloc(&us_.blk_nseg, (size_t)dv_.pool_capacity * sizeof(int32_t)));
     OSN_TRY(cudaMalloc(&us_.blk_cur, (size_t)dv_.pool_capacity * sizeof(int32_t)));
     OSN_TRY(cudaMalloc(&us_.blk_info, (size_t)dv_.pool_capacity * sizeof(int4)));
     OSN_TRY(cudaMalloc(&us_.touched, (size_t)dv_.pool_capacity * sizeof(int32_t)));
     OSN_TRY(cudaMalloc(&us_.cross_list, (size_t)dv_.pool_capacity * sizeof(int32_t)));
+    OSN_TRY(cudaMalloc(&us_.big_list, (size_t)dv_.pool_capacity * sizeof(int32_t)));
     OSN_TRY(cudaMalloc(&us_.ctl, sizeof(UpdateControl)));
     OSN_TRY(cudaMalloc(&mesh_ctl_, 2 * sizeof(int32_t)));
     OSN_TRY(cudaMallocHost(&host_small_, 8 * sizeof(int64_t)));
@@ -87,7 +87,6 @@ bool Volume::alloc_device(uint32_t hash_slots) {
     OSN_TRY(cudaMemsetAsync(dv_.g, 0, n_vox * sizeof(float), stream_));
     OSN_TRY(cudaMemsetAsync(dv_.b, 0, n_vox * sizeof(float), stream_));
     OSN_TRY(cudaMemsetAsync(us_.blk_cnt, 0, (size_t)dv_.pool_capacity * sizeof(int32_t), stream_));
-    OSN_TRY(cudaMemsetAsync(us_.blk_nseg, 0, (size_t)dv_.pool_capacity * sizeof(int32_t), stream_));
     OSN_TRY(cudaMemsetAsync(us_.blk_cur, 0, (size_t)dv_.pool_capacity * sizeof(int32_t), stream_));
     OSN_TRY(cudaMemsetAsync(us_.ctl, 0, sizeof(UpdateControl), stream_));
     OSN_TRY(cudaStreamSynchronize(stream_));
@@ -113,13 +112,13 @@ Volume::~Volume() {
     cudaFree(dv_.g);
     cudaFree(dv_.b);
     cudaFree(us_.blk_cnt);
-    cudaFree(us_.blk_nseg);
     cudaFree(us_.blk_cur);
     cudaFree(us_.blk_info);
     cudaFree(us_.segs);
-    cudaFree(us_.seg_list);
+    cudaFree(us_.bins);
     cudaFree(us_.touched);
     cudaFree(us_.cross_list);
+    cudaFree(us_.big_list);
     cudaFree(us_.ctl);
     cudaFree(us_.records);
     cudaFree(mesh_posnor_);
@@ -198,19 +197,19 @@ bool Volume::ensure_records(int64_t n_records, int64_t n_segs) {
     cudaStreamSynchronize(stream_);
     if (n_records > us_.record_cap) {
         cudaFree(us_.records);
+        cudaFree(us_.bins);
         us_.records = nullptr;
+        us_.bins = nullptr;
         us_.record_cap = 0;
         if (cudaMalloc(&us_.records, (size_t)n_records * sizeof(Record)) != cudaSuccess) return false;
+        if (cudaMalloc(&us_.bins, (size_t)n_records * sizeof(Record)) != cudaSuccess) return false;
         us_.record_cap = n_records;
     }
     if (n_segs > us_.seg_cap) {
         cudaFree(us_.segs);
-        cudaFree(us_.seg_list);
         us_.segs = nullptr;
-        us_.seg_list = nullptr;
         us_.seg_cap = 0;
         if (cudaMalloc(&us_.segs, (size_t)n_segs * sizeof(int4)) != cudaSuccess) return false;
-        if (cudaMalloc(&us_.seg_list, (size_t)n_segs * sizeof(int2)) != cudaSuccess) return false;
         us_.seg_cap = n_segs;
     }
     return true;
@@ -223,12 +222,13 @@ cudaError_t Volume::run_update(const BatchArgs& a, const UpdateScratch& u, bool 
     e = launch_update_stage(dv_, a, u, insert, stream_);
     mark_end(kKUpdateStage);
     if (e != cudaSuccess) return e;
-    mark_start(kKUpdatePlace);
-    e = launch_update_place(u, sm_count_ * 4, stream_);
-    mark_end(kKUpdatePlace);
+    mark_start(kKUpdateBin);
+    e = launch_update_bin(u, sm_count_ * 4, stream_);
+    mark_end(kKUpdateBin);
     if (e != cudaSuccess) return e;
     mark_start(kKUpdateApply);
     e = launch_update_apply(dv_, u, sm_count_ * apply_ctas_per_sm_, stream_);
+    if (e == cudaSuccess) e = launch_update_apply_big(dv_, u, sm_count_, stream_);
     mark_end(kKUpdateApply);
     if (e != cudaSuccess) return e;
     mark_start(kKUpdateCrossing);
@@ -322,8 +322,6 @@ cudaError_t Volume::reset() {
     if (e == cudaSuccess) e = cudaMemsetAsync(dv_.status, 0, sizeof(uint32_t), stream_);
     if (e == cudaSuccess)
         e = cudaMemsetAsync(us_.blk_cnt, 0, (size_t)dv_.pool_capacity * sizeof(int32_t), stream_);
-    if (e == cudaSuccess)
-        e = cudaMemsetAsync(us_.blk_nseg, 0, (size_t)dv_.pool_capacity * sizeof(int32_t), stream_);
     if (e == cudaSuccess)
         e = cudaMemsetAsync(us_.blk_cur, 0, (size_t)dv_.pool_capacity * sizeof(int32_t), stream_);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);

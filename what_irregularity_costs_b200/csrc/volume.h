@@ -15,8 +15,8 @@ enum KernelId : int {
     kKAllocate = 0,        // allocate-only walk
     kKUpdateStage = 1,     // count-and-stage walk (fused with allocation in integrate)
     kKUpdateCrossing = 2,  // ordered cap selection for deferred blocks
-    kKUpdatePlace = 3,     // file segment descriptors under their blocks
-    kKUpdateApply = 4,     // tile read-modify-write
+    kKUpdateBin = 3,       // copy staged segments into contiguous per-block bins
+    kKUpdateApply = 4,     // tile read-modify-write (blocks up to 2048 records, then big blocks)
     kKExtract = 5,
     kKReset = 6,
     kNumKernelIds = 7,
@@ -34,7 +34,9 @@ struct UpdateControl {
     int32_t cta_done;    // stage-kernel CTAs finished (the last one scans)
     int32_t n_segs;      // segment descriptors published
     int32_t n_deferred;  // blocks handed to the crossing kernel
-    int32_t pad[3];
+    int32_t n_big;       // blocks handed to the big-block apply
+    int32_t work3;       // big-block apply work cursor
+    int32_t pad[5];
 };
 
 // One binned contribution: 16 bytes, written and read as one vector.
@@ -48,16 +50,16 @@ static_assert(sizeof(Record) == 16, "record must stay one 128-bit vector");
 
 struct UpdateScratch {
     int32_t* blk_cnt = nullptr;     // [pool] records per block; back to 0 after every update
-    int32_t* blk_nseg = nullptr;    // [pool] segments per block; back to 0 after every update
-    int32_t* blk_cur = nullptr;     // [pool] segment filing cursor; back to 0 after every update
-    int4* blk_info = nullptr;       // [pool] (first segment slot, segments, records, -)
+    int32_t* blk_cur = nullptr;     // [pool] bin filling cursor; back to 0 after every update
+    int4* blk_info = nullptr;       // [pool] (bin offset, records, -, -)
     int32_t* touched = nullptr;     // [pool] touched block indices
     int32_t* cross_list = nullptr;  // [pool] blocks deferred to ordered selection
+    int32_t* big_list = nullptr;    // [pool] blocks with more records than a small CTA takes
     UpdateControl* ctl = nullptr;
     Record* records = nullptr;      // staged records, grouped per (walk CTA, block)
+    Record* bins = nullptr;         // the same records, contiguous per block
     int64_t record_cap = 0;
-    int4* segs = nullptr;           // segment descriptors (block, offset, length, -)
-    int2* seg_list = nullptr;       // descriptors filed per block: (offset, length)
+    int4* segs = nullptr;           // segment descriptors (block, staging offset, length, -)
     int64_t seg_cap = 0;
 };
 
@@ -144,14 +146,16 @@ cudaError_t launch_reset_voxels(const DevVolume& v, int32_t n_blocks, cudaStream
 cudaError_t launch_extract(const DevVolume& v, int32_t n_blocks, float min_w, float iso,
                            float* posnor, uint8_t* rgb, int32_t cap, int32_t* ctl, cudaStream_t s);
 
-// The update pipeline: stage (+ per-block segment ranges) -> place -> apply -> crossing.
+// The update pipeline: stage (+ per-block bins) -> bin -> apply -> crossing.
 cudaError_t launch_update_stage(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
                                 bool insert, cudaStream_t s);
-cudaError_t launch_update_place(const UpdateScratch& u, int n_ctas, cudaStream_t s);
+cudaError_t launch_update_bin(const UpdateScratch& u, int n_ctas, cudaStream_t s);
 cudaError_t launch_update_apply(const DevVolume& v, const UpdateScratch& u, int n_ctas,
                                 cudaStream_t s);
 cudaError_t launch_update_crossing(const DevVolume& v, const UpdateScratch& u, int n_ctas,
                                    cudaStream_t s);
+cudaError_t launch_update_apply_big(const DevVolume& v, const UpdateScratch& u, int n_ctas,
+                                    cudaStream_t s);
 // One-time kernel attributes (dynamic shared memory of apply and crossing).
 cudaError_t prepare_update_kernels();
 size_t apply_smem_bytes();

@@ -19,8 +19,8 @@
 // CTA's records grouped by block into one contiguous staging range (one
 // global atomic per CTA reserves it) and publishes one segment descriptor
 // (block, offset, length) per (CTA, block); the last CTA to finish turns the
-// per-block counts into per-block segment ranges, and a small kernel then
-// files each descriptor under its block (update_kernels.cu).
+// per-block counts into per-block bins, and a small kernel then copies each
+// segment into its block's bin (update_kernels.cu).
 //
 // Samples whose voxel already holds the cap's weight are dropped before they
 // are staged: under "accept while weight before < cap" they cannot be
@@ -137,15 +137,15 @@ __device__ __forceinline__ int cta_exclusive_scan(CtaTable& T, int x, int* total
     return excl;
 }
 
-// Exclusive scan of the touched blocks' segment counts into per-block
-// segment ranges, run by the last CTA once every CTA's segments are out.
-// blk_info[bi] = (first segment, segment count, record count); the per-block
-// counters go back to zero for the next batch.
+// Exclusive scan of the touched blocks' record counts into per-block bins,
+// run by the last CTA once every CTA's segments are out: blk_info[bi] =
+// (bin offset, record count). The per-block counters go back to zero for the
+// next batch.
 __device__ void scan_blocks(CtaTable& T, const UpdateScratch& u) {
     const int n = ld_relaxed_s32(&u.ctl->n_touched);
     int carry = 0;
     for (int base = 0; base < n; base += kWalkThreads * kScanPer) {
-        int b[kScanPer], ns[kScanPer];
+        int b[kScanPer], c[kScanPer];
         int local = 0;
         const int first = base + threadIdx.x * kScanPer;
 #pragma unroll
@@ -153,19 +153,18 @@ __device__ void scan_blocks(CtaTable& T, const UpdateScratch& u) {
             b[q] = first + q < n ? ld_relaxed_s32(&u.touched[first + q]) : -1;
 #pragma unroll
         for (int q = 0; q < kScanPer; ++q) {
-            ns[q] = b[q] >= 0 ? ld_relaxed_s32(&u.blk_nseg[b[q]]) : 0;
-            local += ns[q];
+            c[q] = b[q] >= 0 ? ld_relaxed_s32(&u.blk_cnt[b[q]]) : 0;
+            local += c[q];
         }
         int total = 0;
         int run = carry + cta_exclusive_scan(T, local, &total);
 #pragma unroll
         for (int q = 0; q < kScanPer; ++q) {
             if (b[q] >= 0) {
-                u.blk_info[b[q]] = make_int4(run, ns[q], ld_relaxed_s32(&u.blk_cnt[b[q]]), 0);
+                u.blk_info[b[q]] = make_int4(run, c[q], 0, 0);
                 u.blk_cnt[b[q]] = 0;
-                u.blk_nseg[b[q]] = 0;
             }
-            run += ns[q];
+            run += c[q];
         }
         carry += total;
     }
@@ -278,7 +277,6 @@ walk_kernel(DevVolume v, BatchArgs a, UpdateScratch u, unsigned long long* hist,
                     rec.w_in = 1.0f;
                     *reinterpret_cast<int4*>(&u.records[pos]) = *reinterpret_cast<const int4*>(&rec);
                     u.segs[d] = make_int4(bi, pos, 1, 0);
-                    atomicAdd(&u.blk_nseg[bi], 1);
                     if (atomicAdd(&u.blk_cnt[bi], 1) == 0)
                         u.touched[atomicAdd(&u.ctl->n_touched, 1)] = bi;
                 } else {
@@ -334,7 +332,6 @@ walk_kernel(DevVolume v, BatchArgs a, UpdateScratch u, unsigned long long* hist,
                 const int d = atomicAdd(&u.ctl->n_segs, 1);
                 if (d < u.seg_cap) {
                     u.segs[d] = make_int4(bi, off, c, 0);
-                    atomicAdd(&u.blk_nseg[bi], 1);
                     if (atomicAdd(&u.blk_cnt[bi], c) == 0)
                         u.touched[atomicAdd(&u.ctl->n_touched, 1)] = bi;
                 } else {
@@ -377,7 +374,7 @@ walk_kernel(DevVolume v, BatchArgs a, UpdateScratch u, unsigned long long* hist,
     }
 
     if (TAIL == kTailStage) {
-        // The last CTA to finish turns the per-block counts into segment ranges.
+        // The last CTA to finish turns the per-block counts into bins.
         __syncthreads();
         if (tid == 0) {
             __threadfence();
