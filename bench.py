@@ -190,6 +190,57 @@ def cpu_reference_rate(pts, cams, budget_s=15.0, threads=None):
     return done / t_total, done, threads, t_total
 
 
+def a3_gpu_rate(d_all, offsets, cams, steps, torch):
+    """The reference's own CUDA arm (cpp/src/volume_cuda.cu, built for sm_100a
+    into oracle/_ref by oracle/Makefile) on the same device-resident frames:
+    allocate_blocks + update_voxels per frame through its C ABI, CUDA events
+    around each pass over the trajectory; its reset (a full memset of the
+    pool) is outside the timed region, as in the reference's own harness
+    (cpp/bench/bench_arms.cu:707-753)."""
+    import ctypes as C
+    path = os.path.join(ROOT, "oracle", "_ref", "libosn_tsdf_a3.so")
+    if not os.path.exists(path):
+        return None
+    lib = C.CDLL(path)
+    lib.osn_tsdf_cuda_create.restype = C.c_void_p
+    lib.osn_tsdf_cuda_create.argtypes = [C.c_float, C.c_int32, C.c_float, C.c_float]
+    for name in ("osn_tsdf_cuda_allocate_blocks", "osn_tsdf_cuda_update_voxels"):
+        getattr(lib, name).argtypes = [C.c_void_p, C.c_void_p, C.c_int32] + [C.c_float] * 4
+    lib.osn_tsdf_cuda_reset.argtypes = [C.c_void_p]
+    lib.osn_tsdf_cuda_synchronize.argtypes = [C.c_void_p]
+    lib.osn_tsdf_cuda_block_count.argtypes = [C.c_void_p]
+    lib.osn_tsdf_cuda_drop_count.argtypes = [C.c_void_p]
+    lib.osn_tsdf_cuda_drop_count.restype = C.c_uint64
+    lib.osn_tsdf_cuda_destroy.argtypes = [C.c_void_p]
+    v = lib.osn_tsdf_cuda_create(VOXEL, POOL, TRUNC, CAP)
+    if not v:
+        return None
+    total_ms = 0.0
+    try:
+        for step in range(steps + 1):  # the first pass is a warm-up
+            lib.osn_tsdf_cuda_reset(v)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()  # legacy default stream: ordered with the arm's blocking stream
+            for k in range(len(cams)):
+                a, b = int(offsets[k]), int(offsets[k + 1])
+                ptr = d_all.data_ptr() + a * 12
+                lib.osn_tsdf_cuda_allocate_blocks(v, ptr, b - a, *cams[k], 0.0)
+                lib.osn_tsdf_cuda_update_voxels(v, ptr, b - a, *cams[k], 0.0)
+            lib.osn_tsdf_cuda_synchronize(v)
+            e1.record()
+            torch.cuda.synchronize()
+            if step > 0:
+                total_ms += e0.elapsed_time(e1)
+        blocks = lib.osn_tsdf_cuda_block_count(v)
+        drops = lib.osn_tsdf_cuda_drop_count(v)
+    finally:
+        lib.osn_tsdf_cuda_destroy(v)
+    return {"impl": "reference CUDA arm (A3, cpp/src/volume_cuda.cu) built for sm_100a, same GPU",
+            "value": len(cams) * steps / (total_ms / 1e3), "unit": "frames/s",
+            "ms_per_step": total_ms / steps, "blocks": blocks, "drops": int(drops)}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -339,14 +390,14 @@ def run_ours(args):
 
     peak, peak_kind = measured_peak()
     t_alloc = per_kernel["allocate"][0] / 1e3
-    t_update = sum(per_kernel[k][0] for k in ("update_stage", "update_crossing", "update_bin",
+    t_update = sum(per_kernel[k][0] for k in ("update_stage", "update_apply_big", "update_bin",
                                                "update_apply")) / 1e3
     tile_bytes = sum(accepted) * 512 * 2 * 8          # tsdf + weight, read + write
     rgb_bytes = sum(accepted) * 512 * 2 * 12
     update_alg_bytes = 12 * n_points + tile_bytes
     # Algorithmic bytes per launch of each kernel (roofline).
     alg = {
-        "update_apply": tile_bytes / N_FRAMES,
+        "update_apply": tile_bytes / N_FRAMES,  # refined below when the big-block share is known
         "update_stage": 12 * n_points / N_FRAMES,
         "allocate": 12 * n_points / N_FRAMES,
     }
@@ -359,6 +410,13 @@ def run_ours(args):
         "traffic": profile_traffic() if dominant == "update_apply" else None,
         "alg_bytes_per_launch": dom_alg, "mean_launch_us": 1e3 * dom_ms / dom_n if dom_n else None,
     }
+
+    a3 = None
+    if rank == 0 and not args.no_a3:
+        try:
+            a3 = a3_gpu_rate(d_all, offsets, cams, max(1, min(args.steps, 3)), torch)
+        except Exception as e:  # reported beside the line, never required
+            a3 = {"impl": "reference CUDA arm (A3)", "value": None, "error": str(e)}
 
     cpu = None
     if rank == 0 and not args.no_cpu:
@@ -383,6 +441,7 @@ def run_ours(args):
             "config": config_dict(n_points),
             "roofline": roofline,
             "cpu_baseline": cpu,
+            "reference_gpu_arm": a3,
             "e2e": {"value": e2e_value, "unit": "frames/s",
                     "h2d_bytes_per_step": int(all_pts.nbytes), "d2h_bytes_per_step": 16},
             "gpu_launches": int(launches_per_step * args.steps),
@@ -412,6 +471,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-a3", action="store_true", help="skip timing the reference's CUDA arm")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--ref-frames", type=int, default=20,
                     help="frames per step of the reference arm")

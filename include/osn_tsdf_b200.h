@@ -182,7 +182,7 @@ int32_t osn_tsdf_cuda_update_voxels_noalloc(OsnTsdfCudaVolume* v, const float* d
  * bracketed by CUDA events on the volume's stream; kernel_times reads (and
  * waits for) the accumulated per-kernel milliseconds and launch counts.
  * Kernel ids: 0 allocate, 1 update-stage (allocate+stage in integrate),
- * 2 update-crossing (ordered cap selection), 3 update-bin,
+ * 2 update-apply of blocks above 2048 records, 3 update-bin,
  * 4 update-apply, 5 extract, 6 reset. Returns the number of ids written. */
 int32_t osn_tsdf_cuda_set_timing(OsnTsdfCudaVolume* v, int32_t enabled);
 int32_t osn_tsdf_cuda_kernel_times(OsnTsdfCudaVolume* v, double* ms, int64_t* launches,

@@ -162,6 +162,23 @@ def test_pool_exactly_full(cuda):
     assert_same_voxels(gpu, ref)
 
 
+def test_many_rays_through_one_voxel(cuda):
+    """3000 rays through the same voxels plus a sparse frame: voxels with
+    thousands of records in one batch cross the cap in the big-block path."""
+    rng = np.random.default_rng(7)
+    same = np.repeat(np.float32([[0.31, -0.27, 1.93]]), 3000, axis=0)
+    jitter = (np.float32([0.31, -0.27, 1.93]) +
+              rng.normal(0, 0.01, size=(2000, 3)).astype(np.float32))
+    pts = np.concatenate([same, jitter, same[:500]]).astype(np.float32)
+    gpu, ref = _pair(cuda, [(pts, (0.0, 0.0, 0.0)), (pts[::3], (0.0, 0.0, 0.0))], 0.01, 1 << 12,
+                     0.04, 64.0)
+    assert gpu.status() == 0
+    assert_same_blocks(gpu, ref)
+    assert_same_voxels(gpu, ref)
+    _, _, w, *_ = ref.voxels()
+    assert w.max() == 64.0
+
+
 def test_radius_cutoff_and_offset_camera(cuda):
     """Far cutoff and a camera far from the origin (negative block coordinates)."""
     f = scenes.sphere_frame()

@@ -18,9 +18,7 @@
 //   bin       one warp per segment copies its records into the block's
 //             contiguous bin (L2-resident traffic);
 //   apply     one 128-thread CTA per touched block (persistent, work-queued,
-//             many per SM), 4 voxels per thread; blocks with more than 2048
-//             records go to a 1024-thread CTA instead (one per SM), so the
-//             largest blocks of a frame (~20k records) do not form a tail. The block's five 2 KB tiles
+//             many per SM), 4 voxels per thread. The block's five 2 KB tiles
 //             are staged into shared memory by cp.async.bulk while the CTA
 //             makes one pass over the bin: per-voxel record counts and sums,
 //             combined per warp with __match_any_sync before the shared
@@ -28,11 +26,10 @@
 //             cap. Voxels that cross the cap inside the batch are resolved in
 //             the CTA: their records are grouped per voxel in shared memory
 //             and a warp counts each record's rank by id among its voxel's
-//             records; the `keep` lowest are accepted. Blocks with more such
-//             records than fit are deferred to
-//   crossing  one 256-thread CTA per deferred block: an exact radix select
-//             (4-bit digits over the record ids) finds the id of each
-//             crossing voxel's last accepted record.
+//             records; the `keep` lowest are accepted. Blocks with more than
+//             2048 records, or more crossing records than the CTA holds, go to
+//   big       one 1024-thread CTA per SM and block, same algorithm, crossing
+//             records gathered in groups of up to 16384.
 //
 // Sums are accumulated in 64-bit fixed point (2^-40 resolution, exact for
 // |value| >= 2^-17) and added to the stored sum with one rounding, so results
@@ -48,12 +45,8 @@ namespace {
 constexpr int kApplyThreads = 128;  // 4 voxels per thread
 constexpr int kBigThreads = 1024;   // big blocks: one CTA per SM
 constexpr int kBigRecords = 2048;   // blocks above this go to the big-block apply
-constexpr int kCrossThreads = 256;  // deferred blocks: two voxels per thread
 constexpr int kCrossCap = 1024;     // crossing records resolved inside apply
 constexpr int kBigCrossCap = 16384; // crossing records resolved inside the big-block apply
-constexpr int kCrossList = 4096;    // crossing records the deferred kernel holds in shared memory
-constexpr int kDigitBits = 4;
-constexpr int kDigits = 1 << kDigitBits;
 constexpr double kFixScale = 1099511627776.0;      // 2^40
 constexpr double kFixInv = 1.0 / 1099511627776.0;  // 2^-40
 
@@ -80,6 +73,9 @@ __device__ __forceinline__ float add_fix(float t0, unsigned long long acc) {
 
 __global__ void __launch_bounds__(256)
 update_bin_kernel(UpdateScratch u) {
+    // One warp per segment over a grid of ~19k warps, so the descriptor load
+    // and the cursor atomic of many segments are in flight at once; four
+    // 16-byte records per lane in flight during the copy.
     const int n = (int)min((long long)u.ctl->n_segs, (long long)u.seg_cap);
     const int lane = threadIdx.x & 31;
     const int warps = gridDim.x * (blockDim.x >> 5);
@@ -90,7 +86,15 @@ update_bin_kernel(UpdateScratch u) {
         at = __shfl_sync(0xffffffffu, at, 0);
         const int4* src = reinterpret_cast<const int4*>(u.records + sg.y);
         int4* dst = reinterpret_cast<int4*>(u.bins + at);
-        for (int k = lane; k < sg.z; k += 32) dst[k] = src[k];
+        for (int k = lane; k < sg.z; k += 128) {
+            int4 r[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if (k + 32 * q < sg.z) r[q] = src[k + 32 * q];
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if (k + 32 * q < sg.z) dst[k + 32 * q] = r[q];
+        }
     }
 }
 
@@ -263,11 +267,13 @@ update_apply_kernel(DevVolume v, UpdateScratch u) {
                 if (w < warp) before += S.warp_tot[w];
                 total += S.warp_tot[w];
             }
-            if (t == 0) atomicAdd(&u.ctl->n_crossing, 1);
             if (total > kCrossCap) {
+                // More crossing records than this CTA holds: the big-block
+                // CTA (room for kBigCrossCap) takes the whole block.
                 deferred = true;
-                if (t == 0) u.cross_list[atomicAdd(&u.ctl->n_deferred, 1)] = bi;
+                if (t == 0) u.big_list[atomicAdd(&u.ctl->n_big, 1)] = bi;
             } else {
+                if (t == 0) atomicAdd(&u.ctl->n_crossing, 1);
                 int run = before + incl - mine;
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
@@ -338,11 +344,11 @@ update_apply_kernel(DevVolume v, UpdateScratch u) {
 
 // ---- apply, big blocks ----------------------------------------------------
 //
-// Blocks with more than kBigRecords records: one 1024-thread CTA per SM
-// (persistent over the big list), so a 20k-record block is one pass of ~20
-// records per thread. Threads 0-511 own one voxel each. Crossing voxels are
-// resolved in the CTA as in the regular apply, with room for kBigCrossCap
-// records.
+// Blocks with more than kBigRecords records, and blocks whose cap-crossing
+// records overflow the regular CTA: one 1024-thread CTA per SM (persistent
+// over the big list), so a 20k-record block is one pass of ~20 records per
+// thread. Threads 0-511 own one voxel each. Crossing voxels are resolved in
+// the CTA as in the regular apply, in groups of up to kBigCrossCap records.
 struct BigSmem {
     int cnt[kBlockVoxels];
     unsigned long long sum[kBlockVoxels];
@@ -352,7 +358,7 @@ struct BigSmem {
     int ccur[kBlockVoxels];
     uint32_t cid[kBigCrossCap];
     float cval[kBigCrossCap];
-    int item, flags, ncv, warp_tot[kBigThreads / 32];
+    int item, flags, ncv, group_hi, warp_tot[kBigThreads / 32];
 };
 
 __global__ void __launch_bounds__(kBigThreads, 1)
@@ -371,7 +377,7 @@ update_apply_big_kernel(DevVolume v, UpdateScratch u) {
         S.ncv = 0;
     }
     for (;;) {
-        if (t == 0) S.item = atomicAdd(&u.ctl->work3, 1);
+        if (t == 0) S.item = atomicAdd(&u.ctl->work_big, 1);
         __syncthreads();
         const int item = S.item;
         if (item >= n_items) break;
@@ -392,7 +398,6 @@ update_apply_big_kernel(DevVolume v, UpdateScratch u) {
         if (keep > 0) atomicOr(&S.flags, crossing ? 3 : 1);
         __syncthreads();
         const int block_flags = S.flags;
-        bool deferred = false;
 
         if (block_flags & 2) {
             if (owner) {
@@ -422,38 +427,66 @@ update_apply_big_kernel(DevVolume v, UpdateScratch u) {
                 S.warp_tot[lane] = w;  // inclusive per warp
             }
             __syncthreads();
-            const int total = S.warp_tot[kBigThreads / 32 - 1];
             if (t == 0) atomicAdd(&u.ctl->n_crossing, 1);
-            if (total > kBigCrossCap) {
-                deferred = true;
-                if (t == 0) u.cross_list[atomicAdd(&u.ctl->n_deferred, 1)] = bi;
-            } else {
-                if (t < ncv) {
-                    S.cstart[t] = (warp ? S.warp_tot[warp - 1] : 0) + incl - mine;
-                    S.ccur[t] = 0;
-                }
-                __syncthreads();
-                for (int k = t; k < nrec; k += kBigThreads) {
-                    const Record rec = recs[k];
-                    const int ci = S.ci[rec.lv & 511u];
-                    if (ci < 0) continue;
-                    const int pos = S.cstart[ci] + atomicAdd(&S.ccur[ci], 1);
-                    S.cid[pos] = rec.id;
-                    S.cval[pos] = __fmul_rn(rec.sdf_n, rec.w_in);
-                }
-                __syncthreads();
-                for (int ci = warp; ci < ncv; ci += kBigThreads / 32) {
-                    const int lv = S.cl[ci];
-                    const int nv = S.cnt[lv];
-                    const int kv = accept_count(v.weight[(size_t)bi * kBlockVoxels + lv], v.weight_cap, nv);
-                    const unsigned long long acc = ranked_sum(S.cid, S.cval, S.cstart[ci], nv, kv, lane);
-                    if (lane == 0) S.sum[lv] = acc;
-                }
-            }
+            if (t < ncv) S.cstart[t] = (warp ? S.warp_tot[warp - 1] : 0) + incl - mine;
             __syncthreads();
+            // Crossing voxels in groups whose records fit the buffer: one
+            // pass over the bin gathers a group, warps rank its voxels.
+            for (int lo = 0; lo < ncv;) {
+                if (t == 0) {
+                    int hi = lo + 1;
+                    while (hi < ncv && S.cstart[hi] + S.cnt[S.cl[hi]] - S.cstart[lo] <= kBigCrossCap) ++hi;
+                    S.group_hi = hi;
+                }
+                __syncthreads();
+                const int hi = S.group_hi;
+                const int base = S.cstart[lo];
+                if (S.cnt[S.cl[lo]] <= kBigCrossCap) {
+                    if (t >= lo && t < hi) S.ccur[t] = 0;
+                    __syncthreads();
+                    for (int k = t; k < nrec; k += kBigThreads) {
+                        const Record rec = recs[k];
+                        const int ci = S.ci[rec.lv & 511u];
+                        if (ci < lo || ci >= hi) continue;
+                        const int pos = S.cstart[ci] - base + atomicAdd(&S.ccur[ci], 1);
+                        S.cid[pos] = rec.id;
+                        S.cval[pos] = __fmul_rn(rec.sdf_n, rec.w_in);
+                    }
+                    __syncthreads();
+                    for (int ci = lo + warp; ci < hi; ci += kBigThreads / 32) {
+                        const int lv = S.cl[ci];
+                        const int nv = S.cnt[lv];
+                        const int kv = accept_count(v.weight[(size_t)bi * kBlockVoxels + lv], v.weight_cap, nv);
+                        const unsigned long long acc =
+                            ranked_sum(S.cid, S.cval, S.cstart[ci] - base, nv, kv, lane);
+                        if (lane == 0) S.sum[lv] = acc;
+                    }
+                } else {
+                    // One voxel with more records than the buffer holds (only
+                    // an adversarial batch gets here): rank its records
+                    // against the bin in global memory.
+                    const int lv = S.cl[lo];
+                    const int kv = accept_count(v.weight[(size_t)bi * kBlockVoxels + lv], v.weight_cap,
+                                                S.cnt[lv]);
+                    if (t == 0) S.sum[lv] = 0ull;
+                    __syncthreads();
+                    for (int k = t; k < nrec; k += kBigThreads) {
+                        const Record rec = recs[k];
+                        if ((int)(rec.lv & 511u) != lv) continue;
+                        int rank = 0;
+                        for (int f = 0; f < nrec; ++f) {
+                            const Record o = recs[f];
+                            rank += ((int)(o.lv & 511u) == lv && o.id < rec.id) ? 1 : 0;
+                        }
+                        if (rank < kv) atomicAdd(&S.sum[lv], to_fix(__fmul_rn(rec.sdf_n, rec.w_in)));
+                    }
+                }
+                __syncthreads();
+                lo = hi;
+            }
         }
 
-        if (!deferred && keep > 0) {
+        if (keep > 0) {
             v.tsdf[vox] = add_fix(v.tsdf[vox], S.sum[t]);
             v.weight[vox] = __fadd_rn(w0, (float)keep);
             const float dc = __fmul_rn(128.0f, (float)keep);
@@ -462,8 +495,8 @@ update_apply_big_kernel(DevVolume v, UpdateScratch u) {
             v.b[vox] = __fadd_rn(v.b[vox], dc);
         }
         if (t == 0) {
-            if (!deferred && (block_flags & 1)) atomicAdd(&u.ctl->n_accepted, 1);
-            if (!deferred) u.blk_cur[bi] = 0;  // done with its bin
+            if (block_flags & 1) atomicAdd(&u.ctl->n_accepted, 1);
+            u.blk_cur[bi] = 0;  // done with its bin
         }
         if (owner) {
             S.cnt[t] = 0;
@@ -473,183 +506,6 @@ update_apply_big_kernel(DevVolume v, UpdateScratch u) {
         if (t == 0) {
             S.flags = 0;
             S.ncv = 0;
-        }
-    }
-}
-
-// ---- crossing (deferred blocks) -------------------------------------------
-
-// The records of the crossing voxels are compacted into shared memory once
-// (when they fit), and the radix select runs only over the id bits that
-// differ within the block: a 640x480 frame's block spans ids of a few
-// hundred rows, ~20 bits, i.e. 5 four-bit passes. Histograms are kept for
-// crossing voxels only.
-struct CrossSmem {
-    int cnt[kBlockVoxels];
-    unsigned long long sum[kBlockVoxels];
-    int keep[kBlockVoxels];
-    short ci[kBlockVoxels];  // crossing index of a voxel, or -1
-    short lv[kBlockVoxels];  // voxel of a crossing index
-    uint32_t prefix[kBlockVoxels];
-    int rank[kBlockVoxels];
-    uint32_t hist[kBlockVoxels * kDigits];
-    uint32_t id[kCrossList];
-    float val[kCrossList];
-    unsigned short lci[kCrossList];
-    int item, ncv, nlist;
-    unsigned int minid, maxid;
-};
-
-__global__ void __launch_bounds__(kCrossThreads, 2)
-update_crossing_kernel(DevVolume v, UpdateScratch u) {
-    extern __shared__ __align__(16) unsigned char cross_smem[];
-    CrossSmem& S = *reinterpret_cast<CrossSmem*>(cross_smem);
-    const int t = threadIdx.x;
-    const int n_items = u.ctl->n_deferred;
-    for (;;) {
-        if (t == 0) {
-            S.item = atomicAdd(&u.ctl->work2, 1);
-            S.ncv = 0;
-            S.nlist = 0;
-            S.minid = 0xffffffffu;
-            S.maxid = 0u;
-        }
-        for (int k = t; k < kBlockVoxels; k += kCrossThreads) {
-            S.cnt[k] = 0;
-            S.sum[k] = 0ull;
-        }
-        __syncthreads();
-        const int item = S.item;
-        if (item >= n_items) break;
-        const int32_t bi = u.cross_list[item];
-        const int4 info = u.blk_info[bi];
-        const Record* recs = u.bins + info.x;
-        const int nrec = info.y;
-
-        for (int k = t; k < nrec; k += kCrossThreads) {
-            const Record rec = recs[k];
-            const uint32_t lv = rec.lv & 511u;
-            atomicAdd(&S.cnt[lv], 1);
-            atomicAdd(&S.sum[lv], to_fix(__fmul_rn(rec.sdf_n, rec.w_in)));
-        }
-        __syncthreads();
-
-        for (int k = t; k < kBlockVoxels; k += kCrossThreads) {
-            const float w0 = v.weight[(size_t)bi * kBlockVoxels + k];
-            const int n = S.cnt[k];
-            const int keep = accept_count(w0, v.weight_cap, n);
-            S.keep[k] = keep;
-            short ci = -1;
-            if (keep > 0 && keep < n) {
-                ci = (short)atomicAdd(&S.ncv, 1);
-                S.lv[ci] = (short)k;
-                S.rank[ci] = keep;
-                S.sum[k] = 0ull;  // re-summed over the accepted records below
-            }
-            S.ci[k] = ci;
-        }
-        __syncthreads();
-
-        // Compact the crossing voxels' records.
-        for (int k = t; k < nrec; k += kCrossThreads) {
-            const Record rec = recs[k];
-            const int ci = S.ci[rec.lv & 511u];
-            if (ci < 0) continue;
-            atomicMin(&S.minid, rec.id);
-            atomicMax(&S.maxid, rec.id);
-            const int slot = atomicAdd(&S.nlist, 1);
-            if (slot < kCrossList) {
-                S.id[slot] = rec.id;
-                S.val[slot] = __fmul_rn(rec.sdf_n, rec.w_in);
-                S.lci[slot] = (unsigned short)ci;
-            }
-        }
-        __syncthreads();
-        const int ncv = S.ncv;
-        const bool spill = S.nlist > kCrossList;  // too many: read them from the bin
-        const int n_scan = spill ? nrec : S.nlist;
-        const uint32_t diff = S.minid ^ S.maxid;
-        const int hi_bit = diff ? 31 - __clz(diff) : 0;
-        const int top = (hi_bit / kDigitBits) * kDigitBits;
-        const uint32_t common =
-            top + kDigitBits >= 32 ? 0u : (S.minid >> (top + kDigitBits)) << (top + kDigitBits);
-        for (int c = t; c < ncv; c += kCrossThreads) S.prefix[c] = common;
-
-        // Radix select over the differing bits, most significant digit first:
-        // afterwards prefix[c] is the id of crossing voxel c's keep-th
-        // smallest record, i.e. its last accepted one.
-        for (int shift = top; shift >= 0; shift -= kDigitBits) {
-            for (int k = t; k < ncv * kDigits; k += kCrossThreads) S.hist[k] = 0u;
-            __syncthreads();
-            for (int k = t; k < n_scan; k += kCrossThreads) {
-                uint32_t id;
-                int ci;
-                if (spill) {
-                    const Record rec = recs[k];
-                    ci = S.ci[rec.lv & 511u];
-                    if (ci < 0) continue;
-                    id = rec.id;
-                } else {
-                    id = S.id[k];
-                    ci = S.lci[k];
-                }
-                if (((uint64_t)id >> (shift + kDigitBits)) !=
-                    ((uint64_t)S.prefix[ci] >> (shift + kDigitBits)))
-                    continue;
-                atomicAdd(&S.hist[ci * kDigits + ((id >> shift) & (kDigits - 1))], 1u);
-            }
-            __syncthreads();
-            for (int c = t; c < ncv; c += kCrossThreads) {
-                int acc = 0, d = 0;
-                const int rank = S.rank[c];
-                for (; d < kDigits - 1; ++d) {
-                    const int h = (int)S.hist[c * kDigits + d];
-                    if (acc + h >= rank) break;
-                    acc += h;
-                }
-                S.rank[c] = rank - acc;
-                S.prefix[c] |= (uint32_t)d << shift;
-            }
-            __syncthreads();
-        }
-
-        // Sum the accepted records of the crossing voxels.
-        for (int k = t; k < n_scan; k += kCrossThreads) {
-            uint32_t id;
-            int ci;
-            float val;
-            if (spill) {
-                const Record rec = recs[k];
-                ci = S.ci[rec.lv & 511u];
-                if (ci < 0) continue;
-                id = rec.id;
-                val = __fmul_rn(rec.sdf_n, rec.w_in);
-            } else {
-                id = S.id[k];
-                ci = S.lci[k];
-                val = S.val[k];
-            }
-            if (id <= S.prefix[ci]) atomicAdd(&S.sum[S.lv[ci]], to_fix(val));
-        }
-        __syncthreads();
-
-        int any = 0;
-        for (int k = t; k < kBlockVoxels; k += kCrossThreads) {
-            const int keep = S.keep[k];
-            if (keep <= 0) continue;
-            any = 1;
-            const size_t vox = (size_t)bi * kBlockVoxels + k;
-            v.tsdf[vox] = add_fix(v.tsdf[vox], S.sum[k]);
-            v.weight[vox] = __fadd_rn(v.weight[vox], (float)keep);
-            const float dc = __fmul_rn(128.0f, (float)keep);
-            v.r[vox] = __fadd_rn(v.r[vox], dc);
-            v.g[vox] = __fadd_rn(v.g[vox], dc);
-            v.b[vox] = __fadd_rn(v.b[vox], dc);
-        }
-        const int any_keep = __syncthreads_or(any);
-        if (t == 0) {
-            if (any_keep) atomicAdd(&u.ctl->n_accepted, 1);
-            u.blk_cur[bi] = 0;  // done with its bin
         }
     }
 }
@@ -673,18 +529,8 @@ cudaError_t launch_update_apply_big(const DevVolume& v, const UpdateScratch& u, 
     return cudaGetLastError();
 }
 
-cudaError_t launch_update_crossing(const DevVolume& v, const UpdateScratch& u, int n_ctas,
-                                   cudaStream_t s) {
-    update_crossing_kernel<<<n_ctas, kCrossThreads, sizeof(CrossSmem), s>>>(v, u);
-    return cudaGetLastError();
-}
-
 cudaError_t prepare_update_kernels() {
-    cudaError_t e = cudaFuncSetAttribute(update_crossing_kernel,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)sizeof(CrossSmem));
-    if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(update_apply_big_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(update_apply_big_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)sizeof(BigSmem));
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(update_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,

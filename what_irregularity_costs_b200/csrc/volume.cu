@@ -68,7 +68,6 @@ bool Volume::alloc_device(uint32_t hash_slots) {
     OSN_TRY(cudaMalloc(&us_.blk_cur, (size_t)dv_.pool_capacity * sizeof(int32_t)));
     OSN_TRY(cudaMalloc(&us_.blk_info, (size_t)dv_.pool_capacity * sizeof(int4)));
     OSN_TRY(cudaMalloc(&us_.touched, (size_t)dv_.pool_capacity * sizeof(int32_t)));
-    OSN_TRY(cudaMalloc(&us_.cross_list, (size_t)dv_.pool_capacity * sizeof(int32_t)));
     OSN_TRY(cudaMalloc(&us_.big_list, (size_t)dv_.pool_capacity * sizeof(int32_t)));
     OSN_TRY(cudaMalloc(&us_.ctl, sizeof(UpdateControl)));
     OSN_TRY(cudaMalloc(&mesh_ctl_, 2 * sizeof(int32_t)));
@@ -95,7 +94,6 @@ bool Volume::alloc_device(uint32_t hash_slots) {
     int per_sm = 0;
     OSN_TRY(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
     apply_ctas_per_sm_ = std::max(1, per_sm / (int)(apply_smem_bytes() + 1024));
-    cross_ctas_per_sm_ = 2;
     return true;
 }
 
@@ -117,7 +115,6 @@ Volume::~Volume() {
     cudaFree(us_.segs);
     cudaFree(us_.bins);
     cudaFree(us_.touched);
-    cudaFree(us_.cross_list);
     cudaFree(us_.big_list);
     cudaFree(us_.ctl);
     cudaFree(us_.records);
@@ -223,17 +220,16 @@ cudaError_t Volume::run_update(const BatchArgs& a, const UpdateScratch& u, bool 
     mark_end(kKUpdateStage);
     if (e != cudaSuccess) return e;
     mark_start(kKUpdateBin);
-    e = launch_update_bin(u, sm_count_ * 4, stream_);
+    e = launch_update_bin(u, sm_count_ * 16, stream_);
     mark_end(kKUpdateBin);
     if (e != cudaSuccess) return e;
     mark_start(kKUpdateApply);
     e = launch_update_apply(dv_, u, sm_count_ * apply_ctas_per_sm_, stream_);
-    if (e == cudaSuccess) e = launch_update_apply_big(dv_, u, sm_count_, stream_);
     mark_end(kKUpdateApply);
     if (e != cudaSuccess) return e;
-    mark_start(kKUpdateCrossing);
-    e = launch_update_crossing(dv_, u, sm_count_ * cross_ctas_per_sm_, stream_);
-    mark_end(kKUpdateCrossing);
+    mark_start(kKUpdateApplyBig);
+    e = launch_update_apply_big(dv_, u, sm_count_, stream_);
+    mark_end(kKUpdateApplyBig);
     return e;
 }
 

@@ -14,9 +14,9 @@ namespace osn_b200 {
 enum KernelId : int {
     kKAllocate = 0,        // allocate-only walk
     kKUpdateStage = 1,     // count-and-stage walk (fused with allocation in integrate)
-    kKUpdateCrossing = 2,  // ordered cap selection for deferred blocks
+    kKUpdateApplyBig = 2,  // tile read-modify-write of blocks above 2048 records
     kKUpdateBin = 3,       // copy staged segments into contiguous per-block bins
-    kKUpdateApply = 4,     // tile read-modify-write (blocks up to 2048 records, then big blocks)
+    kKUpdateApply = 4,     // tile read-modify-write (blocks up to 2048 records)
     kKExtract = 5,
     kKReset = 6,
     kNumKernelIds = 7,
@@ -30,13 +30,11 @@ struct UpdateControl {
     int32_t work;        // apply-kernel work cursor
     int32_t n_accepted;  // blocks that accepted at least one contribution
     int32_t n_crossing;  // blocks that needed ordered cap selection
-    int32_t work2;       // crossing-kernel work cursor
     int32_t cta_done;    // stage-kernel CTAs finished (the last one scans)
     int32_t n_segs;      // segment descriptors published
-    int32_t n_deferred;  // blocks handed to the crossing kernel
     int32_t n_big;       // blocks handed to the big-block apply
-    int32_t work3;       // big-block apply work cursor
-    int32_t pad[5];
+    int32_t work_big;    // big-block apply work cursor
+    int32_t pad[7];
 };
 
 // One binned contribution: 16 bytes, written and read as one vector.
@@ -53,7 +51,6 @@ struct UpdateScratch {
     int32_t* blk_cur = nullptr;     // [pool] bin filling cursor; back to 0 after every update
     int4* blk_info = nullptr;       // [pool] (bin offset, records, -, -)
     int32_t* touched = nullptr;     // [pool] touched block indices
-    int32_t* cross_list = nullptr;  // [pool] blocks deferred to ordered selection
     int32_t* big_list = nullptr;    // [pool] blocks with more records than a small CTA takes
     UpdateControl* ctl = nullptr;
     Record* records = nullptr;      // staged records, grouped per (walk CTA, block)
@@ -114,7 +111,6 @@ private:
     UpdateScratch us_{};
     int sm_count_ = 148;
     int apply_ctas_per_sm_ = 2;
-    int cross_ctas_per_sm_ = 2;
 
     // Extraction scratch (device output for the host-copy path, counters).
     float* mesh_posnor_ = nullptr;
@@ -146,14 +142,12 @@ cudaError_t launch_reset_voxels(const DevVolume& v, int32_t n_blocks, cudaStream
 cudaError_t launch_extract(const DevVolume& v, int32_t n_blocks, float min_w, float iso,
                            float* posnor, uint8_t* rgb, int32_t cap, int32_t* ctl, cudaStream_t s);
 
-// The update pipeline: stage (+ per-block bins) -> bin -> apply -> crossing.
+// The update pipeline: stage (+ per-block bins) -> bin -> apply -> big-block apply.
 cudaError_t launch_update_stage(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
                                 bool insert, cudaStream_t s);
 cudaError_t launch_update_bin(const UpdateScratch& u, int n_ctas, cudaStream_t s);
 cudaError_t launch_update_apply(const DevVolume& v, const UpdateScratch& u, int n_ctas,
                                 cudaStream_t s);
-cudaError_t launch_update_crossing(const DevVolume& v, const UpdateScratch& u, int n_ctas,
-                                   cudaStream_t s);
 cudaError_t launch_update_apply_big(const DevVolume& v, const UpdateScratch& u, int n_ctas,
                                     cudaStream_t s);
 // One-time kernel attributes (dynamic shared memory of apply and crossing).

@@ -17,7 +17,7 @@ import numpy as np
 
 from . import _lib
 
-KERNEL_NAMES = ["allocate", "update_stage", "update_crossing", "update_bin", "update_apply",
+KERNEL_NAMES = ["allocate", "update_stage", "update_apply_big", "update_bin", "update_apply",
                 "extract", "reset"]
 
 
