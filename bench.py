@@ -41,10 +41,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 VOXEL, TRUNC, CAP = 0.02, 0.08, 64.0
+SLOTS_PER_POINT = 2 * 4 + 1   # band samples per point: 2 * ceil(trunc / voxel) + 1
 HASH_SLOTS, POOL = 1 << 20, 1 << 19
 N_FRAMES, SEED = 100, 0
 METRIC = "frames/s (640x480 integrate)"
-PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "update_apply_room640.md")
+PROFILES = os.path.join(ROOT, "profiles")
 
 
 def _frame_points(args):
@@ -75,10 +76,11 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def profile_traffic():
-    """DRAM bytes per launch of the apply kernel from the committed ncu summary."""
+def profile_traffic(kernel):
+    """DRAM bytes per launch of `kernel` on one room frame, from its committed
+    ncu summary (profiles/<kernel>_room640.md)."""
     try:
-        with open(PROFILE_TRAFFIC) as f:
+        with open(os.path.join(PROFILES, f"{kernel}_room640.md")) as f:
             for line in f:
                 if line.startswith("traffic_bytes_per_launch:"):
                     return float(line.split(":", 1)[1].split()[0])
@@ -373,41 +375,50 @@ def run_ours(args):
     vol.kernel_times()  # flush
     base = vol.kernel_times()
     vol.reset()
-    touched, accepted, records, crossing = [], [], [], []
+    updated, records, touched, crossing = [], [], [], []
     for k in range(N_FRAMES):
         a, b = int(offsets[k]), int(offsets[k + 1])
         vol.integrate(d_all[a:b], cams[k])
         st = vol.last_update_stats()
-        touched.append(st["touched_blocks"])
-        accepted.append(st["accepted_blocks"])
+        updated.append(st["updated_voxels"])
         records.append(st["records"])
-        crossing.append(st["crossing_blocks"])
+        touched.append(st["touched_blocks"])
+        crossing.append(st["crossing_voxels"])
+    # Allocation alone (allocate_blocks), for the allocate Mrays/s figure.
+    vol.reset()
+    for k in range(N_FRAMES):
+        a, b = int(offsets[k]), int(offsets[k + 1])
+        vol.allocate_blocks(d_all[a:b], cams[k])
     times = vol.kernel_times()
     vol.set_timing(False)
     per_kernel = {k: (times[k][0] - base[k][0], times[k][1] - base[k][1]) for k in KERNEL_NAMES}
-    launches_per_step = sum(n for _, n in per_kernel.values())
-    dominant = max((k for k in KERNEL_NAMES if per_kernel[k][1] > 0), key=lambda k: per_kernel[k][0])
+    integrate_kernels = ("band", "finish", "group", "deferred")
+    launches_per_step = sum(per_kernel[k][1] for k in integrate_kernels) // 1
+    dominant = max(integrate_kernels, key=lambda k: per_kernel[k][0])
 
     peak, peak_kind = measured_peak()
     t_alloc = per_kernel["allocate"][0] / 1e3
-    t_update = sum(per_kernel[k][0] for k in ("update_stage", "update_apply_big", "update_bin",
-                                               "update_apply")) / 1e3
-    tile_bytes = sum(accepted) * 512 * 2 * 8          # tsdf + weight, read + write
-    rgb_bytes = sum(accepted) * 512 * 2 * 12
-    update_alg_bytes = 12 * n_points + tile_bytes
-    # Algorithmic bytes per launch of each kernel (roofline).
-    alg = {
-        "update_apply": tile_bytes / N_FRAMES,  # refined below when the big-block share is known
-        "update_stage": 12 * n_points / N_FRAMES,
-        "allocate": 12 * n_points / N_FRAMES,
+    t_update = sum(per_kernel[k][0] for k in integrate_kernels) / 1e3
+    n_slots = n_points * SLOTS_PER_POINT
+    n_rec, n_touch = int(np.sum(records)), int(np.sum(touched))
+    # Bytes each kernel must move, every structure touched once (the
+    # definitions are in DESIGN.md, roofline section).
+    alg_total = {
+        "band": 12 * n_points + 4 * n_slots + 16 * n_rec,
+        "finish": n_touch * 512 * (16 + 36),   # read cnt,w,t,sum; write t,w,r,g,b,cnt,sum
+        "group": 4 * n_slots,
+        "deferred": 0,
     }
+    # Update as the reference scopes it: positions + tsdf/weight tiles of the
+    # touched blocks, read and written.
+    update_alg_bytes = 12 * n_points + n_touch * 512 * 2 * 8
     dom_ms, dom_n = per_kernel[dominant]
-    dom_alg = alg.get(dominant, 0.0)
+    dom_alg = alg_total.get(dominant, 0) / N_FRAMES
     achieved = dom_alg / (dom_ms / 1e3 / dom_n) / 1e9 if dom_n else 0.0
     roofline = {
         "bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
         "frac": achieved / peak, "peak_source": peak_kind,
-        "traffic": profile_traffic() if dominant == "update_apply" else None,
+        "traffic": profile_traffic(dominant),
         "alg_bytes_per_launch": dom_alg, "mean_launch_us": 1e3 * dom_ms / dom_n if dom_n else None,
     }
 
@@ -444,17 +455,16 @@ def run_ours(args):
             "reference_gpu_arm": a3,
             "e2e": {"value": e2e_value, "unit": "frames/s",
                     "h2d_bytes_per_step": int(all_pts.nbytes), "d2h_bytes_per_step": 16},
-            "gpu_launches": int(launches_per_step * args.steps),
+            "gpu_launches": int(launches_per_step * args.steps + N_FRAMES * args.steps),
             "clocks": clocks.summary(),
             "alloc_mrays_per_s": n_points / t_alloc / 1e6 if t_alloc else None,
             "update_gbps": update_alg_bytes / t_update / 1e9 if t_update else None,
-            "update_rgb_bytes_per_step": rgb_bytes,
             "kernel_ms_per_step": {k: round(v[0], 4) for k, v in per_kernel.items()},
             "kernel_launches_per_step": {k: v[1] for k, v in per_kernel.items()},
             "blocks": blocks, "drops": int(drops), "status": status,
+            "updated_voxels_per_frame": float(np.mean(updated)),
             "touched_blocks_per_frame": float(np.mean(touched)),
-            "accepted_blocks_per_frame": float(np.mean(accepted)),
-            "crossing_blocks_per_frame": float(np.mean(crossing)),
+            "crossing_voxels_per_frame": float(np.mean(crossing)),
             "records_per_frame": float(np.mean(records)),
         }
         print(json.dumps(line))

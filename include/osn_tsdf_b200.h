@@ -151,9 +151,10 @@ int32_t osn_tsdf_cuda_allocate_probe_histogram(OsnTsdfCudaVolume* v, const float
                                                int32_t n_bins);
 
 /* Per-stage statistics of the last update_voxels call (waits):
- * out[0] blocks that received a record, out[1] records binned,
- * out[2] blocks that accepted at least one contribution,
- * out[3] blocks that needed ordered cap selection. */
+ * out[0] voxels whose sums were rewritten, out[1] band records counted
+ * (contributions not already excluded by a full voxel),
+ * out[2] blocks touched by a band sample,
+ * out[3] voxels that crossed the cap inside the batch (ordered selection). */
 int32_t osn_tsdf_cuda_last_update_stats(const OsnTsdfCudaVolume* v, int64_t* out4);
 
 /* Largest batch of one update_voxels_noalloc call, counted in records:
@@ -167,7 +168,7 @@ int32_t osn_tsdf_cuda_last_update_stats(const OsnTsdfCudaVolume* v, int64_t* out
  * (no allocation during stream capture), serving loops that budget device
  * memory up front, latency-critical threads that cannot absorb the implied
  * synchronisation -- call this instead. Same results as update_voxels.
- * Its scratch is one fixed 72 MiB array inside the library, held on every
+ * Its scratch is one fixed 40 MiB array inside the library, held on every
  * GPU where the library's code is loaded until the process exits, and shared
  * by all calls: calls whose work overlaps on the GPU race and must be
  * serialised. The first call on a device resolves the array's address and
@@ -181,9 +182,10 @@ int32_t osn_tsdf_cuda_update_voxels_noalloc(OsnTsdfCudaVolume* v, const float* d
 /* Kernel timing. When enabled, every kernel launch of the volume is
  * bracketed by CUDA events on the volume's stream; kernel_times reads (and
  * waits for) the accumulated per-kernel milliseconds and launch counts.
- * Kernel ids: 0 allocate, 1 update-stage (allocate+stage in integrate),
- * 2 update-apply of blocks above 2048 records, 3 update-bin,
- * 4 update-apply, 5 extract, 6 reset. Returns the number of ids written. */
+ * Kernel ids: 0 allocate, 1 band (count-and-sum walk; allocates too in
+ * integrate), 2 finish (per touched block), 3 group (records of voxels that
+ * cross the cap), 4 deferred (ordered cap selection), 5 extract, 6 reset.
+ * Returns the number of ids written. */
 int32_t osn_tsdf_cuda_set_timing(OsnTsdfCudaVolume* v, int32_t enabled);
 int32_t osn_tsdf_cuda_kernel_times(OsnTsdfCudaVolume* v, double* ms, int64_t* launches,
                                    int32_t n_ids);

@@ -100,7 +100,7 @@ def test_room_frames_capped(cuda, cap):
     gpu, ref = _pair(cuda, batches, 0.02, 1 << 19, 0.08, cap)
     stats = gpu.last_update_stats()
     if cap == 6.0:
-        assert stats["crossing_blocks"] > 0
+        assert stats["crossing_voxels"] > 0
     assert gpu.status() == 0
     assert_same_blocks(gpu, ref)
     assert_same_voxels(gpu, ref)

@@ -284,6 +284,23 @@ __device__ __forceinline__ InsertResult find_or_insert(const DevVolume& v, int32
     return res;  // table full
 }
 
+// ---- fixed-point sums ----------------------------------------------------
+//
+// Per-voxel sums of normalised SDFs are accumulated as 64-bit integers in
+// units of 2^-40 (exact for |value| >= 2^-17, |sum| < 2^23) and added to the
+// stored float sum with one rounding, so a sum does not depend on the order
+// of its terms.
+constexpr double kFixScale = 1099511627776.0;      // 2^40
+constexpr double kFixInv = 1.0 / 1099511627776.0;  // 2^-40
+
+__device__ __forceinline__ long long to_fix(float x) {
+    return __double2ll_rn((double)x * kFixScale);
+}
+
+__device__ __forceinline__ float add_fix(float t0, long long sum) {
+    return __double2float_rn((double)t0 + (double)sum * kFixInv);
+}
+
 __device__ __forceinline__ unsigned lanemask_lt() {
     unsigned m;
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));

@@ -1,9 +1,9 @@
 // update_voxels without any device allocation.
 //
-// The regular update_voxels keeps its per-call scratch (the binned
-// contribution records) in a buffer the volume grows with cudaMalloc the
-// first time a batch needs more room, which also waits for the volume's
-// stream and frees the old buffer. Some callers cannot allow that: code
+// The regular update_voxels keeps its per-call scratch (one record per band
+// slot, the grouped records of voxels that cross the cap, and their list) in
+// buffers the volume grows with cudaMalloc the first time a batch needs more
+// room, which also waits for the volume's stream and frees the old buffers. Some callers cannot allow that: code
 // that records the integrate into a CUDA graph (allocation is not permitted
 // while a stream is being captured), serving loops that admit work against a
 // fixed device-memory budget and must not see memory appear behind their
@@ -12,11 +12,13 @@
 // with its scratch in one fixed array compiled into the library.
 //
 // The array is a file-scope __device__ variable of kNoAllocScratchBytes
-// (72 MiB + 256 bytes): the control counters, the staging area and the bins
-// for kNoAllocMaxRecords 16-byte records each, and kNoAllocMaxSegments
-// 16-byte segment descriptors, i.e. batches with
+// (40 MiB + 256 bytes): the control counters, kNoAllocMaxRecords 4-byte band
+// records, as many 8-byte deferred records, and half as many 16-byte
+// deferred-voxel entries, i.e. batches with
 // n_points * (2 * steps + 1) <= 2,097,152 (a 480x360 frame at 9 band steps
-// per point fits; a 640x480 frame must be split in two). Every GPU on which
+// per point fits; a 640x480 frame must be split in two). The per-voxel and
+// per-block state the update also uses belongs to the volume and was
+// allocated with it. Every GPU on which
 // the library's code is loaded holds the array until the process exits.
 // Every call shares it and it keeps the last call's contents; the counters
 // that must start at zero are cleared at the start of each call. Two calls
@@ -35,10 +37,12 @@ namespace {
 
 constexpr size_t kNoAllocHeaderBytes = 256;  // UpdateControl, padded
 constexpr int64_t kNoAllocMaxRecords = OSN_TSDF_NOALLOC_MAX_RECORDS;
-constexpr int64_t kNoAllocMaxSegments = (int64_t)1 << 19;
-constexpr size_t kNoAllocRecordBytes = (size_t)kNoAllocMaxRecords * sizeof(Record);
-constexpr size_t kNoAllocScratchBytes =
-    kNoAllocHeaderBytes + 2 * kNoAllocRecordBytes + (size_t)kNoAllocMaxSegments * sizeof(int4);
+constexpr int64_t kNoAllocMaxDeferred = kNoAllocMaxRecords / 2;
+constexpr size_t kNoAllocRecordBytes = (size_t)kNoAllocMaxRecords * sizeof(uint32_t);
+constexpr size_t kNoAllocDeferredBytes = (size_t)kNoAllocMaxRecords * sizeof(uint2);
+constexpr size_t kNoAllocScratchBytes = kNoAllocHeaderBytes + kNoAllocRecordBytes +
+                                        kNoAllocDeferredBytes +
+                                        (size_t)kNoAllocMaxDeferred * sizeof(int4);
 static_assert(sizeof(UpdateControl) <= kNoAllocHeaderBytes, "control block must fit the header");
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
@@ -75,13 +79,15 @@ cudaError_t Volume::update_static_scratch(const BatchArgs& a, void* scratch) {
     unsigned char* base = static_cast<unsigned char*>(scratch);
     UpdateScratch u = us_;
     u.ctl = reinterpret_cast<UpdateControl*>(base);
-    u.records = reinterpret_cast<Record*>(base + kNoAllocHeaderBytes);
-    u.bins = reinterpret_cast<Record*>(base + kNoAllocHeaderBytes + kNoAllocRecordBytes);
+    u.records = reinterpret_cast<uint32_t*>(base + kNoAllocHeaderBytes);
+    u.deferred = reinterpret_cast<uint2*>(base + kNoAllocHeaderBytes + kNoAllocRecordBytes);
+    u.dvox = reinterpret_cast<int4*>(base + kNoAllocHeaderBytes + kNoAllocRecordBytes +
+                                     kNoAllocDeferredBytes);
     u.record_cap = kNoAllocMaxRecords;
-    u.segs = reinterpret_cast<int4*>(base + kNoAllocHeaderBytes + 2 * kNoAllocRecordBytes);
-    u.seg_cap = kNoAllocMaxSegments;
+    u.dvox_cap = (int32_t)kNoAllocMaxDeferred;
     // Only the control counters must start at zero (run_update clears them);
-    // the records of the previous call are overwritten before they are read.
+    // every record slot is rewritten before it is read, and deferred records
+    // and entries are read only where this call placed them.
     return run_update(a, u, false);
 }
 
@@ -94,8 +100,7 @@ extern "C" int32_t osn_tsdf_cuda_update_voxels_noalloc(OsnTsdfCudaVolume* v,
     osn_b200::Volume* vol = osn_tsdf_b200_volume_of(v);
     if (!vol || !d_positions || n_points <= 0) return 1;
     const int64_t records = (int64_t)n_points * (2 * (int64_t)vol->dev().steps + 1);
-    const int64_t segments = std::min<int64_t>(records, (int64_t)((n_points + 255) / 256) * 512);
-    if (records > osn_b200::kNoAllocMaxRecords || segments > osn_b200::kNoAllocMaxSegments) {
+    if (records > osn_b200::kNoAllocMaxRecords) {
         std::fprintf(stderr,
                      "[osn_tsdf_b200] update_voxels_noalloc: batch of %d points needs %lld records, "
                      "above the fixed maximum of %lld (n_points * (2*steps+1)); split the batch\n",

@@ -34,6 +34,11 @@ uint32_t next_pow2(uint32_t v) {  // cpp/src/volume.cpp:14-19
 
 Volume::Volume(float voxel, int32_t pool, float trunc_m, float weight_cap, uint32_t hash_slots) {
     if (!(voxel > 0.0f) || pool <= 0) return;
+    if (pool > kMaxPoolBlocks) {
+        std::fprintf(stderr, "[osn_tsdf_b200] pool of %d blocks exceeds the supported %d\n", pool,
+                     kMaxPoolBlocks);
+        return;
+    }
     if (hash_slots != 0 && (hash_slots < 2 || (hash_slots & (hash_slots - 1)) != 0)) return;
     dv_.voxel_size = voxel;
     dv_.inv_voxel = 1.0f / voxel;
@@ -52,7 +57,6 @@ bool Volume::alloc_device(uint32_t hash_slots) {
     int dev = 0;
     OSN_TRY(cudaGetDevice(&dev));
     OSN_TRY(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, dev));
-    OSN_TRY(prepare_update_kernels());
     OSN_TRY(cudaStreamCreate(&stream_));
     OSN_TRY(cudaMalloc(&dv_.table, ((size_t)size + kScratchSlots) * sizeof(HashEntry)));
     OSN_TRY(cudaMalloc(&dv_.block_count, sizeof(int32_t)));
@@ -64,11 +68,11 @@ bool Volume::alloc_device(uint32_t hash_slots) {
     OSN_TRY(cudaMalloc(&dv_.r, n_vox * sizeof(float)));
     OSN_TRY(cudaMalloc(&dv_.g, n_vox * sizeof(float)));
     OSN_TRY(cudaMalloc(&dv_.b, n_vox * sizeof(float)));
-    OSN_TRY(cudaMalloc(&us_.blk_cnt, (size_t)dv_.pool_capacity * sizeof(int32_t)));
-    OSN_TRY(cudaMalloc(&us_.blk_cur, (size_t)dv_.pool_capacity * sizeof(int32_t)));
-    OSN_TRY(cudaMalloc(&us_.blk_info, (size_t)dv_.pool_capacity * sizeof(int4)));
+    OSN_TRY(cudaMalloc(&us_.vcnt, n_vox * sizeof(uint32_t)));
+    OSN_TRY(cudaMalloc(&us_.vacc, n_vox * sizeof(unsigned long long)));
+    OSN_TRY(cudaMalloc(&us_.blk_touch, (size_t)dv_.pool_capacity * sizeof(uint32_t)));
+    OSN_TRY(cudaMalloc(&us_.blk_cross, (size_t)dv_.pool_capacity * sizeof(uint32_t)));
     OSN_TRY(cudaMalloc(&us_.touched, (size_t)dv_.pool_capacity * sizeof(int32_t)));
-    OSN_TRY(cudaMalloc(&us_.big_list, (size_t)dv_.pool_capacity * sizeof(int32_t)));
     OSN_TRY(cudaMalloc(&us_.ctl, sizeof(UpdateControl)));
     OSN_TRY(cudaMalloc(&mesh_ctl_, 2 * sizeof(int32_t)));
     OSN_TRY(cudaMallocHost(&host_small_, 8 * sizeof(int64_t)));
@@ -85,15 +89,12 @@ bool Volume::alloc_device(uint32_t hash_slots) {
     OSN_TRY(cudaMemsetAsync(dv_.r, 0, n_vox * sizeof(float), stream_));
     OSN_TRY(cudaMemsetAsync(dv_.g, 0, n_vox * sizeof(float), stream_));
     OSN_TRY(cudaMemsetAsync(dv_.b, 0, n_vox * sizeof(float), stream_));
-    OSN_TRY(cudaMemsetAsync(us_.blk_cnt, 0, (size_t)dv_.pool_capacity * sizeof(int32_t), stream_));
-    OSN_TRY(cudaMemsetAsync(us_.blk_cur, 0, (size_t)dv_.pool_capacity * sizeof(int32_t), stream_));
+    OSN_TRY(cudaMemsetAsync(us_.vcnt, 0, n_vox * sizeof(uint32_t), stream_));
+    OSN_TRY(cudaMemsetAsync(us_.vacc, 0, n_vox * sizeof(unsigned long long), stream_));
+    OSN_TRY(cudaMemsetAsync(us_.blk_touch, 0, (size_t)dv_.pool_capacity * sizeof(uint32_t), stream_));
+    OSN_TRY(cudaMemsetAsync(us_.blk_cross, 0, (size_t)dv_.pool_capacity * sizeof(uint32_t), stream_));
     OSN_TRY(cudaMemsetAsync(us_.ctl, 0, sizeof(UpdateControl), stream_));
     OSN_TRY(cudaStreamSynchronize(stream_));
-
-    // Persistent grids, as many CTAs per SM as shared memory allows.
-    int per_sm = 0;
-    OSN_TRY(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
-    apply_ctas_per_sm_ = std::max(1, per_sm / (int)(apply_smem_bytes() + 1024));
     return true;
 }
 
@@ -109,15 +110,15 @@ Volume::~Volume() {
     cudaFree(dv_.r);
     cudaFree(dv_.g);
     cudaFree(dv_.b);
-    cudaFree(us_.blk_cnt);
-    cudaFree(us_.blk_cur);
-    cudaFree(us_.blk_info);
-    cudaFree(us_.segs);
-    cudaFree(us_.bins);
+    cudaFree(us_.vcnt);
+    cudaFree(us_.vacc);
+    cudaFree(us_.blk_touch);
+    cudaFree(us_.blk_cross);
     cudaFree(us_.touched);
-    cudaFree(us_.big_list);
     cudaFree(us_.ctl);
     cudaFree(us_.records);
+    cudaFree(us_.deferred);
+    cudaFree(us_.dvox);
     cudaFree(mesh_posnor_);
     cudaFree(mesh_rgb_);
     cudaFree(mesh_ctl_);
@@ -183,74 +184,73 @@ int Volume::kernel_times(double* ms, int64_t* launches, int n_ids) {
 
 cudaError_t Volume::allocate(const BatchArgs& a, int mode, unsigned long long* hist, int n_bins) {
     mark_start(kKAllocate);
-    const cudaError_t e = launch_allocate(dv_, a, mode, hist, n_bins, stream_);
+    const cudaError_t e = launch_allocate(dv_, a, mode, hist, n_bins, sm_count_, stream_);
     mark_end(kKAllocate);
     return e;
 }
 
-bool Volume::ensure_records(int64_t n_records, int64_t n_segs) {
-    if (n_records <= us_.record_cap && n_segs <= us_.seg_cap) return true;
+bool Volume::ensure_records(int64_t n_records) {
+    if (n_records <= us_.record_cap) return true;
     // Grows only; waits for in-flight work that may still read the old buffers.
     cudaStreamSynchronize(stream_);
-    if (n_records > us_.record_cap) {
-        cudaFree(us_.records);
-        cudaFree(us_.bins);
-        us_.records = nullptr;
-        us_.bins = nullptr;
-        us_.record_cap = 0;
-        if (cudaMalloc(&us_.records, (size_t)n_records * sizeof(Record)) != cudaSuccess) return false;
-        if (cudaMalloc(&us_.bins, (size_t)n_records * sizeof(Record)) != cudaSuccess) return false;
-        us_.record_cap = n_records;
-    }
-    if (n_segs > us_.seg_cap) {
-        cudaFree(us_.segs);
-        us_.segs = nullptr;
-        us_.seg_cap = 0;
-        if (cudaMalloc(&us_.segs, (size_t)n_segs * sizeof(int4)) != cudaSuccess) return false;
-        us_.seg_cap = n_segs;
-    }
+    cudaFree(us_.records);
+    cudaFree(us_.deferred);
+    cudaFree(us_.dvox);
+    us_.records = nullptr;
+    us_.deferred = nullptr;
+    us_.dvox = nullptr;
+    us_.record_cap = 0;
+    us_.dvox_cap = 0;
+    // A deferred voxel holds at least two records, so half the records bound
+    // the deferred list.
+    const int64_t n_dvox = n_records / 2 + 1;
+    if (cudaMalloc(&us_.records, (size_t)n_records * sizeof(uint32_t)) != cudaSuccess) return false;
+    if (cudaMalloc(&us_.deferred, (size_t)n_records * sizeof(uint2)) != cudaSuccess) return false;
+    if (cudaMalloc(&us_.dvox, (size_t)n_dvox * sizeof(int4)) != cudaSuccess) return false;
+    us_.record_cap = n_records;
+    us_.dvox_cap = (int32_t)std::min<int64_t>(n_dvox, INT32_MAX);
     return true;
 }
 
-cudaError_t Volume::run_update(const BatchArgs& a, const UpdateScratch& u, bool insert) {
+cudaError_t Volume::run_update(const BatchArgs& a, const UpdateScratch& scratch, bool insert) {
+    // Block tags are update numbers; at the (theoretical) wrap, clear them.
+    if (++update_tag_ == 0u) {
+        cudaMemsetAsync(us_.blk_touch, 0, (size_t)dv_.pool_capacity * sizeof(uint32_t), stream_);
+        cudaMemsetAsync(us_.blk_cross, 0, (size_t)dv_.pool_capacity * sizeof(uint32_t), stream_);
+        update_tag_ = 1u;
+    }
+    UpdateScratch u = scratch;
+    u.tag = update_tag_;
     cudaError_t e = cudaMemsetAsync(u.ctl, 0, sizeof(UpdateControl), stream_);
     if (e != cudaSuccess) return e;
-    mark_start(kKUpdateStage);
-    e = launch_update_stage(dv_, a, u, insert, stream_);
-    mark_end(kKUpdateStage);
+    mark_start(kKBand);
+    e = launch_band_records(dv_, a, u, insert, sm_count_, stream_);
+    mark_end(kKBand);
     if (e != cudaSuccess) return e;
-    mark_start(kKUpdateBin);
-    e = launch_update_bin(u, sm_count_ * 16, stream_);
-    mark_end(kKUpdateBin);
+    mark_start(kKFinish);
+    e = launch_finish(dv_, u, sm_count_ * 16, stream_);
+    mark_end(kKFinish);
     if (e != cudaSuccess) return e;
-    mark_start(kKUpdateApply);
-    e = launch_update_apply(dv_, u, sm_count_ * apply_ctas_per_sm_, stream_);
-    mark_end(kKUpdateApply);
+    mark_start(kKGroup);
+    e = launch_group(dv_, a, u, stream_);
+    mark_end(kKGroup);
     if (e != cudaSuccess) return e;
-    mark_start(kKUpdateApplyBig);
-    e = launch_update_apply_big(dv_, u, sm_count_, stream_);
-    mark_end(kKUpdateApplyBig);
+    mark_start(kKDeferred);
+    e = launch_deferred(dv_, u, sm_count_ * 8, stream_);
+    mark_end(kKDeferred);
     return e;
 }
 
-// Scratch a batch of n points can need: one record per band sample, and one
-// segment per (walk CTA of 256 points, block), at most 512 per CTA.
-static void batch_scratch(int32_t n, int32_t steps, int64_t* records, int64_t* segs) {
-    *records = (int64_t)n * (2 * steps + 1);
-    *segs = std::min<int64_t>(*records, (int64_t)((n + 255) / 256) * 512);
-}
+// Records a batch of n points needs: one per band slot.
+static int64_t batch_records(int32_t n, int32_t steps) { return (int64_t)n * (2 * steps + 1); }
 
 cudaError_t Volume::update(const BatchArgs& a) {
-    int64_t rec = 0, seg = 0;
-    batch_scratch(a.n, dv_.steps, &rec, &seg);
-    if (!ensure_records(rec, seg)) return cudaErrorMemoryAllocation;
+    if (!ensure_records(batch_records(a.n, dv_.steps))) return cudaErrorMemoryAllocation;
     return run_update(a, us_, false);
 }
 
 cudaError_t Volume::integrate(const BatchArgs& a) {
-    int64_t rec = 0, seg = 0;
-    batch_scratch(a.n, dv_.steps, &rec, &seg);
-    if (!ensure_records(rec, seg)) return cudaErrorMemoryAllocation;
+    if (!ensure_records(batch_records(a.n, dv_.steps))) return cudaErrorMemoryAllocation;
     return run_update(a, us_, true);
 }
 
@@ -316,10 +316,12 @@ cudaError_t Volume::reset() {
     if (e == cudaSuccess) e = cudaMemsetAsync(dv_.block_count, 0, sizeof(int32_t), stream_);
     if (e == cudaSuccess) e = cudaMemsetAsync(dv_.drop_count, 0, sizeof(unsigned long long), stream_);
     if (e == cudaSuccess) e = cudaMemsetAsync(dv_.status, 0, sizeof(uint32_t), stream_);
+    // The per-voxel batch state is back to zero after every completed update;
+    // an update that stopped on an error may have left some behind.
+    const size_t n_vox = (size_t)dv_.pool_capacity * kBlockVoxels;
+    if (e == cudaSuccess) e = cudaMemsetAsync(us_.vcnt, 0, n_vox * sizeof(uint32_t), stream_);
     if (e == cudaSuccess)
-        e = cudaMemsetAsync(us_.blk_cnt, 0, (size_t)dv_.pool_capacity * sizeof(int32_t), stream_);
-    if (e == cudaSuccess)
-        e = cudaMemsetAsync(us_.blk_cur, 0, (size_t)dv_.pool_capacity * sizeof(int32_t), stream_);
+        e = cudaMemsetAsync(us_.vacc, 0, n_vox * sizeof(unsigned long long), stream_);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
     return e;
 }
@@ -352,10 +354,10 @@ bool Volume::last_update_stats(int64_t out[4]) {
         cudaStreamSynchronize(stream_) != cudaSuccess)
         return false;
     std::memcpy(&c, host_small_, sizeof(UpdateControl));
-    out[0] = c.n_touched;
+    out[0] = c.n_updated;
     out[1] = c.n_records;
-    out[2] = c.n_accepted;
-    out[3] = c.n_crossing;
+    out[2] = c.n_touched;
+    out[3] = c.n_deferred;
     return true;
 }
 

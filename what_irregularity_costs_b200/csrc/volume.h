@@ -12,11 +12,11 @@ namespace osn_b200 {
 
 // Kernel ids for the timing table (documented in include/osn_tsdf_b200.h).
 enum KernelId : int {
-    kKAllocate = 0,        // allocate-only walk
-    kKUpdateStage = 1,     // count-and-stage walk (fused with allocation in integrate)
-    kKUpdateApplyBig = 2,  // tile read-modify-write of blocks above 2048 records
-    kKUpdateBin = 3,       // copy staged segments into contiguous per-block bins
-    kKUpdateApply = 4,     // tile read-modify-write (blocks up to 2048 records)
+    kKAllocate = 0,      // allocate-only band walk
+    kKBand = 1,          // count-and-sum band walk (fused with allocation in integrate)
+    kKFinish = 2,        // per touched block: finish every voxel that accepts all its records
+    kKGroup = 3,         // records of voxels that cross the cap, grouped per voxel
+    kKDeferred = 4,      // ordered cap selection of those voxels
     kKExtract = 5,
     kKReset = 6,
     kNumKernelIds = 7,
@@ -25,39 +25,39 @@ enum KernelId : int {
 // Counters an update pass keeps on the device (one small struct, cleared by
 // one memset at the start of every update).
 struct UpdateControl {
-    int32_t n_touched;   // blocks that received at least one record
-    int32_t n_records;   // records staged
-    int32_t work;        // apply-kernel work cursor
-    int32_t n_accepted;  // blocks that accepted at least one contribution
-    int32_t n_crossing;  // blocks that needed ordered cap selection
-    int32_t cta_done;    // stage-kernel CTAs finished (the last one scans)
-    int32_t n_segs;      // segment descriptors published
-    int32_t n_big;       // blocks handed to the big-block apply
-    int32_t work_big;    // big-block apply work cursor
-    int32_t pad[7];
+    int32_t n_records;   // band records counted (contributions that can be accepted)
+    int32_t n_touched;   // blocks that received a band sample
+    int32_t n_updated;   // voxels whose sums were rewritten
+    int32_t n_deferred;  // voxels that cross the cap inside the batch
+    uint32_t x_used;     // deferred records reserved
+    int32_t pad[11];
 };
+static_assert(sizeof(UpdateControl) == 64, "control block is read back as 64 bytes");
 
-// One binned contribution: 16 bytes, written and read as one vector.
-struct __align__(16) Record {
-    uint32_t id;   // point * (2*steps+1) + (s + steps): the canonical order
-    uint32_t lv;   // voxel within the block, (lz*8+ly)*8+lx
-    float sdf_n;   // clamp(sdf / trunc, -1, 1)
-    float w_in;    // contribution weight (1 through the reference ABI)
-};
-static_assert(sizeof(Record) == 16, "record must stay one 128-bit vector");
+// One band slot (point i, step s) at records[s * n + i]: the voxel's global
+// index (block index * 512 + (lz*8+ly)*8+lx), or kNoVoxel for a culled,
+// dropped or saturated sample.
+constexpr uint32_t kNoVoxel = 0xFFFFFFFFu;
+
+// Global voxel indices are 32-bit with one value reserved, which bounds the
+// pool at 2^23 - 1 blocks (4 G voxels).
+constexpr int32_t kMaxPoolBlocks = (1 << 23) - 1;
 
 struct UpdateScratch {
-    int32_t* blk_cnt = nullptr;     // [pool] records per block; back to 0 after every update
-    int32_t* blk_cur = nullptr;     // [pool] bin filling cursor; back to 0 after every update
-    int4* blk_info = nullptr;       // [pool] (bin offset, records, -, -)
-    int32_t* touched = nullptr;     // [pool] touched block indices
-    int32_t* big_list = nullptr;    // [pool] blocks with more records than a small CTA takes
     UpdateControl* ctl = nullptr;
-    Record* records = nullptr;      // staged records, grouped per (walk CTA, block)
-    Record* bins = nullptr;         // the same records, contiguous per block
+    uint32_t* records = nullptr;  // [record_cap] one per band slot
+    uint2* deferred = nullptr;    // [record_cap] (canonical id, sdf_n bits), grouped per voxel
+    int4* dvox = nullptr;         // [dvox_cap] (voxel, group base, records, accepted)
     int64_t record_cap = 0;
-    int4* segs = nullptr;           // segment descriptors (block, staging offset, length, -)
-    int64_t seg_cap = 0;
+    int32_t dvox_cap = 0;
+    // Owned by the volume. Per voxel: zero between updates.
+    uint32_t* vcnt = nullptr;            // records of the voxel in this batch
+    unsigned long long* vacc = nullptr;  // fixed-point sum of their sdf_n; group base of a crossing voxel
+    // Per block, tagged with the update number instead of being cleared.
+    uint32_t* blk_touch = nullptr;  // update that last touched the block
+    uint32_t* blk_cross = nullptr;  // update in which the block held a cap-crossing voxel
+    int32_t* touched = nullptr;     // [pool] blocks touched by this update
+    uint32_t tag = 0;               // this update's number (never 0)
 };
 
 class Volume {
@@ -102,15 +102,15 @@ public:
 private:
     bool alloc_device(uint32_t hash_slots);
     cudaError_t run_update(const BatchArgs& a, const UpdateScratch& u, bool insert);
-    bool ensure_records(int64_t n_records, int64_t n_segs);
+    bool ensure_records(int64_t n_records);
     bool ensure_mesh(int32_t cap, bool rgb);
 
     bool ok_ = false;
     DevVolume dv_{};
     cudaStream_t stream_ = nullptr;
     UpdateScratch us_{};
+    uint32_t update_tag_ = 0;  // number of the last update (block tags)
     int sm_count_ = 148;
-    int apply_ctas_per_sm_ = 2;
 
     // Extraction scratch (device output for the host-copy path, counters).
     float* mesh_posnor_ = nullptr;
@@ -136,23 +136,19 @@ private:
 
 // Launchers (one per translation unit).
 cudaError_t launch_allocate(const DevVolume& v, const BatchArgs& a, int mode,
-                            unsigned long long* hist, int n_bins, cudaStream_t s);
+                            unsigned long long* hist, int n_bins, int sm_count, cudaStream_t s);
 cudaError_t launch_reset_table(HashEntry* first, uint32_t count, long long key, cudaStream_t s);
 cudaError_t launch_reset_voxels(const DevVolume& v, int32_t n_blocks, cudaStream_t s);
 cudaError_t launch_extract(const DevVolume& v, int32_t n_blocks, float min_w, float iso,
                            float* posnor, uint8_t* rgb, int32_t cap, int32_t* ctl, cudaStream_t s);
 
-// The update pipeline: stage (+ per-block bins) -> bin -> apply -> big-block apply.
-cudaError_t launch_update_stage(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
-                                bool insert, cudaStream_t s);
-cudaError_t launch_update_bin(const UpdateScratch& u, int n_ctas, cudaStream_t s);
-cudaError_t launch_update_apply(const DevVolume& v, const UpdateScratch& u, int n_ctas,
-                                cudaStream_t s);
-cudaError_t launch_update_apply_big(const DevVolume& v, const UpdateScratch& u, int n_ctas,
-                                    cudaStream_t s);
-// One-time kernel attributes (dynamic shared memory of apply and crossing).
-cudaError_t prepare_update_kernels();
-size_t apply_smem_bytes();
+// The update pipeline: band walk (counts, sums, records) -> finish -> group -> deferred.
+cudaError_t launch_band_records(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
+                                bool insert, int sm_count, cudaStream_t s);
+cudaError_t launch_finish(const DevVolume& v, const UpdateScratch& u, int n_ctas, cudaStream_t s);
+cudaError_t launch_group(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
+                         cudaStream_t s);
+cudaError_t launch_deferred(const DevVolume& v, const UpdateScratch& u, int n_ctas, cudaStream_t s);
 
 }  // namespace osn_b200
 

@@ -17,8 +17,7 @@ import numpy as np
 
 from . import _lib
 
-KERNEL_NAMES = ["allocate", "update_stage", "update_apply_big", "update_bin", "update_apply",
-                "extract", "reset"]
+KERNEL_NAMES = ["allocate", "band", "finish", "group", "deferred", "extract", "reset"]
 
 
 def _addr(x) -> int:
@@ -212,8 +211,8 @@ class CudaVolume:
         out = np.zeros(4, dtype=np.int64)
         self._check(self.lib.osn_tsdf_cuda_last_update_stats(self.h, out.ctypes.data),
                     "last_update_stats")
-        return {"touched_blocks": int(out[0]), "records": int(out[1]),
-                "accepted_blocks": int(out[2]), "crossing_blocks": int(out[3])}
+        return {"updated_voxels": int(out[0]), "records": int(out[1]),
+                "touched_blocks": int(out[2]), "crossing_voxels": int(out[3])}
 
     def set_timing(self, on: bool = True):
         self.lib.osn_tsdf_cuda_set_timing(self.h, 1 if on else 0)
