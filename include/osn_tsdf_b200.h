@@ -168,7 +168,7 @@ int32_t osn_tsdf_cuda_last_update_stats(const OsnTsdfCudaVolume* v, int64_t* out
  * (no allocation during stream capture), serving loops that budget device
  * memory up front, latency-critical threads that cannot absorb the implied
  * synchronisation -- call this instead. Same results as update_voxels.
- * Its scratch is one fixed 40 MiB array inside the library, held on every
+ * Its scratch is one fixed 32 MiB array inside the library, held on every
  * GPU where the library's code is loaded until the process exits, and shared
  * by all calls: calls whose work overlaps on the GPU race and must be
  * serialised. The first call on a device resolves the array's address and

@@ -13,17 +13,20 @@
 // (their keys in a per-thread column of shared memory) and resolves each
 // once. The resolution is warp-cooperative: for each run index the warp's
 // lanes group equal block keys with __match_any_sync and only the lowest lane
-// of a group probes the global table (and inserts), then broadcasts the pool
-// index with a shuffle -- neighbouring pixels share blocks, so the table sees
-// a fraction of the per-sample probes and far fewer contending CAS attempts
-// on a new block.
+// of a group probes the global table (and inserts), leaving the pool index in
+// shared memory for the group -- neighbouring pixels share blocks, so the
+// table sees a fraction of the per-sample probes and far fewer contending CAS
+// attempts on a new block. The groups of all run indices are formed first and
+// each leader then resolves its runs with their home-slot probes in flight
+// together, so a chunk waits for about one table access, not one per run.
 //
 // Update tail. The group leader also tags the block as touched by this update
-// (one atomic exchange; the first tagger appends it to the touched list).
+// (one atomic exchange unless a cached read already shows the tag; the first
+// tagger appends it to the touched list).
 // Every band sample whose voxel can still accept a contribution adds one to
 // the voxel's batch count and its normalised SDF, in 2^-40 fixed point, to
-// the voxel's 64-bit sum: two fire-and-forget L2 reductions, whose order does
-// not matter. Every band slot (point i, step s) also gets a 4-byte record at
+// the voxel's 64-bit sum: fire-and-forget L2 reductions, whose order does not
+// matter, issued once per run of consecutive lanes that share the voxel. Every band slot (point i, step s) also gets a 4-byte record at
 // records[(s + steps) * n + i] -- step-major, so each store of a warp is one
 // contiguous 128-byte line -- holding the voxel's global index or kNoVoxel;
 // only voxels that cross the cap read them again (their canonical order is
@@ -49,8 +52,11 @@ constexpr int kRunShift = 9;
 constexpr uint32_t kValid = 1u << 30;
 
 template <int MODE>
-__device__ __forceinline__ int32_t resolve(const DevVolume& v, int bx, int by, int bz, long long key,
+__device__ __forceinline__ int32_t resolve(const DevVolume& v, long long key,
                                            unsigned long long* hist, int n_bins) {
+    const int bx = unpack_axis(key, 2 * kCoordBits);
+    const int by = unpack_axis(key, kCoordBits);
+    const int bz = unpack_axis(key, 0);
     if (MODE == kLookupOnly) return find_block(v, bx, by, bz, key);
     const InsertResult r = find_or_insert<MODE>(v, bx, by, bz, key);
     if (MODE == kAllocProbeHist && n_bins > 0)
@@ -58,23 +64,106 @@ __device__ __forceinline__ int32_t resolve(const DevVolume& v, int bx, int by, i
     return r.idx;
 }
 
+// Modes whose first probe may be answered from the block's home slot alone.
+template <int MODE>
+__device__ __forceinline__ constexpr bool has_fast_probe() {
+    return MODE == kAllocInsert || MODE == kLookupOnly;
+}
+
+// The block's home-slot entry, through L1. A slot goes empty -> claimed
+// (key, -1) -> published (key, index) and never changes again within an
+// update, so an entry that shows this key with a valid index is final, and
+// with no concurrent insertion (lookup) an empty home slot means absent.
+template <int MODE>
+__device__ __forceinline__ int4 home_entry(const DevVolume& v, long long key) {
+    if (!has_fast_probe<MODE>()) return make_int4(0, 0, -1, 0);
+    const uint32_t h = hash_slot(unpack_axis(key, 2 * kCoordBits), unpack_axis(key, kCoordBits),
+                                 unpack_axis(key, 0), v.hash_mask);
+    const int4* e = reinterpret_cast<const int4*>(&v.table[h]);
+    return MODE == kLookupOnly ? __ldg(e) : __ldca(e);
+}
+
+// The pool index the home entry settles, or -2 when the full probe is needed.
+template <int MODE>
+__device__ __forceinline__ int32_t settle_home(const DevVolume& v, int4 raw, long long key) {
+    if (!has_fast_probe<MODE>()) return -2;
+    const long long k0 = ((long long)(unsigned)raw.y << 32) | (unsigned)raw.x;
+    if (k0 == key && raw.z >= 0 && raw.z < v.pool_capacity) return raw.z;
+    if (MODE == kLookupOnly && k0 == kEmptyKey) return -1;
+    return -2;
+}
+
+// The full probe (and insertion) protocol, out of line: it is the rare path
+// of the fast-probe modes and keeps their walk loop in registers.
+template <int MODE>
+__device__ __noinline__ int32_t resolve_slow(HashEntry* table, uint32_t hash_mask, int32_t pool,
+                                             int32_t* block_count, unsigned long long* drop_count,
+                                             BlockCoord* block_coord, uint32_t* status,
+                                             long long key) {
+    DevVolume v{};
+    v.table = table;
+    v.hash_mask = hash_mask;
+    v.pool_capacity = pool;
+    v.block_count = block_count;
+    v.drop_count = drop_count;
+    v.block_coord = block_coord;
+    v.status = status;
+    return resolve<MODE>(v, key, nullptr, 0);
+}
+
+template <int MODE>
+__device__ __forceinline__ int32_t resolve_from(const DevVolume& v, int4 raw, long long key,
+                                                unsigned long long* hist, int n_bins) {
+    if (!has_fast_probe<MODE>()) return resolve<MODE>(v, key, hist, n_bins);
+    const int32_t bi = settle_home<MODE>(v, raw, key);
+    if (bi != -2) return bi;
+    return resolve_slow<MODE>(v.table, v.hash_mask, v.pool_capacity, v.block_count, v.drop_count,
+                              v.block_coord, v.status, key);
+}
+
+// Tag a block as touched by this update; the first tagger appends it to the
+// touched list. A cached read that already shows the tag saves the exchange
+// (a stale read can only show an older tag).
+__device__ __forceinline__ void tag_touched(const UpdateScratch& u, int32_t bi, uint32_t seen) {
+    if (bi < 0 || seen == u.tag) return;
+    if (atomicExch(&u.blk_touch[bi], u.tag) != u.tag) u.touched[atomicAdd(&u.ctl->n_touched, 1)] = bi;
+}
+
 template <int MODE, bool RECORDS>
-__global__ void __launch_bounds__(kBandThreads)
+__global__ void __launch_bounds__(kBandThreads, 8)
 band_kernel(DevVolume v, BatchArgs a, UpdateScratch u, unsigned long long* hist, int n_bins) {
     // Per-thread columns: run q of thread t at [q][t] (no bank conflicts).
     __shared__ long long run_key[kChunk][kBandThreads];
-    __shared__ int32_t run_bi[kChunk][kBandThreads];
+    __shared__ int32_t run_bi[kChunk][kBandThreads];    // written by the run's group leader
+    __shared__ uint8_t run_src[kChunk][kBandThreads];   // leader lane of the run's group
     const int t = threadIdx.x;
-    const int lane = t & 31;
+    const int lane = t & 31, wbase = t & ~31;
     const bool counts_drops = MODE != kLookupOnly && MODE != kAllocNoCas && MODE != kAllocCountingCas;
     const bool sat_check = RECORDS && v.weight_cap > 0.0f;
     const int n_tiles = (a.n + kBandThreads - 1) / kBandThreads;
     uint32_t drops = 0, counted = 0;
 
+    // The point of the next tile is loaded one tile ahead.
+    float nx = 0.0f, ny = 0.0f, nz = 0.0f;
+    {
+        const int i0 = blockIdx.x * kBandThreads + t;
+        if (blockIdx.x < n_tiles && i0 < a.n) {
+            nx = a.pos[(size_t)i0 * 3 + 0];
+            ny = a.pos[(size_t)i0 * 3 + 1];
+            nz = a.pos[(size_t)i0 * 3 + 2];
+        }
+    }
     for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
         const int i = tile * kBandThreads + t;
+        const float px = nx, py = ny, pz = nz;
+        const int inext = i + gridDim.x * kBandThreads;
+        if (inext < a.n) {
+            nx = a.pos[(size_t)inext * 3 + 0];
+            ny = a.pos[(size_t)inext * 3 + 1];
+            nz = a.pos[(size_t)inext * 3 + 2];
+        }
         Ray r;
-        const bool live = i < a.n && ray_setup(a, i, r);
+        const bool live = i < a.n && ray_setup_at(a, px, py, pz, r);
         uint32_t* rec = RECORDS ? u.records + i : nullptr;  // slot (s = -steps, i)
 
         for (int c0 = -v.steps; c0 <= v.steps; c0 += kChunk) {
@@ -83,7 +172,7 @@ band_kernel(DevVolume v, BatchArgs a, UpdateScratch u, unsigned long long* hist,
             int n_run = 0;
             long long last = kNoKey;
 
-            // Phase 1: the chunk's samples; distinct blocks in walk order.
+            // Phase 1: the chunk's samples; runs of equal blocks in walk order.
 #pragma unroll
             for (int j = 0; j < kChunk; ++j) {
                 st[j] = 0u;
@@ -108,23 +197,40 @@ band_kernel(DevVolume v, BatchArgs a, UpdateScratch u, unsigned long long* hist,
                 }
             }
 
-            // Phase 2: warp rounds, one per run index; one probe per distinct key.
+            // Phase 2a: group equal keys across the warp, one round per run
+            // index; the lowest lane of a group leads it.
+            uint32_t lead = 0u;
             for (int q = 0; q < kChunk; ++q) {
                 if (!__any_sync(0xffffffffu, q < n_run)) break;
                 const long long key = q < n_run ? run_key[q][t] : kNoKey;
                 const unsigned grp = __match_any_sync(0xffffffffu, key);
                 const int leader = __ffs(grp) - 1;
-                int32_t bi = -1;
-                if (key != kNoKey && lane == leader) {
-                    const int bx = unpack_axis(key, 2 * kCoordBits);
-                    const int by = unpack_axis(key, kCoordBits);
-                    const int bz = unpack_axis(key, 0);
-                    bi = resolve<MODE>(v, bx, by, bz, key, hist, n_bins);
-                    if (RECORDS && bi >= 0 && atomicExch(&u.blk_touch[bi], u.tag) != u.tag)
-                        u.touched[atomicAdd(&u.ctl->n_touched, 1)] = bi;
-                }
-                run_bi[q][t] = __shfl_sync(0xffffffffu, bi, leader);
+                if (q < n_run) run_src[q][t] = (uint8_t)leader;
+                if (key != kNoKey && lane == leader) lead |= 1u << q;
             }
+            // Phase 2b: each leader resolves its runs two at a time, both
+            // home-slot probes (and then both tag reads) in flight together.
+            while (lead) {
+                const int qa = __ffs(lead) - 1;
+                lead &= lead - 1u;
+                const int qb = lead ? __ffs(lead) - 1 : -1;
+                if (qb >= 0) lead &= lead - 1u;
+                const long long ka = run_key[qa][t];
+                const long long kb = qb >= 0 ? run_key[qb][t] : kNoKey;
+                const int4 ra = home_entry<MODE>(v, ka);
+                const int4 rb = qb >= 0 ? home_entry<MODE>(v, kb) : make_int4(0, 0, -1, 0);
+                const int32_t ba = resolve_from<MODE>(v, ra, ka, hist, n_bins);
+                const int32_t bb = qb >= 0 ? resolve_from<MODE>(v, rb, kb, hist, n_bins) : -1;
+                run_bi[qa][t] = ba;
+                if (qb >= 0) run_bi[qb][t] = bb;
+                if (RECORDS) {
+                    const uint32_t sa = ba >= 0 ? __ldca(&u.blk_touch[ba]) : u.tag;
+                    const uint32_t sb = bb >= 0 ? __ldca(&u.blk_touch[bb]) : u.tag;
+                    tag_touched(u, ba, sa);
+                    tag_touched(u, bb, sb);
+                }
+            }
+            __syncwarp();
 
             // Phase 3: drops; then every sample's weight gather in flight
             // together; then the saturation gate, counts, sums and records.
@@ -133,7 +239,8 @@ band_kernel(DevVolume v, BatchArgs a, UpdateScratch u, unsigned long long* hist,
             for (int j = 0; j < kChunk; ++j) {
                 vox[j] = kNoVoxel;
                 if (st[j] & kValid) {
-                    const int32_t bi = run_bi[(st[j] >> kRunShift) & 15u][t];
+                    const uint32_t q = (st[j] >> kRunShift) & 15u;
+                    const int32_t bi = run_bi[q][wbase + run_src[q][t]];
                     if (bi < 0) {
                         if (counts_drops) ++drops;
                     } else {
@@ -157,10 +264,11 @@ band_kernel(DevVolume v, BatchArgs a, UpdateScratch u, unsigned long long* hist,
                         atomicAdd(&u.vacc[out], (unsigned long long)to_fix(sdf_n));
                         ++counted;
                     }
-                    if (i < a.n) *rec = out;
+                    if (i < a.n) __stcs(rec, out);  // read again only for crossing voxels
                     rec += a.n;
                 }
             }
+            __syncwarp();  // run columns are rewritten by the next chunk
         }
     }
 

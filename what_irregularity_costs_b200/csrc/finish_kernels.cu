@@ -28,13 +28,14 @@
 //              reserves a group of n deferred records instead and its block
 //              is tagged.
 //   group      one pass over the records of the batch: a record of a tagged
-//              block whose voxel reserved a group takes the next place in
-//              it (canonical id and normalised SDF, recomputed from its point
-//              -- these are a few percent of the records).
-//   deferred   one warp per crossing voxel selects the keep records with the
-//              smallest canonical ids (ranking in registers up to 256
-//              records, a radix select of the keep-th id beyond that) and
-//              finishes the voxel.
+//              block whose voxel reserved a group puts its slot in the next
+//              place of the group (a few percent of the records).
+//   deferred   one warp per crossing voxel: each lane recomputes the
+//              canonical id and normalised SDF of its records from their
+//              points (the walk's arithmetic, same rounding), then the warp
+//              selects the keep records with the smallest ids (ranking in
+//              registers up to 256 records, a radix select of the keep-th id
+//              beyond that) and finishes the voxel.
 //
 // Sums are 64-bit fixed point added to the stored sum with one rounding, so
 // results do not depend on the order in which threads meet the records:
@@ -118,9 +119,9 @@ finish_kernel(DevVolume v, UpdateScratch u) {
         reinterpret_cast<float4*>(v.weight)[q4] = make_float4(wn[0], wn[1], wn[2], wn[3]);
         const float4 c = make_float4(__fmul_rn(128.0f, wn[0]), __fmul_rn(128.0f, wn[1]),
                                      __fmul_rn(128.0f, wn[2]), __fmul_rn(128.0f, wn[3]));
-        reinterpret_cast<float4*>(v.r)[q4] = c;
-        reinterpret_cast<float4*>(v.g)[q4] = c;
-        reinterpret_cast<float4*>(v.b)[q4] = c;
+        __stcs(reinterpret_cast<float4*>(v.r) + q4, c);  // write-only: keep them out of L2
+        __stcs(reinterpret_cast<float4*>(v.g) + q4, c);
+        __stcs(reinterpret_cast<float4*>(v.b) + q4, c);
         reinterpret_cast<uint4*>(u.vcnt)[q4] = make_uint4(cnt[0], cnt[1], cnt[2], cnt[3]);
         reinterpret_cast<ulonglong2*>(u.vacc)[2 * q4] = make_ulonglong2(acc[0], acc[1]);
         reinterpret_cast<ulonglong2*>(u.vacc)[2 * q4 + 1] = make_ulonglong2(acc[2], acc[3]);
@@ -131,42 +132,38 @@ finish_kernel(DevVolume v, UpdateScratch u) {
 
 // ---- group ---------------------------------------------------------------
 
-// One record of the batch: if its voxel reserved a group, place it.
-__device__ __forceinline__ void group_record(const DevVolume& v, const BatchArgs& a,
-                                             const UpdateScratch& u, uint32_t vi, uint32_t slot) {
-    if (vi == kNoVoxel || u.blk_cross[vi / kBlockVoxels] != u.tag) return;
-    const uint32_t hi = (uint32_t)(u.vacc[vi] >> 32);
-    if (hi == 0u) return;  // a voxel of a tagged block that did not cross
-    const uint32_t t = (uint32_t)atomicAdd(&u.vacc[vi], 1ull);
-    if (t >= u.vcnt[vi]) {  // more records than counted: state left by a failed update
-        atomicOr(v.status, kStatusScratchOverflow);
-        return;
-    }
-    // The walk's arithmetic again for this one sample (same rounding).
-    const uint32_t n_steps = 2u * (uint32_t)v.steps + 1u;
-    const uint32_t s = slot / (uint32_t)a.n, i = slot - s * (uint32_t)a.n;
-    Ray r;
-    int vx, vy, vz;
-    float sdf = 0.0f;
-    if (ray_setup(a, (int)i, r)) band_sample(v, a, r, (int)s - v.steps, vx, vy, vz, sdf);
-    const float sdf_n = fminf(fmaxf(__fmul_rn(sdf, v.inv_trunc), -1.0f), 1.0f);
-    u.deferred[(size_t)(hi - 1u) + t] = make_uint2(i * n_steps + s, __float_as_uint(sdf_n));
-}
-
 __global__ void __launch_bounds__(kGroupThreads)
-group_kernel(DevVolume v, BatchArgs a, UpdateScratch u, uint32_t n_slots) {
+group_kernel(UpdateScratch u, uint32_t n_slots) {
     if (u.ctl->n_deferred == 0) return;  // no voxel crossed the cap in this batch
-    const uint32_t n_quads = n_slots / 4u;
-    const uint4* rec4 = reinterpret_cast<const uint4*>(u.records);
-    const uint32_t q = blockIdx.x * kGroupThreads + threadIdx.x;
-    if (q < n_quads) {
-        const uint4 r = rec4[q];
-        group_record(v, a, u, r.x, 4u * q);
-        group_record(v, a, u, r.y, 4u * q + 1u);
-        group_record(v, a, u, r.z, 4u * q + 2u);
-        group_record(v, a, u, r.w, 4u * q + 3u);
-    } else if (q == n_quads) {
-        for (uint32_t k = 4u * q; k < n_slots; ++k) group_record(v, a, u, u.records[k], k);
+    // Four records per thread, phase by phase: the block-tag gathers of all
+    // four in flight together, then the (rare) records of crossing voxels
+    // take the next place of their voxel's group.
+    const uint32_t q = blockIdx.x * kGroupThreads + threadIdx.x;  // quad of slots
+    if (4u * q >= n_slots) return;
+    uint32_t vi[4];
+    if (4u * q + 3u < n_slots) {
+        const uint4 r = __ldcs(reinterpret_cast<const uint4*>(u.records) + q);
+        vi[0] = r.x;
+        vi[1] = r.y;
+        vi[2] = r.z;
+        vi[3] = r.w;
+    } else {
+#pragma unroll
+        for (uint32_t m = 0; m < 4u; ++m) vi[m] = 4u * q + m < n_slots ? u.records[4u * q + m] : kNoVoxel;
+    }
+    bool cand[4];
+#pragma unroll
+    for (int m = 0; m < 4; ++m)
+        cand[m] = vi[m] != kNoVoxel && u.blk_cross[vi[m] / kBlockVoxels] == u.tag;
+    uint32_t hi[4];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) hi[m] = cand[m] ? (uint32_t)(u.vacc[vi[m]] >> 32) : 0u;
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        if (hi[m] == 0u) continue;  // not a voxel that reserved a group
+        const uint32_t t = (uint32_t)atomicAdd(&u.vacc[vi[m]], 1ull);
+        if (t < u.vcnt[vi[m]]) u.deferred[(size_t)(hi[m] - 1u) + t] = 4u * q + m;
+        else atomicOr(u.status, kStatusScratchOverflow);  // state left by a failed update
     }
 }
 
@@ -174,14 +171,17 @@ group_kernel(DevVolume v, BatchArgs a, UpdateScratch u, uint32_t n_slots) {
 
 // The keep-th smallest id (1-based) of a group, by four 8-bit radix passes
 // with a per-warp histogram. Ids are distinct, so exactly keep ids are <= it.
-__device__ uint32_t radix_select(const uint2* X, int n, int keep, uint32_t* hist, int lane) {
+__device__ uint32_t slot_id(const DevVolume& v, const BatchArgs& a, uint32_t slot);
+
+__device__ uint32_t radix_select(const DevVolume& v, const BatchArgs& a, const uint32_t* X, int n,
+                                 int keep, uint32_t* hist, int lane) {
     uint32_t prefix = 0u, pmask = 0u;
     int need = keep;
     for (int shift = 24; shift >= 0; shift -= 8) {
         for (int b = lane; b < 256; b += 32) hist[b] = 0u;
         __syncwarp();
         for (int k = lane; k < n; k += 32) {
-            const uint32_t id = X[k].x;
+            const uint32_t id = slot_id(v, a, X[k]);
             if ((id & pmask) == prefix) atomicAdd(&hist[(id >> shift) & 255u], 1u);
         }
         __syncwarp();
@@ -221,8 +221,27 @@ __device__ uint32_t radix_select(const uint2* X, int n, int keep, uint32_t* hist
     return prefix;
 }
 
+// Canonical id and normalised SDF of the record in band slot `slot`: the
+// walk's arithmetic again for this one sample (same rounding).
+__device__ __forceinline__ uint32_t slot_record(const DevVolume& v, const BatchArgs& a, uint32_t slot,
+                                                float& sdf_n) {
+    const uint32_t n_steps = 2u * (uint32_t)v.steps + 1u;
+    const uint32_t s = slot / (uint32_t)a.n, i = slot - s * (uint32_t)a.n;
+    Ray r;
+    int vx, vy, vz;
+    float sdf = 0.0f;
+    if (ray_setup(a, (int)i, r)) band_sample(v, a, r, (int)s - v.steps, vx, vy, vz, sdf);
+    sdf_n = fminf(fmaxf(__fmul_rn(sdf, v.inv_trunc), -1.0f), 1.0f);
+    return i * n_steps + s;
+}
+
+__device__ __forceinline__ uint32_t slot_id(const DevVolume& v, const BatchArgs& a, uint32_t slot) {
+    const uint32_t s = slot / (uint32_t)a.n;
+    return (slot - s * (uint32_t)a.n) * (2u * (uint32_t)v.steps + 1u) + s;
+}
+
 __global__ void __launch_bounds__(kDeferThreads)
-deferred_kernel(DevVolume v, UpdateScratch u) {
+deferred_kernel(DevVolume v, BatchArgs a, UpdateScratch u) {
     __shared__ uint32_t hist[kDeferWarps][256];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int nd = min(u.ctl->n_deferred, u.dvox_cap);
@@ -231,25 +250,27 @@ deferred_kernel(DevVolume v, UpdateScratch u) {
         const int4 e = u.dvox[d];  // (voxel, group base, records, accepted)
         const uint32_t vi = (uint32_t)e.x;
         const int n = e.z, keep = e.w;
-        const uint2* X = u.deferred + (uint32_t)e.y;
+        const uint32_t* X = u.deferred + (uint32_t)e.y;
         long long fix = 0;
         if (n <= 32 * kRankRegs) {
+            // Up to 8 records per lane, ranked by id against all others.
             uint32_t id[kRankRegs];
             float val[kRankRegs];
             int rank[kRankRegs];
+            const int rows = (n + 31) / 32;
 #pragma unroll
             for (int r = 0; r < kRankRegs; ++r) {
                 const int k = r * 32 + lane;
-                const uint2 x = k < n ? X[k] : make_uint2(0xFFFFFFFFu, 0u);
-                id[r] = x.x;
-                val[r] = __uint_as_float(x.y);
+                id[r] = 0xFFFFFFFFu;
+                val[r] = 0.0f;
                 rank[r] = 0;
+                if (r < rows && k < n) id[r] = slot_record(v, a, X[k], val[r]);
             }
-            const int rows = (n + 31) / 32;
 #pragma unroll
             for (int rr = 0; rr < kRankRegs; ++rr) {
                 if (rr >= rows) break;
-                for (int src = 0; src < 32; ++src) {
+                const int m = min(32, n - rr * 32);
+                for (int src = 0; src < m; ++src) {
                     const uint32_t other = __shfl_sync(0xffffffffu, id[rr], src);
 #pragma unroll
                     for (int r = 0; r < kRankRegs; ++r)
@@ -258,12 +279,16 @@ deferred_kernel(DevVolume v, UpdateScratch u) {
             }
 #pragma unroll
             for (int r = 0; r < kRankRegs; ++r)
-                if (r * 32 + lane < n && rank[r] < keep) fix += to_fix(val[r]);
+                if (r < rows && r * 32 + lane < n && rank[r] < keep) fix += to_fix(val[r]);
         } else {
-            const uint32_t last = radix_select(X, n, keep, hist[warp], lane);
+            // The keep-th smallest id by radix select over the group's ids,
+            // then the accepted records' values.
+            const uint32_t last = radix_select(v, a, X, n, keep, hist[warp], lane);
             for (int k = lane; k < n; k += 32) {
-                const uint2 x = X[k];
-                if (x.x <= last) fix += to_fix(__uint_as_float(x.y));
+                if (slot_id(v, a, X[k]) > last) continue;
+                float val;
+                slot_record(v, a, X[k], val);
+                fix += to_fix(val);
             }
         }
         for (int o = 16; o > 0; o >>= 1) fix += __shfl_xor_sync(0xffffffffu, fix, o);
@@ -295,14 +320,14 @@ cudaError_t launch_group(const DevVolume& v, const BatchArgs& a, const UpdateScr
                          cudaStream_t s) {
     const uint32_t n_slots = (uint32_t)a.n * (2u * (uint32_t)v.steps + 1u);
     if (n_slots == 0) return cudaSuccess;
-    const uint32_t threads = n_slots / 4u + 1u;
-    group_kernel<<<(threads + kGroupThreads - 1) / kGroupThreads, kGroupThreads, 0, s>>>(v, a, u,
-                                                                                         n_slots);
+    const uint32_t per_cta = kGroupThreads * 4u;
+    group_kernel<<<(n_slots + per_cta - 1u) / per_cta, kGroupThreads, 0, s>>>(u, n_slots);
     return cudaGetLastError();
 }
 
-cudaError_t launch_deferred(const DevVolume& v, const UpdateScratch& u, int n_ctas, cudaStream_t s) {
-    deferred_kernel<<<n_ctas, kDeferThreads, 0, s>>>(v, u);
+cudaError_t launch_deferred(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
+                            int n_ctas, cudaStream_t s) {
+    deferred_kernel<<<n_ctas, kDeferThreads, 0, s>>>(v, a, u);
     return cudaGetLastError();
 }
 

@@ -122,12 +122,13 @@ struct Ray {
     float dist;
 };
 
-// Point set-up. False when the point is gated out by the far cutoff or sits
-// on the camera (volume.cpp:158-166).
-__device__ __forceinline__ bool ray_setup(const BatchArgs& a, int i, Ray& r) {
-    r.px = a.pos[(size_t)i * 3 + 0];
-    r.py = a.pos[(size_t)i * 3 + 1];
-    r.pz = a.pos[(size_t)i * 3 + 2];
+// Point set-up for a point already loaded into (px, py, pz). False when the
+// point is gated out by the far cutoff or sits on the camera
+// (volume.cpp:158-166).
+__device__ __forceinline__ bool ray_setup_at(const BatchArgs& a, float px, float py, float pz, Ray& r) {
+    r.px = px;
+    r.py = py;
+    r.pz = pz;
     const float dx = __fsub_rn(r.px, a.cam_x);
     const float dy = __fsub_rn(r.py, a.cam_y);
     const float dz = __fsub_rn(r.pz, a.cam_z);
@@ -139,6 +140,11 @@ __device__ __forceinline__ bool ray_setup(const BatchArgs& a, int i, Ray& r) {
     r.uy = __fdiv_rn(dy, r.dist);
     r.uz = __fdiv_rn(dz, r.dist);
     return true;
+}
+
+__device__ __forceinline__ bool ray_setup(const BatchArgs& a, int i, Ray& r) {
+    return ray_setup_at(a, a.pos[(size_t)i * 3 + 0], a.pos[(size_t)i * 3 + 1], a.pos[(size_t)i * 3 + 2],
+                        r);
 }
 
 // Band sample s in [-steps, steps]: voxel index and signed distance at the

@@ -12,8 +12,8 @@
 // with its scratch in one fixed array compiled into the library.
 //
 // The array is a file-scope __device__ variable of kNoAllocScratchBytes
-// (40 MiB + 256 bytes): the control counters, kNoAllocMaxRecords 4-byte band
-// records, as many 8-byte deferred records, and half as many 16-byte
+// (32 MiB + 256 bytes): the control counters, kNoAllocMaxRecords 4-byte band
+// records, as many 4-byte deferred slots, and half as many 16-byte
 // deferred-voxel entries, i.e. batches with
 // n_points * (2 * steps + 1) <= 2,097,152 (a 480x360 frame at 9 band steps
 // per point fits; a 640x480 frame must be split in two). The per-voxel and
@@ -39,7 +39,7 @@ constexpr size_t kNoAllocHeaderBytes = 256;  // UpdateControl, padded
 constexpr int64_t kNoAllocMaxRecords = OSN_TSDF_NOALLOC_MAX_RECORDS;
 constexpr int64_t kNoAllocMaxDeferred = kNoAllocMaxRecords / 2;
 constexpr size_t kNoAllocRecordBytes = (size_t)kNoAllocMaxRecords * sizeof(uint32_t);
-constexpr size_t kNoAllocDeferredBytes = (size_t)kNoAllocMaxRecords * sizeof(uint2);
+constexpr size_t kNoAllocDeferredBytes = (size_t)kNoAllocMaxRecords * sizeof(uint32_t);
 constexpr size_t kNoAllocScratchBytes = kNoAllocHeaderBytes + kNoAllocRecordBytes +
                                         kNoAllocDeferredBytes +
                                         (size_t)kNoAllocMaxDeferred * sizeof(int4);
@@ -80,7 +80,7 @@ cudaError_t Volume::update_static_scratch(const BatchArgs& a, void* scratch) {
     UpdateScratch u = us_;
     u.ctl = reinterpret_cast<UpdateControl*>(base);
     u.records = reinterpret_cast<uint32_t*>(base + kNoAllocHeaderBytes);
-    u.deferred = reinterpret_cast<uint2*>(base + kNoAllocHeaderBytes + kNoAllocRecordBytes);
+    u.deferred = reinterpret_cast<uint32_t*>(base + kNoAllocHeaderBytes + kNoAllocRecordBytes);
     u.dvox = reinterpret_cast<int4*>(base + kNoAllocHeaderBytes + kNoAllocRecordBytes +
                                      kNoAllocDeferredBytes);
     u.record_cap = kNoAllocMaxRecords;

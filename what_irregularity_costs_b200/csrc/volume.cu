@@ -74,6 +74,7 @@ bool Volume::alloc_device(uint32_t hash_slots) {
     OSN_TRY(cudaMalloc(&us_.blk_cross, (size_t)dv_.pool_capacity * sizeof(uint32_t)));
     OSN_TRY(cudaMalloc(&us_.touched, (size_t)dv_.pool_capacity * sizeof(int32_t)));
     OSN_TRY(cudaMalloc(&us_.ctl, sizeof(UpdateControl)));
+    us_.status = dv_.status;
     OSN_TRY(cudaMalloc(&mesh_ctl_, 2 * sizeof(int32_t)));
     OSN_TRY(cudaMallocHost(&host_small_, 8 * sizeof(int64_t)));
 
@@ -205,7 +206,7 @@ bool Volume::ensure_records(int64_t n_records) {
     // the deferred list.
     const int64_t n_dvox = n_records / 2 + 1;
     if (cudaMalloc(&us_.records, (size_t)n_records * sizeof(uint32_t)) != cudaSuccess) return false;
-    if (cudaMalloc(&us_.deferred, (size_t)n_records * sizeof(uint2)) != cudaSuccess) return false;
+    if (cudaMalloc(&us_.deferred, (size_t)n_records * sizeof(uint32_t)) != cudaSuccess) return false;
     if (cudaMalloc(&us_.dvox, (size_t)n_dvox * sizeof(int4)) != cudaSuccess) return false;
     us_.record_cap = n_records;
     us_.dvox_cap = (int32_t)std::min<int64_t>(n_dvox, INT32_MAX);
@@ -236,7 +237,7 @@ cudaError_t Volume::run_update(const BatchArgs& a, const UpdateScratch& scratch,
     mark_end(kKGroup);
     if (e != cudaSuccess) return e;
     mark_start(kKDeferred);
-    e = launch_deferred(dv_, u, sm_count_ * 8, stream_);
+    e = launch_deferred(dv_, a, u, sm_count_ * 8, stream_);
     mark_end(kKDeferred);
     return e;
 }

@@ -46,7 +46,7 @@ constexpr int32_t kMaxPoolBlocks = (1 << 23) - 1;
 struct UpdateScratch {
     UpdateControl* ctl = nullptr;
     uint32_t* records = nullptr;  // [record_cap] one per band slot
-    uint2* deferred = nullptr;    // [record_cap] (canonical id, sdf_n bits), grouped per voxel
+    uint32_t* deferred = nullptr; // [record_cap] band slots of crossing voxels' records, grouped per voxel
     int4* dvox = nullptr;         // [dvox_cap] (voxel, group base, records, accepted)
     int64_t record_cap = 0;
     int32_t dvox_cap = 0;
@@ -57,6 +57,7 @@ struct UpdateScratch {
     uint32_t* blk_touch = nullptr;  // update that last touched the block
     uint32_t* blk_cross = nullptr;  // update in which the block held a cap-crossing voxel
     int32_t* touched = nullptr;     // [pool] blocks touched by this update
+    uint32_t* status = nullptr;     // the volume's status word
     uint32_t tag = 0;               // this update's number (never 0)
 };
 
@@ -148,7 +149,8 @@ cudaError_t launch_band_records(const DevVolume& v, const BatchArgs& a, const Up
 cudaError_t launch_finish(const DevVolume& v, const UpdateScratch& u, int n_ctas, cudaStream_t s);
 cudaError_t launch_group(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
                          cudaStream_t s);
-cudaError_t launch_deferred(const DevVolume& v, const UpdateScratch& u, int n_ctas, cudaStream_t s);
+cudaError_t launch_deferred(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
+                            int n_ctas, cudaStream_t s);
 
 }  // namespace osn_b200
 
