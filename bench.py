@@ -280,11 +280,17 @@ def run_reference(args):
     return 0
 
 
+def set_workload(frames, pool):
+    """Frames per step and pool size (the defaults are the benchmark's workload)."""
+    global N_FRAMES, POOL
+    N_FRAMES, POOL = int(frames), int(pool)
+
+
 def config_dict(points):
     return {
-        "workload": "room trajectory, 100 frames 640x480 fx=fy=320, 2 cm voxels, trunc 8 cm, "
-                    "2^20 table slots, pool 2^19 blocks, weight cap 64; step = reset + "
-                    "allocate/update of every frame",
+        "workload": f"room trajectory, {N_FRAMES} frames 640x480 fx=fy=320, 2 cm voxels, "
+                    f"trunc 8 cm, 2^20 table slots, pool {POOL} blocks, weight cap 64; step = "
+                    "reset + allocate/update of every frame",
         "frames_per_step": N_FRAMES, "resolution": [640, 480], "voxel_m": VOXEL,
         "trunc_m": TRUNC, "hash_slots": HASH_SLOTS, "pool_blocks": POOL, "weight_cap": CAP,
         "points_per_step": points, "seed": SEED,
@@ -485,7 +491,11 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--ref-frames", type=int, default=20,
                     help="frames per step of the reference arm")
+    ap.add_argument("--frames", type=int, default=N_FRAMES,
+                    help="frames of the trajectory per step (fewer: a small profiling case)")
+    ap.add_argument("--pool", type=int, default=POOL, help="pool capacity in blocks")
     args = ap.parse_args()
+    set_workload(args.frames, args.pool)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -109,14 +109,30 @@ void osn_tsdf_cuda_synchronize(const OsnTsdfCudaVolume* v);
 
 /* ---- extensions (no counterpart in the reference) ---------------------- */
 
-/* Storage modes for create_ex. */
+/* Voxel storage modes for create_ex.
+ *   FP32      the reference's layout (above): float weighted sums in tsdf,
+ *             weight, r, g, b; 20 bytes per voxel.
+ *   FP16_U16  the MEAN normalised TSDF as IEEE half in tsdf and the weight
+ *             as uint16 in weight (4 bytes per voxel); r, g, b are NULL in
+ *             the device view (through this ABI every contribution is grey,
+ *             so the mean colour of an observed voxel is 128). The running
+ *             average (mean * w + batch sum) / (w + accepted) is formed in
+ *             FP32 and rounded to half once per batch. Weights saturate at
+ *             65535, which is also the cap when weight_cap <= 0 or > 65535.
+ *   FP64      the on-device FP64 oracle: double TSDF sums in tsdf, float
+ *             weights, no colour arrays; the signed distance of every band
+ *             sample is evaluated in double (the samples, blocks and
+ *             accepted contributions are those of FP32).
+ * Hashing, block coordinates and allocation are identical in every mode. */
 #define OSN_TSDF_STORAGE_FP32 0
+#define OSN_TSDF_STORAGE_FP16_U16 1
+#define OSN_TSDF_STORAGE_FP64 2
 
-/* create with an explicit table size. The reference always sizes the table
- * to next_pow2(2 * pool), which caps its load factor below 0.5; hash_slots
- * (a power of two >= 2, or 0 for the reference sizing) reaches the 0.75 and
- * 0.9 load factors of the irregularity sweep. storage must be
- * OSN_TSDF_STORAGE_FP32. */
+/* create with an explicit table size and a storage mode. The reference
+ * always sizes the table to next_pow2(2 * pool), which caps its load factor
+ * below 0.5; hash_slots (a power of two >= 2, or 0 for the reference sizing)
+ * reaches the 0.75 and 0.9 load factors of the irregularity sweep. storage
+ * is one of OSN_TSDF_STORAGE_*; NULL for any other value. */
 OsnTsdfCudaVolume* osn_tsdf_cuda_create_ex(float voxel_size_m, int32_t pool_capacity_blocks,
                                            float trunc_m, float weight_cap, uint32_t hash_slots,
                                            int32_t storage);
@@ -141,6 +157,9 @@ uint32_t osn_tsdf_cuda_status(const OsnTsdfCudaVolume* v);
 
 /* The volume's cudaStream_t, for callers that order their own work after it. */
 void* osn_tsdf_cuda_stream(const OsnTsdfCudaVolume* v);
+
+/* The volume's OSN_TSDF_STORAGE_* mode, or -1 for a NULL or invalid volume. */
+int32_t osn_tsdf_cuda_storage(const OsnTsdfCudaVolume* v);
 
 /* MEASUREMENT: one allocate pass that also records, per warp-leader probe
  * sequence, how many slots it visited: hist[min(steps, n_bins-1)] += 1.

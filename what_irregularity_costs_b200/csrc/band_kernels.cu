@@ -36,6 +36,7 @@
 // "accept while weight before < cap" they cannot be accepted in any order,
 // so leaving them out changes no result.
 #include <algorithm>
+#include <climits>
 #include <mutex>
 
 #include "volume.h"
@@ -45,6 +46,7 @@ namespace {
 
 constexpr int kBandThreads = 128;
 constexpr int kChunk = 9;  // samples per ray held in registers (the whole band at 4 voxels)
+constexpr int kBandMinBlocks = 8;  // resident CTAs per SM the register budget is sized for
 
 // Per-sample state: voxel within block (9 bits), run index (4 bits), valid.
 constexpr uint32_t kLvMask = 0x1FFu;
@@ -123,14 +125,30 @@ __device__ __forceinline__ int32_t resolve_from(const DevVolume& v, int4 raw, lo
 
 // Tag a block as touched by this update; the first tagger appends it to the
 // touched list. A cached read that already shows the tag saves the exchange
-// (a stale read can only show an older tag).
+// (a stale read can only show an older tag). The appends of the lanes that
+// arrive together take their places with one atomic on the list's counter.
 __device__ __forceinline__ void tag_touched(const UpdateScratch& u, int32_t bi, uint32_t seen) {
-    if (bi < 0 || seen == u.tag) return;
-    if (atomicExch(&u.blk_touch[bi], u.tag) != u.tag) u.touched[atomicAdd(&u.ctl->n_touched, 1)] = bi;
+    const bool add = bi >= 0 && seen != u.tag && atomicExch(&u.blk_touch[bi], u.tag) != u.tag;
+    const unsigned act = __activemask();
+    const unsigned want = __ballot_sync(act, add);
+    if (!want) return;
+    const int ldr = __ffs(want) - 1;
+    int base = 0;
+    if ((int)(threadIdx.x & 31) == ldr) base = atomicAdd(&u.ctl->n_touched, __popc(want));
+    base = __shfl_sync(act, base, ldr);
+    if (add) u.touched[base + __popc(want & lanemask_lt())] = bi;
 }
 
-template <int MODE, bool RECORDS>
-__global__ void __launch_bounds__(kBandThreads, 8)
+// Fire-and-forget L2 reductions (no value comes back, nothing waits).
+__device__ __forceinline__ void red_add(uint32_t* p, uint32_t x) {
+    asm volatile("red.global.add.u32 [%0], %1;" ::"l"(p), "r"(x));
+}
+__device__ __forceinline__ void red_add(unsigned long long* p, unsigned long long x) {
+    asm volatile("red.global.add.u64 [%0], %1;" ::"l"(p), "l"(x));
+}
+
+template <int MODE, bool RECORDS, int S>
+__global__ void __launch_bounds__(kBandThreads, kBandMinBlocks)
 band_kernel(DevVolume v, BatchArgs a, UpdateScratch u, unsigned long long* hist, int n_bins) {
     // Per-thread columns: run q of thread t at [q][t] (no bank conflicts).
     __shared__ long long run_key[kChunk][kBandThreads];
@@ -142,6 +160,12 @@ band_kernel(DevVolume v, BatchArgs a, UpdateScratch u, unsigned long long* hist,
     const bool sat_check = RECORDS && v.weight_cap > 0.0f;
     const int n_tiles = (a.n + kBandThreads - 1) / kBandThreads;
     uint32_t drops = 0, counted = 0;
+    __shared__ unsigned s_drops, s_counted;
+    if (t == 0) {
+        s_drops = 0u;
+        s_counted = 0u;
+    }
+    __syncthreads();
 
     // The point of the next tile is loaded one tile ahead.
     float nx = 0.0f, ny = 0.0f, nz = 0.0f;
@@ -252,16 +276,27 @@ band_kernel(DevVolume v, BatchArgs a, UpdateScratch u, unsigned long long* hist,
                 float w0[kChunk];
 #pragma unroll
                 for (int j = 0; j < kChunk; ++j)
-                    w0[j] = (sat_check && vox[j] != kNoVoxel) ? __ldg(&v.weight[vox[j]]) : 0.0f;
+                    w0[j] = (sat_check && vox[j] != kNoVoxel) ? weight_at<S>(v, vox[j]) : 0.0f;
 #pragma unroll
                 for (int j = 0; j < kChunk; ++j) {
                     if (c0 + j > v.steps) break;
                     uint32_t out = kNoVoxel;
                     if (vox[j] != kNoVoxel && !(sat_check && w0[j] >= v.weight_cap)) {
                         out = vox[j];
-                        const float sdf_n = fminf(fmaxf(__fmul_rn(sd[j], v.inv_trunc), -1.0f), 1.0f);
-                        atomicAdd(&u.vcnt[out], 1u);
-                        atomicAdd(&u.vacc[out], (unsigned long long)to_fix(sdf_n));
+                        long long fix;
+                        if constexpr (S == kStoreF64) {
+                            // The oracle's value of the same sample, in double.
+                            const long long key = run_key[(st[j] >> kRunShift) & 15u][t];
+                            const uint32_t lv = st[j] & kLvMask;
+                            const int vx = unpack_axis(key, 2 * kCoordBits) * kBlockDim + (int)(lv & 7u);
+                            const int vy = unpack_axis(key, kCoordBits) * kBlockDim + (int)((lv >> 3) & 7u);
+                            const int vz = unpack_axis(key, 0) * kBlockDim + (int)(lv >> 6);
+                            fix = to_fix(clamp_sdf_n_f64(sdf_f64(v, a, r.px, r.py, r.pz, vx, vy, vz), v.trunc));
+                        } else {
+                            fix = to_fix(fminf(fmaxf(__fmul_rn(sd[j], v.inv_trunc), -1.0f), 1.0f));
+                        }
+                        red_add(&u.vcnt[out], 1u);
+                        red_add(&u.vacc[out], (unsigned long long)fix);
                         ++counted;
                     }
                     if (i < a.n) __stcs(rec, out);  // read again only for crossing voxels
@@ -272,17 +307,17 @@ band_kernel(DevVolume v, BatchArgs a, UpdateScratch u, unsigned long long* hist,
         }
     }
 
-    if (counts_drops) {
-        const unsigned total = __reduce_add_sync(0xffffffffu, drops);
-        if (lane == 0 && total) atomicAdd(v.drop_count, (unsigned long long)total);
-    }
-    if (RECORDS) {
-        const unsigned total = __reduce_add_sync(0xffffffffu, counted);
-        if (lane == 0 && total) atomicAdd(&u.ctl->n_records, (int)total);
-    }
+    // Counters: one global atomic per CTA (per-warp atomics on one line serialise).
+    const unsigned wd = counts_drops ? __reduce_add_sync(0xffffffffu, drops) : 0u;
+    const unsigned wc = RECORDS ? __reduce_add_sync(0xffffffffu, counted) : 0u;
+    if (lane == 0 && wd) atomicAdd(&s_drops, wd);
+    if (lane == 0 && wc) atomicAdd(&s_counted, wc);
+    __syncthreads();
+    if (t == 0 && s_drops) atomicAdd(v.drop_count, (unsigned long long)s_drops);
+    if (t == 0 && s_counted) atomicAdd(&u.ctl->n_records, (int)s_counted);
 }
 
-template <int MODE, bool RECORDS>
+template <int MODE, bool RECORDS, int S = kStoreF32>
 cudaError_t launch(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
                    unsigned long long* hist, int n_bins, int sm_count, cudaStream_t s) {
     if (a.n <= 0) return cudaSuccess;
@@ -291,14 +326,14 @@ cudaError_t launch(const DevVolume& v, const BatchArgs& a, const UpdateScratch& 
     static int per_sm = 0;
     static std::once_flag once;
     std::call_once(once, [] {
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, band_kernel<MODE, RECORDS>,
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, band_kernel<MODE, RECORDS, S>,
                                                           kBandThreads, 0) != cudaSuccess ||
             per_sm < 1)
             per_sm = 1;
     });
     const int tiles = (a.n + kBandThreads - 1) / kBandThreads;
     const int grid = std::min(tiles, per_sm * sm_count);
-    band_kernel<MODE, RECORDS><<<grid, kBandThreads, 0, s>>>(v, a, u, hist, n_bins);
+    band_kernel<MODE, RECORDS, S><<<grid, kBandThreads, 0, s>>>(v, a, u, hist, n_bins);
     return cudaGetLastError();
 }
 
@@ -321,8 +356,17 @@ cudaError_t launch_allocate(const DevVolume& v, const BatchArgs& a, int mode,
 
 cudaError_t launch_band_records(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
                                 bool insert, int sm_count, cudaStream_t s) {
-    return insert ? launch<kAllocInsert, true>(v, a, u, nullptr, 0, sm_count, s)
-                  : launch<kLookupOnly, true>(v, a, u, nullptr, 0, sm_count, s);
+    switch (v.storage) {
+        case kStoreF16U16:
+            return insert ? launch<kAllocInsert, true, kStoreF16U16>(v, a, u, nullptr, 0, sm_count, s)
+                          : launch<kLookupOnly, true, kStoreF16U16>(v, a, u, nullptr, 0, sm_count, s);
+        case kStoreF64:
+            return insert ? launch<kAllocInsert, true, kStoreF64>(v, a, u, nullptr, 0, sm_count, s)
+                          : launch<kLookupOnly, true, kStoreF64>(v, a, u, nullptr, 0, sm_count, s);
+        default:
+            return insert ? launch<kAllocInsert, true>(v, a, u, nullptr, 0, sm_count, s)
+                          : launch<kLookupOnly, true>(v, a, u, nullptr, 0, sm_count, s);
+    }
 }
 
 }  // namespace osn_b200

@@ -14,8 +14,8 @@ static_assert(sizeof(OsnTsdfDeviceView) == 104,
 
 struct OsnTsdfCudaVolume {
     Volume vol;
-    OsnTsdfCudaVolume(float voxel, int32_t pool, float trunc, float cap, uint32_t slots)
-        : vol(voxel, pool, trunc, cap, slots) {}
+    OsnTsdfCudaVolume(float voxel, int32_t pool, float trunc, float cap, uint32_t slots, int storage)
+        : vol(voxel, pool, trunc, cap, slots, storage) {}
 };
 
 namespace {
@@ -65,10 +65,12 @@ OsnTsdfCudaVolume* osn_tsdf_cuda_create(float voxel_size_m, int32_t pool_capacit
 OsnTsdfCudaVolume* osn_tsdf_cuda_create_ex(float voxel_size_m, int32_t pool_capacity_blocks,
                                            float trunc_m, float weight_cap, uint32_t hash_slots,
                                            int32_t storage) {
-    if (storage != OSN_TSDF_STORAGE_FP32) return nullptr;
+    if (storage != OSN_TSDF_STORAGE_FP32 && storage != OSN_TSDF_STORAGE_FP16_U16 &&
+        storage != OSN_TSDF_STORAGE_FP64)
+        return nullptr;
     if (!(voxel_size_m > 0.0f) || pool_capacity_blocks <= 0) return nullptr;
     auto* v = new (std::nothrow) OsnTsdfCudaVolume(voxel_size_m, pool_capacity_blocks, trunc_m,
-                                                   weight_cap, hash_slots);
+                                                   weight_cap, hash_slots, storage);
     if (!v) return nullptr;
     if (!v->vol.ok()) {
         delete v;
@@ -99,8 +101,12 @@ int32_t osn_tsdf_cuda_device_view(const OsnTsdfCudaVolume* v, OsnTsdfDeviceView*
     out->block_dim = osn_b200::kBlockDim;
     out->voxel_size_m = d.voxel_size;
     out->trunc_m = d.trunc;
-    out->weight_cap = d.weight_cap;
+    out->weight_cap = v->vol.weight_cap();
     return 0;
+}
+
+int32_t osn_tsdf_cuda_storage(const OsnTsdfCudaVolume* v) {
+    return usable(v) ? v->vol.storage() : -1;
 }
 
 int32_t osn_tsdf_cuda_allocate_blocks(OsnTsdfCudaVolume* v, const float* d_positions,

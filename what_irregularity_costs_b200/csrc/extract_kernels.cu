@@ -138,6 +138,7 @@ __device__ __forceinline__ void emit_triangle(const Vert& a, const Vert& b, cons
     }
 }
 
+template <int S>
 __global__ void __launch_bounds__(kExtractThreads)
 extract_kernel(DevVolume v, int32_t n_blocks, float min_w, float iso, float* out_posnor,
                uint8_t* out_rgb, int32_t cap, int32_t* ctl) {
@@ -167,15 +168,22 @@ extract_kernel(DevVolume v, int32_t n_blocks, float min_w, float iso, float* out
         h.val[k] = 0.0f;
         if (nb >= 0) {
             const size_t idx = (size_t)nb * kBlockVoxels + (size_t)((((hz & 7) * kBlockDim) + (hy & 7)) * kBlockDim + (hx & 7));
-            const float w = v.weight[idx];
+            const float w = weight_at<S>(v, idx);
             if (!(w < min_w || w <= 0.0f)) {
                 ok = 1;
-                const float inv = __fdiv_rn(1.0f, w);
-                h.val[k] = __fmul_rn(v.tsdf[idx], inv);
+                h.val[k] = mean_at<S>(v, idx, w);
                 if (want_col) {
-                    h.col[0][k] = __fmul_rn(v.r[idx], inv);
-                    h.col[1][k] = __fmul_rn(v.g[idx], inv);
-                    h.col[2][k] = __fmul_rn(v.b[idx], inv);
+                    if constexpr (S == kStoreF32) {
+                        const float inv = __fdiv_rn(1.0f, w);
+                        h.col[0][k] = __fmul_rn(v.r[idx], inv);
+                        h.col[1][k] = __fmul_rn(v.g[idx], inv);
+                        h.col[2][k] = __fmul_rn(v.b[idx], inv);
+                    } else {
+                        // No colour arrays: every contribution is grey.
+                        h.col[0][k] = 128.0f;
+                        h.col[1][k] = 128.0f;
+                        h.col[2][k] = 128.0f;
+                    }
                 }
             }
         }
@@ -275,15 +283,22 @@ __global__ void reset_table_kernel(HashEntry* table, uint32_t count, long long k
     }
 }
 
-__global__ void reset_voxels_kernel(DevVolume v, size_t n_vec4) {
+// Zero the first n_voxels voxels of every array of the volume's storage, 16
+// bytes per store (n_voxels is a multiple of 512).
+__global__ void reset_voxels_kernel(DevVolume v, size_t n_voxels) {
     const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
-    for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n_vec4;
+    const size_t n_t = n_voxels * (size_t)tsdf_bytes(v.storage) / 16;
+    const size_t n_w = n_voxels * (size_t)weight_bytes(v.storage) / 16;
+    const bool rgb = v.storage == kStoreF32;
+    for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n_t;
          k += (size_t)gridDim.x * blockDim.x) {
         reinterpret_cast<float4*>(v.tsdf)[k] = z;
-        reinterpret_cast<float4*>(v.weight)[k] = z;
-        reinterpret_cast<float4*>(v.r)[k] = z;
-        reinterpret_cast<float4*>(v.g)[k] = z;
-        reinterpret_cast<float4*>(v.b)[k] = z;
+        if (k < n_w) reinterpret_cast<float4*>(v.weight)[k] = z;
+        if (rgb) {
+            reinterpret_cast<float4*>(v.r)[k] = z;
+            reinterpret_cast<float4*>(v.g)[k] = z;
+            reinterpret_cast<float4*>(v.b)[k] = z;
+        }
     }
 }
 
@@ -292,7 +307,20 @@ __global__ void reset_voxels_kernel(DevVolume v, size_t n_vec4) {
 cudaError_t launch_extract(const DevVolume& v, int32_t n_blocks, float min_w, float iso,
                            float* posnor, uint8_t* rgb, int32_t cap, int32_t* ctl, cudaStream_t s) {
     if (n_blocks <= 0) return cudaSuccess;
-    extract_kernel<<<n_blocks, kExtractThreads, 0, s>>>(v, n_blocks, min_w, iso, posnor, rgb, cap, ctl);
+    switch (v.storage) {
+        case kStoreF16U16:
+            extract_kernel<kStoreF16U16><<<n_blocks, kExtractThreads, 0, s>>>(v, n_blocks, min_w, iso,
+                                                                               posnor, rgb, cap, ctl);
+            break;
+        case kStoreF64:
+            extract_kernel<kStoreF64><<<n_blocks, kExtractThreads, 0, s>>>(v, n_blocks, min_w, iso,
+                                                                            posnor, rgb, cap, ctl);
+            break;
+        default:
+            extract_kernel<kStoreF32><<<n_blocks, kExtractThreads, 0, s>>>(v, n_blocks, min_w, iso,
+                                                                            posnor, rgb, cap, ctl);
+            break;
+    }
     return cudaGetLastError();
 }
 
@@ -305,9 +333,10 @@ cudaError_t launch_reset_table(HashEntry* first, uint32_t count, long long key, 
 
 cudaError_t launch_reset_voxels(const DevVolume& v, int32_t n_blocks, cudaStream_t s) {
     if (n_blocks <= 0) return cudaSuccess;
-    const size_t n_vec4 = (size_t)n_blocks * kBlockVoxels / 4;
-    const int grid = (int)std::min<size_t>((n_vec4 + 255) / 256, (size_t)148 * 16);
-    reset_voxels_kernel<<<grid, 256, 0, s>>>(v, n_vec4);
+    const size_t n_voxels = (size_t)n_blocks * kBlockVoxels;
+    const size_t n_vec = n_voxels * (size_t)tsdf_bytes(v.storage) / 16;
+    const int grid = (int)std::min<size_t>((n_vec + 255) / 256, (size_t)148 * 16);
+    reset_voxels_kernel<<<grid, 256, 0, s>>>(v, n_voxels);
     return cudaGetLastError();
 }
 

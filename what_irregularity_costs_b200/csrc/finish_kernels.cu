@@ -63,71 +63,196 @@ __device__ __forceinline__ int accept_count(float w0, float cap, int n) {
     return room >= (double)n ? n : (int)room;
 }
 
-// ---- finish --------------------------------------------------------------
+// ---- finish ----------------------------------------------------------------
 
+// Four consecutive voxels of one storage mode, as registers.
+template <int S>
+struct Quad {
+    float w[4];  // weights
+    float t[4];  // FP32: tsdf sums; FP16U16: means
+    double d[4]; // FP64: tsdf sums
+};
+
+template <int S>
+__device__ __forceinline__ void load_quad(const DevVolume& v, size_t q4, Quad<S>& x) {
+    if constexpr (S == kStoreF32) {
+        const float4 w4 = reinterpret_cast<const float4*>(v.weight)[q4];
+        const float4 t4 = reinterpret_cast<const float4*>(v.tsdf)[q4];
+        x.w[0] = w4.x; x.w[1] = w4.y; x.w[2] = w4.z; x.w[3] = w4.w;
+        x.t[0] = t4.x; x.t[1] = t4.y; x.t[2] = t4.z; x.t[3] = t4.w;
+    } else if constexpr (S == kStoreF16U16) {
+        const ushort4 w4 = reinterpret_cast<const ushort4*>(v.weight)[q4];
+        const uint2 h = reinterpret_cast<const uint2*>(v.tsdf)[q4];
+        const __half2 h01 = *reinterpret_cast<const __half2*>(&h.x);
+        const __half2 h23 = *reinterpret_cast<const __half2*>(&h.y);
+        x.w[0] = (float)w4.x; x.w[1] = (float)w4.y; x.w[2] = (float)w4.z; x.w[3] = (float)w4.w;
+        x.t[0] = __low2float(h01); x.t[1] = __high2float(h01);
+        x.t[2] = __low2float(h23); x.t[3] = __high2float(h23);
+    } else {
+        const float4 w4 = reinterpret_cast<const float4*>(v.weight)[q4];
+        const double2 d01 = reinterpret_cast<const double2*>(v.tsdf)[2 * q4];
+        const double2 d23 = reinterpret_cast<const double2*>(v.tsdf)[2 * q4 + 1];
+        x.w[0] = w4.x; x.w[1] = w4.y; x.w[2] = w4.z; x.w[3] = w4.w;
+        x.d[0] = d01.x; x.d[1] = d01.y; x.d[2] = d23.x; x.d[3] = d23.y;
+    }
+}
+
+template <int S>
+__device__ __forceinline__ void store_quad(const DevVolume& v, size_t q4, const Quad<S>& x) {
+    if constexpr (S == kStoreF32) {
+        reinterpret_cast<float4*>(v.tsdf)[q4] = make_float4(x.t[0], x.t[1], x.t[2], x.t[3]);
+        reinterpret_cast<float4*>(v.weight)[q4] = make_float4(x.w[0], x.w[1], x.w[2], x.w[3]);
+        const float4 c = make_float4(__fmul_rn(128.0f, x.w[0]), __fmul_rn(128.0f, x.w[1]),
+                                     __fmul_rn(128.0f, x.w[2]), __fmul_rn(128.0f, x.w[3]));
+        __stcs(reinterpret_cast<float4*>(v.r) + q4, c);  // write-only: keep them out of L2
+        __stcs(reinterpret_cast<float4*>(v.g) + q4, c);
+        __stcs(reinterpret_cast<float4*>(v.b) + q4, c);
+    } else if constexpr (S == kStoreF16U16) {
+        const __half2 h01 = __floats2half2_rn(x.t[0], x.t[1]);
+        const __half2 h23 = __floats2half2_rn(x.t[2], x.t[3]);
+        uint2 h;
+        h.x = *reinterpret_cast<const unsigned*>(&h01);
+        h.y = *reinterpret_cast<const unsigned*>(&h23);
+        reinterpret_cast<uint2*>(v.tsdf)[q4] = h;
+        reinterpret_cast<ushort4*>(v.weight)[q4] =
+            make_ushort4((unsigned short)x.w[0], (unsigned short)x.w[1], (unsigned short)x.w[2],
+                         (unsigned short)x.w[3]);
+    } else {
+        reinterpret_cast<double2*>(v.tsdf)[2 * q4] = make_double2(x.d[0], x.d[1]);
+        reinterpret_cast<double2*>(v.tsdf)[2 * q4 + 1] = make_double2(x.d[2], x.d[3]);
+        reinterpret_cast<float4*>(v.weight)[q4] = make_float4(x.w[0], x.w[1], x.w[2], x.w[3]);
+    }
+}
+
+// New stored TSDF of a voxel with weight w0 before the batch that accepts
+// keep contributions whose normalised SDFs sum to fix * 2^-40.
+//   FP32: the sum gets the batch sum added with one rounding;
+//   FP16U16: the mean, (mean * w0 + sum) / (w0 + keep) in FP32, rounded to FP16
+//            (the caller rounds);
+//   FP64: the double sum.
+__device__ __forceinline__ float new_mean_f16(float mean0, float w0, int keep, long long fix) {
+    const float sum = __fadd_rn(__fmul_rn(mean0, w0), (float)((double)fix * kFixInv));
+    return __fdiv_rn(sum, __fadd_rn(w0, (float)keep));
+}
+
+template <int S>
+__device__ __forceinline__ void apply_voxel(Quad<S>& x, int q, int keep, long long fix) {
+    if constexpr (S == kStoreF32) {
+        x.t[q] = add_fix(x.t[q], fix);
+    } else if constexpr (S == kStoreF16U16) {
+        x.t[q] = new_mean_f16(x.t[q], x.w[q], keep, fix);
+    } else {
+        x.d[q] = x.d[q] + (double)fix * kFixInv;
+    }
+    x.w[q] = __fadd_rn(x.w[q], (float)keep);
+}
+
+// Per-CTA sum of a per-thread statistic, one global atomic per CTA (the
+// control counters share a line: per-warp atomics would serialise there).
+__device__ __forceinline__ void cta_add(int* smem_acc, int mine, int* global) {
+    const int w = __reduce_add_sync(0xffffffffu, mine);
+    if ((threadIdx.x & 31) == 0 && w) atomicAdd(smem_acc, w);
+    __syncthreads();
+    if (threadIdx.x == 0 && *smem_acc) atomicAdd(global, *smem_acc);
+}
+
+template <int S>
 __global__ void __launch_bounds__(kFinishThreads)
 finish_kernel(DevVolume v, UpdateScratch u) {
-    const int t = threadIdx.x;
+    __shared__ int s_updated;
+    const int t = threadIdx.x, lane = t & 31;
+    if (t == 0) s_updated = 0;
+    __syncthreads();
     const int n_touched = min(u.ctl->n_touched, v.pool_capacity);
     int updated = 0;
     for (int item = blockIdx.x; item < n_touched; item += gridDim.x) {
         const int32_t bi = u.touched[item];
         const size_t q4 = (size_t)bi * (kBlockVoxels / 4) + t;  // this thread's 4 voxels
         const uint4 c4 = reinterpret_cast<const uint4*>(u.vcnt)[q4];
-        if ((c4.x | c4.y | c4.z | c4.w) == 0u) continue;
-        const float4 w4 = reinterpret_cast<const float4*>(v.weight)[q4];
-        const float4 t4 = reinterpret_cast<const float4*>(v.tsdf)[q4];
-        const ulonglong2 a01 = reinterpret_cast<const ulonglong2*>(u.vacc)[2 * q4];
-        const ulonglong2 a23 = reinterpret_cast<const ulonglong2*>(u.vacc)[2 * q4 + 1];
+        const bool any = (c4.x | c4.y | c4.z | c4.w) != 0u;
+        if (!__any_sync(0xffffffffu, any)) continue;  // warp-uniform skip
+        Quad<S> x;
+        ulonglong2 a01 = make_ulonglong2(0ull, 0ull), a23 = a01;
+        if (any) {
+            load_quad<S>(v, q4, x);
+            a01 = reinterpret_cast<const ulonglong2*>(u.vacc)[2 * q4];
+            a23 = reinterpret_cast<const ulonglong2*>(u.vacc)[2 * q4 + 1];
+        }
         const uint32_t n[4] = {c4.x, c4.y, c4.z, c4.w};
-        const float w0[4] = {w4.x, w4.y, w4.z, w4.w};
-        float tn[4] = {t4.x, t4.y, t4.z, t4.w};
-        float wn[4];
         unsigned long long acc[4] = {a01.x, a01.y, a23.x, a23.y};
-        uint32_t cnt[4];
+        uint32_t cnt[4] = {0u, 0u, 0u, 0u};
+        int keepv[4] = {0, 0, 0, 0};
+        // Voxels crossing the cap reserve a group of their n records; the
+        // reservations of the warp are summed and made with one atomic each.
+        uint32_t my_records = 0u;
+        int my_cross = 0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (n[q] == 0u) continue;
+            keepv[q] = accept_count(x.w[q], v.weight_cap, (int)n[q]);
+            if ((uint32_t)keepv[q] != n[q]) {
+                my_records += n[q];
+                ++my_cross;
+            }
+        }
+        const unsigned crossers = __ballot_sync(0xffffffffu, my_cross > 0);
+        uint32_t rec_base = 0u;
+        int dv_base = 0;
+        if (crossers) {
+            uint32_t rec_incl = my_records;
+            int dv_incl = my_cross;
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t ry = __shfl_up_sync(0xffffffffu, rec_incl, o);
+                const int dy = __shfl_up_sync(0xffffffffu, dv_incl, o);
+                if (lane >= o) {
+                    rec_incl += ry;
+                    dv_incl += dy;
+                }
+            }
+            uint32_t rb = 0u;
+            int db = 0;
+            if (lane == 31) {
+                rb = atomicAdd(&u.ctl->x_used, rec_incl);
+                db = atomicAdd(&u.ctl->n_deferred, dv_incl);
+            }
+            rb = __shfl_sync(0xffffffffu, rb, 31);
+            db = __shfl_sync(0xffffffffu, db, 31);
+            rec_base = rb + rec_incl - my_records;
+            dv_base = db + dv_incl - my_cross;
+        }
+        if (!any) continue;  // no warp-synchronous step follows in this iteration
         bool crossing = false;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-            wn[q] = w0[q];
-            cnt[q] = 0u;
             if (n[q] == 0u) continue;
-            const int keep = accept_count(w0[q], v.weight_cap, (int)n[q]);
-            if ((uint32_t)keep == n[q]) {
-                tn[q] = add_fix(tn[q], (long long)acc[q]);
-                wn[q] = __fadd_rn(w0[q], (float)keep);
+            if ((uint32_t)keepv[q] == n[q]) {
+                apply_voxel<S>(x, q, keepv[q], (long long)acc[q]);
                 acc[q] = 0ull;
                 ++updated;
             } else {
-                // Crosses the cap: reserve a group for its records; the
-                // group pass fills it and the deferred kernel finishes it.
+                // Crosses the cap: its group is filled by the group pass and
+                // the voxel finished by the deferred kernel.
                 const uint32_t vi = (uint32_t)bi * kBlockVoxels + 4u * t + q;
-                const uint32_t base = atomicAdd(&u.ctl->x_used, n[q]);
-                const int d = atomicAdd(&u.ctl->n_deferred, 1);
-                if ((uint64_t)base + n[q] <= (uint64_t)u.record_cap && d < u.dvox_cap) {
-                    u.dvox[d] = make_int4((int)vi, (int)base, (int)n[q], keep);
-                    acc[q] = (unsigned long long)(base + 1u) << 32;  // low half: fill ticket
+                if ((uint64_t)rec_base + n[q] <= (uint64_t)u.record_cap && dv_base < u.dvox_cap) {
+                    u.dvox[dv_base] = make_int4((int)vi, (int)rec_base, (int)n[q], keepv[q]);
+                    acc[q] = (unsigned long long)(rec_base + 1u) << 32;  // low half: fill ticket
                     cnt[q] = n[q];
                 } else {
                     atomicOr(v.status, kStatusScratchOverflow);
                     acc[q] = 0ull;
                 }
+                rec_base += n[q];
+                ++dv_base;
                 crossing = true;
             }
         }
         if (crossing) u.blk_cross[bi] = u.tag;
-        reinterpret_cast<float4*>(v.tsdf)[q4] = make_float4(tn[0], tn[1], tn[2], tn[3]);
-        reinterpret_cast<float4*>(v.weight)[q4] = make_float4(wn[0], wn[1], wn[2], wn[3]);
-        const float4 c = make_float4(__fmul_rn(128.0f, wn[0]), __fmul_rn(128.0f, wn[1]),
-                                     __fmul_rn(128.0f, wn[2]), __fmul_rn(128.0f, wn[3]));
-        __stcs(reinterpret_cast<float4*>(v.r) + q4, c);  // write-only: keep them out of L2
-        __stcs(reinterpret_cast<float4*>(v.g) + q4, c);
-        __stcs(reinterpret_cast<float4*>(v.b) + q4, c);
+        store_quad<S>(v, q4, x);
         reinterpret_cast<uint4*>(u.vcnt)[q4] = make_uint4(cnt[0], cnt[1], cnt[2], cnt[3]);
         reinterpret_cast<ulonglong2*>(u.vacc)[2 * q4] = make_ulonglong2(acc[0], acc[1]);
         reinterpret_cast<ulonglong2*>(u.vacc)[2 * q4 + 1] = make_ulonglong2(acc[2], acc[3]);
     }
-    const unsigned total = __reduce_add_sync(0xffffffffu, (unsigned)updated);
-    if ((t & 31) == 0 && total) atomicAdd(&u.ctl->n_updated, (int)total);
+    cta_add(&s_updated, updated, &u.ctl->n_updated);
 }
 
 // ---- group ---------------------------------------------------------------
@@ -221,17 +346,24 @@ __device__ uint32_t radix_select(const DevVolume& v, const BatchArgs& a, const u
     return prefix;
 }
 
-// Canonical id and normalised SDF of the record in band slot `slot`: the
-// walk's arithmetic again for this one sample (same rounding).
+// Canonical id and normalised SDF (as 2^-40 fixed point) of the record in
+// band slot `slot`: the walk's arithmetic again for this one sample (same
+// rounding; the FP64 oracle's value in double).
+template <int S>
 __device__ __forceinline__ uint32_t slot_record(const DevVolume& v, const BatchArgs& a, uint32_t slot,
-                                                float& sdf_n) {
+                                                long long& fix) {
     const uint32_t n_steps = 2u * (uint32_t)v.steps + 1u;
     const uint32_t s = slot / (uint32_t)a.n, i = slot - s * (uint32_t)a.n;
     Ray r;
-    int vx, vy, vz;
+    int vx = 0, vy = 0, vz = 0;
     float sdf = 0.0f;
-    if (ray_setup(a, (int)i, r)) band_sample(v, a, r, (int)s - v.steps, vx, vy, vz, sdf);
-    sdf_n = fminf(fmaxf(__fmul_rn(sdf, v.inv_trunc), -1.0f), 1.0f);
+    const bool ok = ray_setup(a, (int)i, r);
+    if (ok) band_sample(v, a, r, (int)s - v.steps, vx, vy, vz, sdf);
+    if constexpr (S == kStoreF64) {
+        fix = ok ? to_fix(clamp_sdf_n_f64(sdf_f64(v, a, r.px, r.py, r.pz, vx, vy, vz), v.trunc)) : 0ll;
+    } else {
+        fix = to_fix(fminf(fmaxf(__fmul_rn(sdf, v.inv_trunc), -1.0f), 1.0f));
+    }
     return i * n_steps + s;
 }
 
@@ -240,9 +372,13 @@ __device__ __forceinline__ uint32_t slot_id(const DevVolume& v, const BatchArgs&
     return (slot - s * (uint32_t)a.n) * (2u * (uint32_t)v.steps + 1u) + s;
 }
 
+template <int S>
 __global__ void __launch_bounds__(kDeferThreads)
 deferred_kernel(DevVolume v, BatchArgs a, UpdateScratch u) {
     __shared__ uint32_t hist[kDeferWarps][256];
+    __shared__ int s_updated;
+    if (threadIdx.x == 0) s_updated = 0;
+    __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int nd = min(u.ctl->n_deferred, u.dvox_cap);
     int updated = 0;
@@ -255,16 +391,16 @@ deferred_kernel(DevVolume v, BatchArgs a, UpdateScratch u) {
         if (n <= 32 * kRankRegs) {
             // Up to 8 records per lane, ranked by id against all others.
             uint32_t id[kRankRegs];
-            float val[kRankRegs];
+            long long val[kRankRegs];
             int rank[kRankRegs];
             const int rows = (n + 31) / 32;
 #pragma unroll
             for (int r = 0; r < kRankRegs; ++r) {
                 const int k = r * 32 + lane;
                 id[r] = 0xFFFFFFFFu;
-                val[r] = 0.0f;
+                val[r] = 0ll;
                 rank[r] = 0;
-                if (r < rows && k < n) id[r] = slot_record(v, a, X[k], val[r]);
+                if (r < rows && k < n) id[r] = slot_record<S>(v, a, X[k], val[r]);
             }
 #pragma unroll
             for (int rr = 0; rr < kRankRegs; ++rr) {
@@ -279,40 +415,55 @@ deferred_kernel(DevVolume v, BatchArgs a, UpdateScratch u) {
             }
 #pragma unroll
             for (int r = 0; r < kRankRegs; ++r)
-                if (r < rows && r * 32 + lane < n && rank[r] < keep) fix += to_fix(val[r]);
+                if (r < rows && r * 32 + lane < n && rank[r] < keep) fix += val[r];
         } else {
             // The keep-th smallest id by radix select over the group's ids,
             // then the accepted records' values.
             const uint32_t last = radix_select(v, a, X, n, keep, hist[warp], lane);
             for (int k = lane; k < n; k += 32) {
                 if (slot_id(v, a, X[k]) > last) continue;
-                float val;
-                slot_record(v, a, X[k], val);
-                fix += to_fix(val);
+                long long val;
+                slot_record<S>(v, a, X[k], val);
+                fix += val;
             }
         }
         for (int o = 16; o > 0; o >>= 1) fix += __shfl_xor_sync(0xffffffffu, fix, o);
         if (lane == 0) {
-            const float wn = __fadd_rn(v.weight[vi], (float)keep);
-            v.tsdf[vi] = add_fix(v.tsdf[vi], fix);
-            v.weight[vi] = wn;
-            const float c = __fmul_rn(128.0f, wn);
-            v.r[vi] = c;
-            v.g[vi] = c;
-            v.b[vi] = c;
+            if constexpr (S == kStoreF32) {
+                const float wn = __fadd_rn(v.weight[vi], (float)keep);
+                v.tsdf[vi] = add_fix(v.tsdf[vi], fix);
+                v.weight[vi] = wn;
+                const float c = __fmul_rn(128.0f, wn);
+                v.r[vi] = c;
+                v.g[vi] = c;
+                v.b[vi] = c;
+            } else if constexpr (S == kStoreF16U16) {
+                unsigned short* w16 = reinterpret_cast<unsigned short*>(v.weight);
+                __half* h = reinterpret_cast<__half*>(v.tsdf);
+                const float w0 = (float)w16[vi];
+                h[vi] = __float2half_rn(new_mean_f16(__half2float(h[vi]), w0, keep, fix));
+                w16[vi] = (unsigned short)__fadd_rn(w0, (float)keep);
+            } else {
+                double* d = reinterpret_cast<double*>(v.tsdf);
+                d[vi] = d[vi] + (double)fix * kFixInv;
+                v.weight[vi] = __fadd_rn(v.weight[vi], (float)keep);
+            }
             u.vacc[vi] = 0ull;
             u.vcnt[vi] = 0u;
             ++updated;
         }
     }
-    const unsigned total = __reduce_add_sync(0xffffffffu, (unsigned)updated);
-    if (lane == 0 && total) atomicAdd(&u.ctl->n_updated, (int)total);
+    cta_add(&s_updated, updated, &u.ctl->n_updated);
 }
 
 }  // namespace
 
 cudaError_t launch_finish(const DevVolume& v, const UpdateScratch& u, int n_ctas, cudaStream_t s) {
-    finish_kernel<<<n_ctas, kFinishThreads, 0, s>>>(v, u);
+    switch (v.storage) {
+        case kStoreF16U16: finish_kernel<kStoreF16U16><<<n_ctas, kFinishThreads, 0, s>>>(v, u); break;
+        case kStoreF64: finish_kernel<kStoreF64><<<n_ctas, kFinishThreads, 0, s>>>(v, u); break;
+        default: finish_kernel<kStoreF32><<<n_ctas, kFinishThreads, 0, s>>>(v, u); break;
+    }
     return cudaGetLastError();
 }
 
@@ -327,7 +478,11 @@ cudaError_t launch_group(const DevVolume& v, const BatchArgs& a, const UpdateScr
 
 cudaError_t launch_deferred(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
                             int n_ctas, cudaStream_t s) {
-    deferred_kernel<<<n_ctas, kDeferThreads, 0, s>>>(v, a, u);
+    switch (v.storage) {
+        case kStoreF16U16: deferred_kernel<kStoreF16U16><<<n_ctas, kDeferThreads, 0, s>>>(v, a, u); break;
+        case kStoreF64: deferred_kernel<kStoreF64><<<n_ctas, kDeferThreads, 0, s>>>(v, a, u); break;
+        default: deferred_kernel<kStoreF32><<<n_ctas, kDeferThreads, 0, s>>>(v, a, u); break;
+    }
     return cudaGetLastError();
 }
 

@@ -18,6 +18,7 @@
 #pragma once
 
 #include <cstdint>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 namespace osn_b200 {
@@ -41,6 +42,22 @@ constexpr int kSpinLimit = 1 << 20;
 // Bits of the device status word.
 constexpr uint32_t kStatusSpinTimeout = 1u;
 constexpr uint32_t kStatusScratchOverflow = 2u;
+
+// Voxel storage modes (OSN_TSDF_STORAGE_* in include/osn_tsdf_b200.h).
+//   kStoreF32     the reference's layout: float weighted sums tsdf, weight,
+//                 r, g, b (20 bytes per voxel).
+//   kStoreF16U16  the mean normalised TSDF as FP16 and the weight as uint16
+//                 (4 bytes per voxel); the running average is formed in FP32
+//                 from the stored mean and the batch's exact sums. No colour
+//                 arrays: through the C ABI every contribution is grey (128),
+//                 so a voxel's mean colour is 128 wherever its weight is set.
+//   kStoreF64     the FP64 oracle: double TSDF sums computed from SDFs
+//                 evaluated in double at the same band samples, float weights
+//                 (integers, exact). No colour arrays.
+enum Storage : int { kStoreF32 = 0, kStoreF16U16 = 1, kStoreF64 = 2 };
+
+// The largest weight a uint16 voxel holds; the effective cap of kStoreF16U16.
+constexpr float kU16WeightMax = 65535.0f;
 
 struct HashEntry {
     long long key;
@@ -70,10 +87,38 @@ struct DevVolume {
     float inv_voxel;  // 1.0f / voxel_size, computed on the host (volume.cpp:148)
     float trunc;
     float inv_trunc;  // 1.0f / trunc (volume.cpp:203)
-    float weight_cap;
+    float weight_cap;  // effective cap: <= 0 disables (FP32/FP64); at most 65535 for uint16 weights
     int32_t steps;    // max(1, ceil(trunc * inv_voxel)) (volume.cpp:171)
     uint32_t* status;
+    int32_t storage;  // Storage
 };
+
+// Bytes per voxel of the tsdf and weight arrays of a storage mode.
+__host__ __device__ constexpr int tsdf_bytes(int storage) {
+    return storage == kStoreF16U16 ? 2 : storage == kStoreF64 ? 8 : 4;
+}
+__host__ __device__ constexpr int weight_bytes(int storage) { return storage == kStoreF16U16 ? 2 : 4; }
+
+// Weight of voxel i (read-only path: kernels that run after the volume's
+// weights were last written).
+template <int S>
+__device__ __forceinline__ float weight_at(const DevVolume& v, size_t i) {
+    if constexpr (S == kStoreF16U16)
+        return (float)__ldg(reinterpret_cast<const unsigned short*>(v.weight) + i);
+    else
+        return __ldg(v.weight + i);
+}
+
+// Mean normalised TSDF of voxel i given its weight w > 0.
+template <int S>
+__device__ __forceinline__ float mean_at(const DevVolume& v, size_t i, float w) {
+    if constexpr (S == kStoreF16U16)
+        return __half2float(reinterpret_cast<const __half*>(v.tsdf)[i]);
+    else if constexpr (S == kStoreF64)
+        return (float)(reinterpret_cast<const double*>(v.tsdf)[i] / (double)w);
+    else
+        return __fmul_rn(v.tsdf[i], __fdiv_rn(1.0f, w));  // marching_tets.cpp: sum * (1/w)
+}
 
 // One batch: camera origin and squared far cutoff (0 disables).
 struct BatchArgs {
@@ -163,6 +208,24 @@ __device__ __forceinline__ bool band_sample(const DevVolume& v, const BatchArgs&
         __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(ex, ex), __fmul_rn(ey, ey)), __fmul_rn(ez, ez)));
     sdf = __fsub_rn(r.dist, dv);
     return !(sdf < -v.trunc);
+}
+
+// The FP64 oracle's signed distance of the same band sample: the point's
+// distance and the voxel centre's distance evaluated in double.
+__device__ __forceinline__ double sdf_f64(const DevVolume& v, const BatchArgs& a, float px, float py,
+                                          float pz, int vx, int vy, int vz) {
+    const double dx = (double)px - (double)a.cam_x;
+    const double dy = (double)py - (double)a.cam_y;
+    const double dz = (double)pz - (double)a.cam_z;
+    const double vs = (double)v.voxel_size;
+    const double ex = ((double)vx + 0.5) * vs - (double)a.cam_x;
+    const double ey = ((double)vy + 0.5) * vs - (double)a.cam_y;
+    const double ez = ((double)vz + 0.5) * vs - (double)a.cam_z;
+    return sqrt(dx * dx + dy * dy + dz * dz) - sqrt(ex * ex + ey * ey + ez * ez);
+}
+
+__device__ __forceinline__ double clamp_sdf_n_f64(double sdf, float trunc) {
+    return fmin(fmax(sdf / (double)trunc, -1.0), 1.0);
 }
 
 // ---- lookups after allocation has completed --------------------------------
@@ -299,9 +362,10 @@ __device__ __forceinline__ InsertResult find_or_insert(const DevVolume& v, int32
 constexpr double kFixScale = 1099511627776.0;      // 2^40
 constexpr double kFixInv = 1.0 / 1099511627776.0;  // 2^-40
 
-__device__ __forceinline__ long long to_fix(float x) {
-    return __double2ll_rn((double)x * kFixScale);
-}
+// x * 2^40 is exact in float (a power-of-two scale of |x| <= 1), so rounding
+// it to an integer in float gives the same value as in double.
+__device__ __forceinline__ long long to_fix(float x) { return __float2ll_rn(x * 1099511627776.0f); }
+__device__ __forceinline__ long long to_fix(double x) { return __double2ll_rn(x * kFixScale); }
 
 __device__ __forceinline__ float add_fix(float t0, long long sum) {
     return __double2float_rn((double)t0 + (double)sum * kFixInv);

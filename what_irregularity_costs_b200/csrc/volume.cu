@@ -32,8 +32,10 @@ uint32_t next_pow2(uint32_t v) {  // cpp/src/volume.cpp:14-19
     } while (0)
 }  // namespace
 
-Volume::Volume(float voxel, int32_t pool, float trunc_m, float weight_cap, uint32_t hash_slots) {
+Volume::Volume(float voxel, int32_t pool, float trunc_m, float weight_cap, uint32_t hash_slots,
+               int storage) {
     if (!(voxel > 0.0f) || pool <= 0) return;
+    if (storage != kStoreF32 && storage != kStoreF16U16 && storage != kStoreF64) return;
     if (pool > kMaxPoolBlocks) {
         std::fprintf(stderr, "[osn_tsdf_b200] pool of %d blocks exceeds the supported %d\n", pool,
                      kMaxPoolBlocks);
@@ -44,7 +46,13 @@ Volume::Volume(float voxel, int32_t pool, float trunc_m, float weight_cap, uint3
     dv_.inv_voxel = 1.0f / voxel;
     dv_.trunc = trunc_m > 0.0f ? trunc_m : 4.0f * voxel;  // types.hpp:104-106
     dv_.inv_trunc = 1.0f / dv_.trunc;
-    dv_.weight_cap = weight_cap;
+    // uint16 weights saturate at 65535: that is the cap when none (or a larger
+    // one) is given.
+    dv_.storage = storage;
+    dv_.weight_cap = storage == kStoreF16U16
+                         ? (weight_cap > 0.0f ? std::min(weight_cap, kU16WeightMax) : kU16WeightMax)
+                         : weight_cap;
+    weight_cap_ = weight_cap;
     dv_.pool_capacity = pool;
     dv_.steps = std::max(1, (int32_t)std::ceil(dv_.trunc * dv_.inv_voxel));
     ok_ = alloc_device(hash_slots);
@@ -63,11 +71,16 @@ bool Volume::alloc_device(uint32_t hash_slots) {
     OSN_TRY(cudaMalloc(&dv_.drop_count, sizeof(unsigned long long)));
     OSN_TRY(cudaMalloc(&dv_.status, sizeof(uint32_t)));
     OSN_TRY(cudaMalloc(&dv_.block_coord, (size_t)dv_.pool_capacity * sizeof(BlockCoord)));
-    OSN_TRY(cudaMalloc(&dv_.tsdf, n_vox * sizeof(float)));
-    OSN_TRY(cudaMalloc(&dv_.weight, n_vox * sizeof(float)));
-    OSN_TRY(cudaMalloc(&dv_.r, n_vox * sizeof(float)));
-    OSN_TRY(cudaMalloc(&dv_.g, n_vox * sizeof(float)));
-    OSN_TRY(cudaMalloc(&dv_.b, n_vox * sizeof(float)));
+    const size_t t_bytes = n_vox * (size_t)tsdf_bytes(dv_.storage);
+    const size_t w_bytes = n_vox * (size_t)weight_bytes(dv_.storage);
+    const bool rgb = dv_.storage == kStoreF32;
+    OSN_TRY(cudaMalloc(&dv_.tsdf, t_bytes));
+    OSN_TRY(cudaMalloc(&dv_.weight, w_bytes));
+    if (rgb) {
+        OSN_TRY(cudaMalloc(&dv_.r, n_vox * sizeof(float)));
+        OSN_TRY(cudaMalloc(&dv_.g, n_vox * sizeof(float)));
+        OSN_TRY(cudaMalloc(&dv_.b, n_vox * sizeof(float)));
+    }
     OSN_TRY(cudaMalloc(&us_.vcnt, n_vox * sizeof(uint32_t)));
     OSN_TRY(cudaMalloc(&us_.vacc, n_vox * sizeof(unsigned long long)));
     OSN_TRY(cudaMalloc(&us_.blk_touch, (size_t)dv_.pool_capacity * sizeof(uint32_t)));
@@ -85,11 +98,13 @@ bool Volume::alloc_device(uint32_t hash_slots) {
     OSN_TRY(cudaMemsetAsync(dv_.block_count, 0, sizeof(int32_t), stream_));
     OSN_TRY(cudaMemsetAsync(dv_.drop_count, 0, sizeof(unsigned long long), stream_));
     OSN_TRY(cudaMemsetAsync(dv_.status, 0, sizeof(uint32_t), stream_));
-    OSN_TRY(cudaMemsetAsync(dv_.tsdf, 0, n_vox * sizeof(float), stream_));
-    OSN_TRY(cudaMemsetAsync(dv_.weight, 0, n_vox * sizeof(float), stream_));
-    OSN_TRY(cudaMemsetAsync(dv_.r, 0, n_vox * sizeof(float), stream_));
-    OSN_TRY(cudaMemsetAsync(dv_.g, 0, n_vox * sizeof(float), stream_));
-    OSN_TRY(cudaMemsetAsync(dv_.b, 0, n_vox * sizeof(float), stream_));
+    OSN_TRY(cudaMemsetAsync(dv_.tsdf, 0, t_bytes, stream_));
+    OSN_TRY(cudaMemsetAsync(dv_.weight, 0, w_bytes, stream_));
+    if (rgb) {
+        OSN_TRY(cudaMemsetAsync(dv_.r, 0, n_vox * sizeof(float), stream_));
+        OSN_TRY(cudaMemsetAsync(dv_.g, 0, n_vox * sizeof(float), stream_));
+        OSN_TRY(cudaMemsetAsync(dv_.b, 0, n_vox * sizeof(float), stream_));
+    }
     OSN_TRY(cudaMemsetAsync(us_.vcnt, 0, n_vox * sizeof(uint32_t), stream_));
     OSN_TRY(cudaMemsetAsync(us_.vacc, 0, n_vox * sizeof(unsigned long long), stream_));
     OSN_TRY(cudaMemsetAsync(us_.blk_touch, 0, (size_t)dv_.pool_capacity * sizeof(uint32_t), stream_));

@@ -63,7 +63,8 @@ struct UpdateScratch {
 
 class Volume {
 public:
-    Volume(float voxel, int32_t pool, float trunc_m, float weight_cap, uint32_t hash_slots);
+    Volume(float voxel, int32_t pool, float trunc_m, float weight_cap, uint32_t hash_slots,
+           int storage = kStoreF32);
     ~Volume();
     Volume(const Volume&) = delete;
     Volume& operator=(const Volume&) = delete;
@@ -73,7 +74,8 @@ public:
     cudaStream_t stream() const { return stream_; }
     float voxel_size() const { return dv_.voxel_size; }
     float trunc() const { return dv_.trunc; }
-    float weight_cap() const { return dv_.weight_cap; }
+    float weight_cap() const { return weight_cap_; }  // as given at creation
+    int storage() const { return dv_.storage; }
     int32_t pool() const { return dv_.pool_capacity; }
     uint32_t hash_mask() const { return dv_.hash_mask; }
 
@@ -108,6 +110,7 @@ private:
 
     bool ok_ = false;
     DevVolume dv_{};
+    float weight_cap_ = 0.0f;
     cudaStream_t stream_ = nullptr;
     UpdateScratch us_{};
     uint32_t update_tag_ = 0;  // number of the last update (block tags)

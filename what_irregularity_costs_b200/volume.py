@@ -19,6 +19,10 @@ from . import _lib
 
 KERNEL_NAMES = ["allocate", "band", "finish", "group", "deferred", "extract", "reset"]
 
+# Voxel storage modes (OSN_TSDF_STORAGE_* in include/osn_tsdf_b200.h).
+STORAGE_FP32, STORAGE_FP16_U16, STORAGE_FP64 = 0, 1, 2
+STORAGE_NAMES = {STORAGE_FP32: "fp32", STORAGE_FP16_U16: "fp16_u16", STORAGE_FP64: "fp64"}
+
 
 def _addr(x) -> int:
     """Device address of a CUDA tensor (or an int address)."""
@@ -66,10 +70,11 @@ class CudaVolume:
     """One hash-blocked TSDF volume on the GPU (drop-in for the reference's CudaVolume)."""
 
     def __init__(self, voxel_size_m: float, pool_capacity_blocks: int, trunc_m: float = -1.0,
-                 weight_cap: float = 32.0, hash_slots: int = 0):
+                 weight_cap: float = 32.0, hash_slots: int = 0, storage: int = STORAGE_FP32):
         self.lib = _lib.load()
+        self.storage = int(storage)
         self.h = self.lib.osn_tsdf_cuda_create_ex(voxel_size_m, pool_capacity_blocks, trunc_m,
-                                                  weight_cap, hash_slots, 0)
+                                                  weight_cap, hash_slots, self.storage)
         if not self.h:
             raise ValueError("osn_tsdf_cuda_create rejected the parameters or the device "
                              "allocation failed")
@@ -236,8 +241,30 @@ class CudaVolume:
     def coord_set(self) -> set:
         return set(map(tuple, self.coords().tolist()))
 
+    def means(self):
+        """(coords, mean TSDF, weight) in any storage mode: (block_count, 512) float64
+        arrays; the mean is 0 where the weight is 0."""
+        n = min(self.block_count(), self.device_view().pool_capacity)
+        view = self.device_view()
+        coords = self.coords()
+        if n <= 0:
+            z = np.zeros((0, 512), dtype=np.float64)
+            return coords, z, z.copy()
+        if self.storage == STORAGE_FP16_U16:
+            mean = device_tensor(view.tsdf, (n, 512), "<f2").cpu().numpy().astype(np.float64)
+            w = device_tensor(view.weight, (n, 512), "<u2").cpu().numpy().astype(np.float64)
+        else:
+            typ = "<f8" if self.storage == STORAGE_FP64 else "<f4"
+            t = device_tensor(view.tsdf, (n, 512), typ).cpu().numpy().astype(np.float64)
+            w = device_tensor(view.weight, (n, 512), "<f4").cpu().numpy().astype(np.float64)
+            mean = np.divide(t, w, out=np.zeros_like(t), where=w > 0)
+        return coords, mean, w
+
     def voxels(self):
-        """(coords, tsdf, weight, r, g, b): the five arrays as (block_count, 512) float32."""
+        """(coords, tsdf, weight, r, g, b): the five arrays as (block_count, 512) float32
+        (FP32 storage: the reference's weighted sums)."""
+        if self.storage != STORAGE_FP32:
+            raise ValueError("voxels() reads the FP32 layout; use means() for other storage")
         n = min(self.block_count(), self.device_view().pool_capacity)
         view = self.device_view()
         out = [self.coords()]
