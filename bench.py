@@ -376,10 +376,24 @@ def run_ours(args):
     e2e_ms = max_over_ranks(e0.elapsed_time(e1), dist, torch)
     e2e_value = frames_total / (e2e_ms / 1e3)
 
-    # -- one instrumented step: per-kernel times and stage statistics ---------
+    # -- one instrumented step: per-kernel CUDA-event times (every launch of
+    # the volume bracketed on its stream; no synchronisation between frames)
     vol.set_timing(True)
     vol.kernel_times()  # flush
     base = vol.kernel_times()
+    vol.reset()
+    for k in range(N_FRAMES):
+        a, b = int(offsets[k]), int(offsets[k + 1])
+        vol.integrate(d_all[a:b], cams[k])
+    # Allocation alone (allocate_blocks), for the allocate Mrays/s figure.
+    vol.reset()
+    for k in range(N_FRAMES):
+        a, b = int(offsets[k]), int(offsets[k + 1])
+        vol.allocate_blocks(d_all[a:b], cams[k])
+    times = vol.kernel_times()
+    vol.set_timing(False)
+    per_kernel = {k: (times[k][0] - base[k][0], times[k][1] - base[k][1]) for k in KERNEL_NAMES}
+    # -- stage statistics of every frame (read back per frame; untimed)
     vol.reset()
     updated, records, touched, crossing = [], [], [], []
     for k in range(N_FRAMES):
@@ -390,16 +404,8 @@ def run_ours(args):
         records.append(st["records"])
         touched.append(st["touched_blocks"])
         crossing.append(st["crossing_voxels"])
-    # Allocation alone (allocate_blocks), for the allocate Mrays/s figure.
-    vol.reset()
-    for k in range(N_FRAMES):
-        a, b = int(offsets[k]), int(offsets[k + 1])
-        vol.allocate_blocks(d_all[a:b], cams[k])
-    times = vol.kernel_times()
-    vol.set_timing(False)
-    per_kernel = {k: (times[k][0] - base[k][0], times[k][1] - base[k][1]) for k in KERNEL_NAMES}
-    integrate_kernels = ("band", "finish", "group", "deferred")
-    launches_per_step = sum(per_kernel[k][1] for k in integrate_kernels) // 1
+    integrate_kernels = ("band", "finish", "group", "values", "deferred")
+    launches_per_step = sum(per_kernel[k][1] for k in integrate_kernels) + 2  # + reset's two
     dominant = max(integrate_kernels, key=lambda k: per_kernel[k][0])
 
     peak, peak_kind = measured_peak()
@@ -413,6 +419,7 @@ def run_ours(args):
         "band": 12 * n_points + 4 * n_slots + 16 * n_rec,
         "finish": n_touch * 512 * (16 + 36),   # read cnt,w,t,sum; write t,w,r,g,b,cnt,sum
         "group": 4 * n_slots,
+        "values": 0,
         "deferred": 0,
     }
     # Update as the reference scopes it: positions + tsdf/weight tiles of the
@@ -461,7 +468,7 @@ def run_ours(args):
             "reference_gpu_arm": a3,
             "e2e": {"value": e2e_value, "unit": "frames/s",
                     "h2d_bytes_per_step": int(all_pts.nbytes), "d2h_bytes_per_step": 16},
-            "gpu_launches": int(launches_per_step * args.steps + N_FRAMES * args.steps),
+            "gpu_launches": int(launches_per_step * args.steps),
             "clocks": clocks.summary(),
             "alloc_mrays_per_s": n_points / t_alloc / 1e6 if t_alloc else None,
             "update_gbps": update_alg_bytes / t_update / 1e9 if t_update else None,

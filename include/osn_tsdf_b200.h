@@ -187,7 +187,7 @@ int32_t osn_tsdf_cuda_last_update_stats(const OsnTsdfCudaVolume* v, int64_t* out
  * (no allocation during stream capture), serving loops that budget device
  * memory up front, latency-critical threads that cannot absorb the implied
  * synchronisation -- call this instead. Same results as update_voxels.
- * Its scratch is one fixed 32 MiB array inside the library, held on every
+ * Its scratch is one fixed 48 MiB array inside the library, held on every
  * GPU where the library's code is loaded until the process exits, and shared
  * by all calls: calls whose work overlaps on the GPU race and must be
  * serialised. The first call on a device resolves the array's address and
@@ -203,7 +203,8 @@ int32_t osn_tsdf_cuda_update_voxels_noalloc(OsnTsdfCudaVolume* v, const float* d
  * waits for) the accumulated per-kernel milliseconds and launch counts.
  * Kernel ids: 0 allocate, 1 band (count-and-sum walk; allocates too in
  * integrate), 2 finish (per touched block), 3 group (records of voxels that
- * cross the cap), 4 deferred (ordered cap selection), 5 extract, 6 reset.
+ * cross the cap), 4 deferred (ordered cap selection), 5 extract, 6 reset,
+ * 7 values (ids and signed distances of the grouped records).
  * Returns the number of ids written. */
 int32_t osn_tsdf_cuda_set_timing(OsnTsdfCudaVolume* v, int32_t enabled);
 int32_t osn_tsdf_cuda_kernel_times(OsnTsdfCudaVolume* v, double* ms, int64_t* launches,

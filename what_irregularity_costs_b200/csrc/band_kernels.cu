@@ -166,6 +166,7 @@ band_kernel(DevVolume v, BatchArgs a, UpdateScratch u, unsigned long long* hist,
         s_counted = 0u;
     }
     __syncthreads();
+    launch_dependents();  // the finish pass may be scheduled as CTAs retire
 
     // The point of the next tile is loaded one tile ahead.
     float nx = 0.0f, ny = 0.0f, nz = 0.0f;

@@ -27,20 +27,26 @@
 //              to zero. A voxel that crosses the cap inside the batch
 //              reserves a group of n deferred records instead and its block
 //              is tagged.
-//   group      one pass over the records of the batch: a record of a tagged
-//              block whose voxel reserved a group puts its slot in the next
-//              place of the group (a few percent of the records).
-//   deferred   one warp per crossing voxel: each lane recomputes the
-//              canonical id and normalised SDF of its records from their
-//              points (the walk's arithmetic, same rounding), then the warp
-//              selects the keep records with the smallest ids (ranking in
-//              registers up to 256 records, a radix select of the keep-th id
-//              beyond that) and finishes the voxel.
+//              Crossing voxels go to one of two lists: small groups (at most
+//              kLaneRecords records, most of them) and large ones.
+//   group      one pass over the records of the batch, eight per thread: a
+//              record of a tagged block whose voxel reserved a group takes
+//              the next place of the group (a few percent of the records).
+//   values     one thread per grouped record: its canonical id and
+//              normalised SDF, recomputed from its point (the walk's
+//              arithmetic, same rounding).
+//   deferred   selects the keep records with the smallest ids of every
+//              crossing voxel and finishes it: one half-warp per small group
+//              (one record per lane, shuffle ranking), one warp per large group
+//              (register ranking up to 256 records, a radix select of the
+//              keep-th id beyond that).
 //
 // Sums are 64-bit fixed point added to the stored sum with one rounding, so
 // results do not depend on the order in which threads meet the records:
 // repeated runs are bit-identical, and a voxel with one contribution per
 // batch gets exactly the reference's fl(tsdf + sdf_n).
+#include <mutex>
+
 #include "volume.h"
 
 namespace osn_b200 {
@@ -48,7 +54,7 @@ namespace {
 
 constexpr int kFinishThreads = 128;  // 4 voxels per thread, one block per CTA pass
 constexpr int kGroupThreads = 256;
-constexpr int kDeferThreads = 256;
+constexpr int kDeferThreads = 128;
 constexpr int kDeferWarps = kDeferThreads / 32;
 constexpr int kRankRegs = 8;  // crossing voxels of up to 256 records are ranked in registers
 
@@ -156,6 +162,122 @@ __device__ __forceinline__ void cta_add(int* smem_acc, int mine, int* global) {
     if (threadIdx.x == 0 && *smem_acc) atomicAdd(global, *smem_acc);
 }
 
+// One touched block's quad of voxels, its arrays already loaded: finish
+// the voxels that accept all their records, reserve groups for those that
+// cross the cap. Warp-synchronous (all lanes of the warp call it).
+template <int S>
+__device__ __forceinline__ void finish_quad(const DevVolume& v, const UpdateScratch& u, int32_t bi,
+                                            size_t q4, int t, int lane, const uint4 c4, Quad<S>& x,
+                                            const ulonglong2 a01, const ulonglong2 a23, int& updated) {
+    const bool any = (c4.x | c4.y | c4.z | c4.w) != 0u;
+    if (!__any_sync(0xffffffffu, any)) return;  // warp-uniform skip
+    const uint32_t n[4] = {c4.x, c4.y, c4.z, c4.w};
+    unsigned long long acc[4] = {a01.x, a01.y, a23.x, a23.y};
+    uint32_t cnt[4] = {0u, 0u, 0u, 0u};
+    int keepv[4] = {0, 0, 0, 0};
+    // Voxels crossing the cap reserve a group of their n records and an
+    // entry in the small (n <= kLaneRecords) or large list; the warp's
+    // reservations are summed and made with one atomic per counter.
+    uint32_t my_records = 0u;
+    uint32_t my_small = 0u, my_large = 0u;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        if (n[q] == 0u) continue;
+        keepv[q] = accept_count(x.w[q], v.weight_cap, (int)n[q]);
+        if (keepv[q] != 0 && (uint32_t)keepv[q] != n[q]) {
+            my_records += n[q];
+            if (n[q] <= (uint32_t)kLaneRecords) ++my_small;
+            else ++my_large;
+        }
+    }
+    const unsigned crossers = __ballot_sync(0xffffffffu, my_records > 0u);
+    uint32_t rec_base = 0u, small_at = 0u, large_at = 0u;
+    bool lists_ok = true;
+    if (crossers) {
+        uint32_t rec_incl = my_records, s_incl = my_small, l_incl = my_large;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t ry = __shfl_up_sync(0xffffffffu, rec_incl, o);
+            const uint32_t sy = __shfl_up_sync(0xffffffffu, s_incl, o);
+            const uint32_t ly = __shfl_up_sync(0xffffffffu, l_incl, o);
+            if (lane >= o) {
+                rec_incl += ry;
+                s_incl += sy;
+                l_incl += ly;
+            }
+        }
+        uint32_t rb = 0u;
+        unsigned long long lb = 0ull;
+        if (lane == 31) {
+            rb = atomicAdd(&u.ctl->x_used, rec_incl);
+            lb = atomicAdd(&u.ctl->def_lists, (unsigned long long)s_incl |
+                                                  ((unsigned long long)l_incl << 32));
+        }
+        rb = __shfl_sync(0xffffffffu, rb, 31);
+        lb = __shfl_sync(0xffffffffu, lb, 31);
+        const uint32_t s_tot = __shfl_sync(0xffffffffu, s_incl, 31);
+        const uint32_t l_tot = __shfl_sync(0xffffffffu, l_incl, 31);
+        rec_base = rb + rec_incl - my_records;
+        const uint64_t s0 = lb & 0xFFFFFFFFull, l0 = lb >> 32;
+        small_at = (uint32_t)s0 + s_incl - my_small;
+        large_at = (uint32_t)l0 + l_incl - my_large;
+        // The lists grow towards each other: entries written under a
+        // reservation that fits never overlap later ones.
+        lists_ok = s0 + s_tot + l0 + l_tot <= (uint64_t)u.dvox_cap;
+    }
+    if (!any) return;  // no warp-synchronous step follows
+    bool crossing = false;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        if (n[q] == 0u) continue;
+        if ((uint32_t)keepv[q] == n[q] || keepv[q] == 0) {
+            // All accepted (or none: the voxel was full before the batch).
+            if (keepv[q]) {
+                apply_voxel<S>(x, q, keepv[q], (long long)acc[q]);
+                ++updated;
+            }
+            acc[q] = 0ull;
+        } else {
+            // Crosses the cap: its group is filled by the group pass and
+            // the voxel finished by the deferred kernel.
+            const uint32_t vi = (uint32_t)bi * kBlockVoxels + 4u * t + q;
+            const bool small = n[q] <= (uint32_t)kLaneRecords;
+            const int entry = small ? (int)small_at : u.dvox_cap - 1 - (int)large_at;
+            if ((uint64_t)rec_base + n[q] <= (uint64_t)u.record_cap && lists_ok) {
+                u.dvox[entry] = make_int4((int)vi, (int)rec_base, (int)n[q], keepv[q]);
+                acc[q] = (unsigned long long)(rec_base + 1u) << 32;  // low half: fill ticket
+                cnt[q] = n[q];
+            } else {
+                // Out of scratch (the status word says so): a reserved
+                // list entry still gets an empty group, never a stale one.
+                if (lists_ok) u.dvox[entry] = make_int4((int)vi, 0, 0, 0);
+                atomicOr(v.status, kStatusScratchOverflow);
+                acc[q] = 0ull;
+            }
+            rec_base += n[q];
+            if (small) ++small_at;
+            else ++large_at;
+            crossing = true;
+        }
+    }
+    if (crossing) u.blk_cross[bi] = u.tag;
+    store_quad<S>(v, q4, x);
+    reinterpret_cast<uint4*>(u.vcnt)[q4] = make_uint4(cnt[0], cnt[1], cnt[2], cnt[3]);
+    reinterpret_cast<ulonglong2*>(u.vacc)[2 * q4] = make_ulonglong2(acc[0], acc[1]);
+    reinterpret_cast<ulonglong2*>(u.vacc)[2 * q4 + 1] = make_ulonglong2(acc[2], acc[3]);
+}
+
+template <int S>
+__device__ __forceinline__ void load_item(const DevVolume& v, const UpdateScratch& u, size_t q4,
+                                          uint4& c4, Quad<S>& x, ulonglong2& a01, ulonglong2& a23) {
+    c4 = reinterpret_cast<const uint4*>(u.vcnt)[q4];
+    load_quad<S>(v, q4, x);
+    a01 = reinterpret_cast<const ulonglong2*>(u.vacc)[2 * q4];
+    a23 = reinterpret_cast<const ulonglong2*>(u.vacc)[2 * q4 + 1];
+}
+
+// Two touched blocks per CTA iteration: the indices of both, then every
+// array of both, are in flight together (each CTA pass is two dependent
+// round trips, whatever the number of blocks it covers).
 template <int S>
 __global__ void __launch_bounds__(kFinishThreads)
 finish_kernel(DevVolume v, UpdateScratch u) {
@@ -163,150 +285,159 @@ finish_kernel(DevVolume v, UpdateScratch u) {
     const int t = threadIdx.x, lane = t & 31;
     if (t == 0) s_updated = 0;
     __syncthreads();
+    launch_dependents();
+    grid_dependency_wait();
     const int n_touched = min(u.ctl->n_touched, v.pool_capacity);
     int updated = 0;
-    for (int item = blockIdx.x; item < n_touched; item += gridDim.x) {
-        const int32_t bi = u.touched[item];
-        const size_t q4 = (size_t)bi * (kBlockVoxels / 4) + t;  // this thread's 4 voxels
-        const uint4 c4 = reinterpret_cast<const uint4*>(u.vcnt)[q4];
-        const bool any = (c4.x | c4.y | c4.z | c4.w) != 0u;
-        if (!__any_sync(0xffffffffu, any)) continue;  // warp-uniform skip
-        Quad<S> x;
-        ulonglong2 a01 = make_ulonglong2(0ull, 0ull), a23 = a01;
-        if (any) {
-            load_quad<S>(v, q4, x);
-            a01 = reinterpret_cast<const ulonglong2*>(u.vacc)[2 * q4];
-            a23 = reinterpret_cast<const ulonglong2*>(u.vacc)[2 * q4 + 1];
-        }
-        const uint32_t n[4] = {c4.x, c4.y, c4.z, c4.w};
-        unsigned long long acc[4] = {a01.x, a01.y, a23.x, a23.y};
-        uint32_t cnt[4] = {0u, 0u, 0u, 0u};
-        int keepv[4] = {0, 0, 0, 0};
-        // Voxels crossing the cap reserve a group of their n records; the
-        // reservations of the warp are summed and made with one atomic each.
-        uint32_t my_records = 0u;
-        int my_cross = 0;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            if (n[q] == 0u) continue;
-            keepv[q] = accept_count(x.w[q], v.weight_cap, (int)n[q]);
-            if ((uint32_t)keepv[q] != n[q]) {
-                my_records += n[q];
-                ++my_cross;
-            }
-        }
-        const unsigned crossers = __ballot_sync(0xffffffffu, my_cross > 0);
-        uint32_t rec_base = 0u;
-        int dv_base = 0;
-        if (crossers) {
-            uint32_t rec_incl = my_records;
-            int dv_incl = my_cross;
-            for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t ry = __shfl_up_sync(0xffffffffu, rec_incl, o);
-                const int dy = __shfl_up_sync(0xffffffffu, dv_incl, o);
-                if (lane >= o) {
-                    rec_incl += ry;
-                    dv_incl += dy;
-                }
-            }
-            uint32_t rb = 0u;
-            int db = 0;
-            if (lane == 31) {
-                rb = atomicAdd(&u.ctl->x_used, rec_incl);
-                db = atomicAdd(&u.ctl->n_deferred, dv_incl);
-            }
-            rb = __shfl_sync(0xffffffffu, rb, 31);
-            db = __shfl_sync(0xffffffffu, db, 31);
-            rec_base = rb + rec_incl - my_records;
-            dv_base = db + dv_incl - my_cross;
-        }
-        if (!any) continue;  // no warp-synchronous step follows in this iteration
-        bool crossing = false;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            if (n[q] == 0u) continue;
-            if ((uint32_t)keepv[q] == n[q]) {
-                apply_voxel<S>(x, q, keepv[q], (long long)acc[q]);
-                acc[q] = 0ull;
-                ++updated;
-            } else {
-                // Crosses the cap: its group is filled by the group pass and
-                // the voxel finished by the deferred kernel.
-                const uint32_t vi = (uint32_t)bi * kBlockVoxels + 4u * t + q;
-                if ((uint64_t)rec_base + n[q] <= (uint64_t)u.record_cap && dv_base < u.dvox_cap) {
-                    u.dvox[dv_base] = make_int4((int)vi, (int)rec_base, (int)n[q], keepv[q]);
-                    acc[q] = (unsigned long long)(rec_base + 1u) << 32;  // low half: fill ticket
-                    cnt[q] = n[q];
-                } else {
-                    atomicOr(v.status, kStatusScratchOverflow);
-                    acc[q] = 0ull;
-                }
-                rec_base += n[q];
-                ++dv_base;
-                crossing = true;
-            }
-        }
-        if (crossing) u.blk_cross[bi] = u.tag;
-        store_quad<S>(v, q4, x);
-        reinterpret_cast<uint4*>(u.vcnt)[q4] = make_uint4(cnt[0], cnt[1], cnt[2], cnt[3]);
-        reinterpret_cast<ulonglong2*>(u.vacc)[2 * q4] = make_ulonglong2(acc[0], acc[1]);
-        reinterpret_cast<ulonglong2*>(u.vacc)[2 * q4 + 1] = make_ulonglong2(acc[2], acc[3]);
+    for (int ia = blockIdx.x; ia < n_touched; ia += 2 * gridDim.x) {
+        const int ib = ia + gridDim.x;
+        const bool has_b = ib < n_touched;  // uniform across the CTA
+        const int32_t ba = u.touched[ia];
+        const int32_t bb = has_b ? u.touched[ib] : ba;
+        const size_t qa = (size_t)ba * (kBlockVoxels / 4) + t;  // this thread's 4 voxels
+        const size_t qb = (size_t)bb * (kBlockVoxels / 4) + t;
+        uint4 ca, cb;
+        Quad<S> xa, xb;
+        ulonglong2 a01, a23, b01, b23;
+        load_item<S>(v, u, qa, ca, xa, a01, a23);
+        if (has_b) load_item<S>(v, u, qb, cb, xb, b01, b23);
+        finish_quad<S>(v, u, ba, qa, t, lane, ca, xa, a01, a23, updated);
+        if (has_b) finish_quad<S>(v, u, bb, qb, t, lane, cb, xb, b01, b23, updated);
     }
     cta_add(&s_updated, updated, &u.ctl->n_updated);
 }
 
 // ---- group ---------------------------------------------------------------
 
+// Canonical id and normalised SDF (2^-40 fixed point) of the record in band
+// slot `slot`: the walk's arithmetic again for this one sample (same
+// rounding; the FP64 oracle's value in double).
+template <int S>
+__device__ __forceinline__ uint32_t slot_record(const DevVolume& v, const BatchArgs& a, uint32_t slot,
+                                                long long& fix) {
+    const uint32_t n_steps = 2u * (uint32_t)v.steps + 1u;
+    const uint32_t s = slot / (uint32_t)a.n, i = slot - s * (uint32_t)a.n;
+    Ray r;
+    int vx = 0, vy = 0, vz = 0;
+    float sdf = 0.0f;
+    const bool ok = ray_setup(a, (int)i, r);
+    if (ok) band_sample(v, a, r, (int)s - v.steps, vx, vy, vz, sdf);
+    if constexpr (S == kStoreF64) {
+        fix = ok ? to_fix(clamp_sdf_n_f64(sdf_f64(v, a, r.px, r.py, r.pz, vx, vy, vz), v.trunc)) : 0ll;
+    } else {
+        fix = to_fix(fminf(fmaxf(__fmul_rn(sdf, v.inv_trunc), -1.0f), 1.0f));
+    }
+    return i * n_steps + s;
+}
+
+constexpr int kGroupPerThread = 8;  // records per thread (two 128-bit loads)
+
 __global__ void __launch_bounds__(kGroupThreads)
 group_kernel(UpdateScratch u, uint32_t n_slots) {
-    if (u.ctl->n_deferred == 0) return;  // no voxel crossed the cap in this batch
-    // Four records per thread, phase by phase: the block-tag gathers of all
-    // four in flight together, then the (rare) records of crossing voxels
-    // take the next place of their voxel's group.
-    const uint32_t q = blockIdx.x * kGroupThreads + threadIdx.x;  // quad of slots
-    if (4u * q >= n_slots) return;
-    uint32_t vi[4];
-    if (4u * q + 3u < n_slots) {
-        const uint4 r = __ldcs(reinterpret_cast<const uint4*>(u.records) + q);
-        vi[0] = r.x;
-        vi[1] = r.y;
-        vi[2] = r.z;
-        vi[3] = r.w;
+    launch_dependents();
+    grid_dependency_wait();
+    if (u.ctl->def_lists == 0ull) return;  // no voxel crossed the cap in this batch
+    // Eight consecutive band slots per thread (same step, neighbouring points,
+    // so mostly the same block): the block-tag gathers of distinct blocks in
+    // flight together, then the (rare) records of crossing voxels take the
+    // next place of their voxel's group with their band slot.
+    const uint32_t first = (blockIdx.x * kGroupThreads + threadIdx.x) * kGroupPerThread;
+    if (first >= n_slots) return;
+    uint32_t vi[kGroupPerThread];
+    if (first + kGroupPerThread <= n_slots) {
+        const uint4 r0 = __ldcs(reinterpret_cast<const uint4*>(u.records + first));
+        const uint4 r1 = __ldcs(reinterpret_cast<const uint4*>(u.records + first) + 1);
+        vi[0] = r0.x; vi[1] = r0.y; vi[2] = r0.z; vi[3] = r0.w;
+        vi[4] = r1.x; vi[5] = r1.y; vi[6] = r1.z; vi[7] = r1.w;
     } else {
 #pragma unroll
-        for (uint32_t m = 0; m < 4u; ++m) vi[m] = 4u * q + m < n_slots ? u.records[4u * q + m] : kNoVoxel;
+        for (int m = 0; m < kGroupPerThread; ++m)
+            vi[m] = first + m < n_slots ? u.records[first + m] : kNoVoxel;
     }
-    bool cand[4];
+    uint32_t tag[kGroupPerThread];
+    bool same[kGroupPerThread];  // same block as the previous slot: reuse its tag
 #pragma unroll
-    for (int m = 0; m < 4; ++m)
-        cand[m] = vi[m] != kNoVoxel && u.blk_cross[vi[m] / kBlockVoxels] == u.tag;
-    uint32_t hi[4];
+    for (int m = 0; m < kGroupPerThread; ++m) {
+        const uint32_t blk = vi[m] / kBlockVoxels;
+        same[m] = m > 0 && vi[m] != kNoVoxel && vi[m - 1] != kNoVoxel && vi[m - 1] / kBlockVoxels == blk;
+        tag[m] = (vi[m] == kNoVoxel || same[m]) ? 0u : u.blk_cross[blk];
+    }
 #pragma unroll
-    for (int m = 0; m < 4; ++m) hi[m] = cand[m] ? (uint32_t)(u.vacc[vi[m]] >> 32) : 0u;
+    for (int m = 1; m < kGroupPerThread; ++m)
+        if (same[m]) tag[m] = tag[m - 1];
+    uint32_t hi[kGroupPerThread];
 #pragma unroll
-    for (int m = 0; m < 4; ++m) {
+    for (int m = 0; m < kGroupPerThread; ++m)
+        hi[m] = (vi[m] != kNoVoxel && tag[m] == u.tag) ? (uint32_t)(u.vacc[vi[m]] >> 32) : 0u;
+#pragma unroll
+    for (int m = 0; m < kGroupPerThread; ++m) {
         if (hi[m] == 0u) continue;  // not a voxel that reserved a group
-        const uint32_t t = (uint32_t)atomicAdd(&u.vacc[vi[m]], 1ull);
-        if (t < u.vcnt[vi[m]]) u.deferred[(size_t)(hi[m] - 1u) + t] = 4u * q + m;
+        const uint32_t tk = (uint32_t)atomicAdd(&u.vacc[vi[m]], 1ull);
+        if (tk < u.vcnt[vi[m]]) u.deferred[(size_t)(hi[m] - 1u) + tk] = first + m;
         else atomicOr(u.status, kStatusScratchOverflow);  // state left by a failed update
+    }
+}
+
+// ---- values --------------------------------------------------------------
+
+// One thread per grouped record: its band slot becomes its canonical id and
+// its normalised SDF (recomputed from the point, the walk's arithmetic with
+// the same rounding; the FP64 oracle's value in double).
+template <int S>
+__global__ void __launch_bounds__(kGroupThreads)
+values_kernel(DevVolume v, BatchArgs a, UpdateScratch u) {
+    launch_dependents();
+    grid_dependency_wait();
+    if (u.ctl->def_lists == 0ull) return;
+    const uint32_t n = (uint32_t)min((long long)u.ctl->x_used, (long long)u.record_cap);
+    for (uint32_t k = blockIdx.x * kGroupThreads + threadIdx.x; k < n; k += gridDim.x * kGroupThreads) {
+        long long fix;
+        const uint32_t id = slot_record<S>(v, a, u.deferred[k], fix);
+        u.deferred[k] = id;
+        u.deferred_fix[k] = fix;
     }
 }
 
 // ---- deferred ------------------------------------------------------------
 
+// Finish a cap-crossing voxel: keep contributions accepted, their values
+// summing to fix * 2^-40.
+template <int S>
+__device__ __forceinline__ void finish_voxel(const DevVolume& v, const UpdateScratch& u, uint32_t vi,
+                                             int keep, long long fix) {
+    if constexpr (S == kStoreF32) {
+        const float wn = __fadd_rn(v.weight[vi], (float)keep);
+        v.tsdf[vi] = add_fix(v.tsdf[vi], fix);
+        v.weight[vi] = wn;
+        const float c = __fmul_rn(128.0f, wn);
+        v.r[vi] = c;
+        v.g[vi] = c;
+        v.b[vi] = c;
+    } else if constexpr (S == kStoreF16U16) {
+        unsigned short* w16 = reinterpret_cast<unsigned short*>(v.weight);
+        __half* h = reinterpret_cast<__half*>(v.tsdf);
+        const float w0 = (float)w16[vi];
+        h[vi] = __float2half_rn(new_mean_f16(__half2float(h[vi]), w0, keep, fix));
+        w16[vi] = (unsigned short)__fadd_rn(w0, (float)keep);
+    } else {
+        double* d = reinterpret_cast<double*>(v.tsdf);
+        d[vi] = d[vi] + (double)fix * kFixInv;
+        v.weight[vi] = __fadd_rn(v.weight[vi], (float)keep);
+    }
+    u.vacc[vi] = 0ull;
+    u.vcnt[vi] = 0u;
+}
+
 // The keep-th smallest id (1-based) of a group, by four 8-bit radix passes
 // with a per-warp histogram. Ids are distinct, so exactly keep ids are <= it.
-__device__ uint32_t slot_id(const DevVolume& v, const BatchArgs& a, uint32_t slot);
-
-__device__ uint32_t radix_select(const DevVolume& v, const BatchArgs& a, const uint32_t* X, int n,
-                                 int keep, uint32_t* hist, int lane) {
+__device__ uint32_t radix_select(const uint32_t* ids, int n, int keep, uint32_t* hist, int lane) {
     uint32_t prefix = 0u, pmask = 0u;
     int need = keep;
     for (int shift = 24; shift >= 0; shift -= 8) {
         for (int b = lane; b < 256; b += 32) hist[b] = 0u;
         __syncwarp();
         for (int k = lane; k < n; k += 32) {
-            const uint32_t id = slot_id(v, a, X[k]);
+            const uint32_t id = ids[k];
             if ((id & pmask) == prefix) atomicAdd(&hist[(id >> shift) & 255u], 1u);
         }
         __syncwarp();
@@ -346,110 +477,98 @@ __device__ uint32_t radix_select(const DevVolume& v, const BatchArgs& a, const u
     return prefix;
 }
 
-// Canonical id and normalised SDF (as 2^-40 fixed point) of the record in
-// band slot `slot`: the walk's arithmetic again for this one sample (same
-// rounding; the FP64 oracle's value in double).
-template <int S>
-__device__ __forceinline__ uint32_t slot_record(const DevVolume& v, const BatchArgs& a, uint32_t slot,
-                                                long long& fix) {
-    const uint32_t n_steps = 2u * (uint32_t)v.steps + 1u;
-    const uint32_t s = slot / (uint32_t)a.n, i = slot - s * (uint32_t)a.n;
-    Ray r;
-    int vx = 0, vy = 0, vz = 0;
-    float sdf = 0.0f;
-    const bool ok = ray_setup(a, (int)i, r);
-    if (ok) band_sample(v, a, r, (int)s - v.steps, vx, vy, vz, sdf);
-    if constexpr (S == kStoreF64) {
-        fix = ok ? to_fix(clamp_sdf_n_f64(sdf_f64(v, a, r.px, r.py, r.pz, vx, vy, vz), v.trunc)) : 0ll;
+// One warp per voxel of the large list: up to 8 records per lane ranked by id
+// against all others in registers, a radix select of the keep-th id beyond
+// 256 records. Returns the sum of the accepted values (on every lane).
+__device__ long long warp_select(const uint32_t* ids, const long long* vals, int n, int keep,
+                                 uint32_t* hist, int lane) {
+    long long fix = 0;
+    if (n <= 32 * kRankRegs) {
+        uint32_t id[kRankRegs];
+        long long val[kRankRegs];
+        int rank[kRankRegs];
+        const int rows = (n + 31) / 32;
+#pragma unroll
+        for (int r = 0; r < kRankRegs; ++r) {
+            const int k = r * 32 + lane;
+            id[r] = 0xFFFFFFFFu;
+            val[r] = 0ll;
+            rank[r] = 0;
+            if (r < rows && k < n) {
+                id[r] = ids[k];
+                val[r] = vals[k];
+            }
+        }
+#pragma unroll
+        for (int rr = 0; rr < kRankRegs; ++rr) {
+            if (rr >= rows) break;
+            const int m = min(32, n - rr * 32);
+            for (int src = 0; src < m; ++src) {
+                const uint32_t other = __shfl_sync(0xffffffffu, id[rr], src);
+#pragma unroll
+                for (int r = 0; r < kRankRegs; ++r)
+                    if (r < rows) rank[r] += other < id[r] ? 1 : 0;
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < kRankRegs; ++r)
+            if (r < rows && r * 32 + lane < n && rank[r] < keep) fix += val[r];
     } else {
-        fix = to_fix(fminf(fmaxf(__fmul_rn(sdf, v.inv_trunc), -1.0f), 1.0f));
+        const uint32_t last = radix_select(ids, n, keep, hist, lane);
+        for (int k = lane; k < n; k += 32)
+            if (ids[k] <= last) fix += vals[k];
     }
-    return i * n_steps + s;
-}
-
-__device__ __forceinline__ uint32_t slot_id(const DevVolume& v, const BatchArgs& a, uint32_t slot) {
-    const uint32_t s = slot / (uint32_t)a.n;
-    return (slot - s * (uint32_t)a.n) * (2u * (uint32_t)v.steps + 1u) + s;
+    for (int o = 16; o > 0; o >>= 1) fix += __shfl_xor_sync(0xffffffffu, fix, o);
+    return fix;
 }
 
 template <int S>
 __global__ void __launch_bounds__(kDeferThreads)
-deferred_kernel(DevVolume v, BatchArgs a, UpdateScratch u) {
+deferred_kernel(DevVolume v, UpdateScratch u) {
     __shared__ uint32_t hist[kDeferWarps][256];
     __shared__ int s_updated;
     if (threadIdx.x == 0) s_updated = 0;
     __syncthreads();
+    launch_dependents();
+    grid_dependency_wait();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int nd = min(u.ctl->n_deferred, u.dvox_cap);
+    const unsigned long long lists = u.ctl->def_lists;
+    int n_small = (int)(lists & 0xFFFFFFFFull), n_large = (int)(lists >> 32);
+    if ((long long)n_small + n_large > (long long)u.dvox_cap) n_small = n_large = 0;  // overflowed
     int updated = 0;
-    for (int d = blockIdx.x * kDeferWarps + warp; d < nd; d += gridDim.x * kDeferWarps) {
-        const int4 e = u.dvox[d];  // (voxel, group base, records, accepted)
-        const uint32_t vi = (uint32_t)e.x;
-        const int n = e.z, keep = e.w;
-        const uint32_t* X = u.deferred + (uint32_t)e.y;
-        long long fix = 0;
-        if (n <= 32 * kRankRegs) {
-            // Up to 8 records per lane, ranked by id against all others.
-            uint32_t id[kRankRegs];
-            long long val[kRankRegs];
-            int rank[kRankRegs];
-            const int rows = (n + 31) / 32;
-#pragma unroll
-            for (int r = 0; r < kRankRegs; ++r) {
-                const int k = r * 32 + lane;
-                id[r] = 0xFFFFFFFFu;
-                val[r] = 0ll;
-                rank[r] = 0;
-                if (r < rows && k < n) id[r] = slot_record<S>(v, a, X[k], val[r]);
-            }
-#pragma unroll
-            for (int rr = 0; rr < kRankRegs; ++rr) {
-                if (rr >= rows) break;
-                const int m = min(32, n - rr * 32);
-                for (int src = 0; src < m; ++src) {
-                    const uint32_t other = __shfl_sync(0xffffffffu, id[rr], src);
-#pragma unroll
-                    for (int r = 0; r < kRankRegs; ++r)
-                        if (r < rows) rank[r] += other < id[r] ? 1 : 0;
-                }
-            }
-#pragma unroll
-            for (int r = 0; r < kRankRegs; ++r)
-                if (r < rows && r * 32 + lane < n && rank[r] < keep) fix += val[r];
-        } else {
-            // The keep-th smallest id by radix select over the group's ids,
-            // then the accepted records' values.
-            const uint32_t last = radix_select(v, a, X, n, keep, hist[warp], lane);
-            for (int k = lane; k < n; k += 32) {
-                if (slot_id(v, a, X[k]) > last) continue;
-                long long val;
-                slot_record<S>(v, a, X[k], val);
-                fix += val;
-            }
-        }
-        for (int o = 16; o > 0; o >>= 1) fix += __shfl_xor_sync(0xffffffffu, fix, o);
+
+    // Large groups: one warp each.
+    const int gw = blockIdx.x * kDeferWarps + warp, nw = gridDim.x * kDeferWarps;
+    for (int d = gw; d < n_large; d += nw) {
+        const int4 e = u.dvox[u.dvox_cap - 1 - d];  // (voxel, group base, records, accepted)
+        const long long fix = warp_select(u.deferred + (uint32_t)e.y, u.deferred_fix + (uint32_t)e.y,
+                                          e.z, e.w, hist[warp], lane);
         if (lane == 0) {
-            if constexpr (S == kStoreF32) {
-                const float wn = __fadd_rn(v.weight[vi], (float)keep);
-                v.tsdf[vi] = add_fix(v.tsdf[vi], fix);
-                v.weight[vi] = wn;
-                const float c = __fmul_rn(128.0f, wn);
-                v.r[vi] = c;
-                v.g[vi] = c;
-                v.b[vi] = c;
-            } else if constexpr (S == kStoreF16U16) {
-                unsigned short* w16 = reinterpret_cast<unsigned short*>(v.weight);
-                __half* h = reinterpret_cast<__half*>(v.tsdf);
-                const float w0 = (float)w16[vi];
-                h[vi] = __float2half_rn(new_mean_f16(__half2float(h[vi]), w0, keep, fix));
-                w16[vi] = (unsigned short)__fadd_rn(w0, (float)keep);
-            } else {
-                double* d = reinterpret_cast<double*>(v.tsdf);
-                d[vi] = d[vi] + (double)fix * kFixInv;
-                v.weight[vi] = __fadd_rn(v.weight[vi], (float)keep);
-            }
-            u.vacc[vi] = 0ull;
-            u.vcnt[vi] = 0u;
+            finish_voxel<S>(v, u, (uint32_t)e.x, e.w, fix);
+            ++updated;
+        }
+    }
+
+    // Small groups (at most kLaneRecords = 16 records): one half-warp each,
+    // one record per lane, ranked by id with shuffles inside the half.
+    static_assert(kLaneRecords == 16, "small groups are ranked by half-warps");
+    const int half = lane >> 4, hl = lane & 15;
+    for (int d0 = 2 * gw; d0 < n_small; d0 += 2 * nw) {  // uniform across the warp
+        const int d = d0 + half;
+        const bool live = d < n_small;
+        const int4 e = live ? u.dvox[d] : make_int4(0, 0, 0, 0);
+        const int n = e.z, keep = e.w;
+        const bool mine = live && hl < n;
+        const uint32_t id = mine ? u.deferred[(uint32_t)e.y + hl] : 0xFFFFFFFFu;
+        const long long val = mine ? u.deferred_fix[(uint32_t)e.y + hl] : 0ll;
+        int rank = 0;
+#pragma unroll
+        for (int src = 0; src < 16; ++src) rank += __shfl_sync(0xffffffffu, id, src, 16) < id ? 1 : 0;
+        long long fix = (mine && rank < keep) ? val : 0ll;
+#pragma unroll
+        for (int o = 8; o > 0; o >>= 1) fix += __shfl_xor_sync(0xffffffffu, fix, o, 16);
+        if (live && hl == 0) {
+            finish_voxel<S>(v, u, (uint32_t)e.x, keep, fix);
             ++updated;
         }
     }
@@ -458,32 +577,69 @@ deferred_kernel(DevVolume v, BatchArgs a, UpdateScratch u) {
 
 }  // namespace
 
-cudaError_t launch_finish(const DevVolume& v, const UpdateScratch& u, int n_ctas, cudaStream_t s) {
+// CTAs of Kernel resident at once on the device (one wave), queried once
+// per kernel.
+template <auto Kernel>
+int resident_grid(int threads, int sm_count) {
+    static int per_sm = 0;
+    static std::once_flag once;
+    std::call_once(once, [&] {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, Kernel, threads, 0) != cudaSuccess ||
+            per_sm < 1)
+            per_sm = 1;
+    });
+    return per_sm * sm_count;
+}
+
+cudaError_t launch_finish(const DevVolume& v, const UpdateScratch& u, int sm_count, cudaStream_t s) {
     switch (v.storage) {
-        case kStoreF16U16: finish_kernel<kStoreF16U16><<<n_ctas, kFinishThreads, 0, s>>>(v, u); break;
-        case kStoreF64: finish_kernel<kStoreF64><<<n_ctas, kFinishThreads, 0, s>>>(v, u); break;
-        default: finish_kernel<kStoreF32><<<n_ctas, kFinishThreads, 0, s>>>(v, u); break;
+        case kStoreF16U16: {
+            return launch_after(finish_kernel<kStoreF16U16>, resident_grid<finish_kernel<kStoreF16U16>>(kFinishThreads, sm_count),
+                                kFinishThreads, s, v, u);
+        }
+        case kStoreF64: {
+            return launch_after(finish_kernel<kStoreF64>, resident_grid<finish_kernel<kStoreF64>>(kFinishThreads, sm_count),
+                                kFinishThreads, s, v, u);
+        }
+        default: {
+            return launch_after(finish_kernel<kStoreF32>, resident_grid<finish_kernel<kStoreF32>>(kFinishThreads, sm_count),
+                                kFinishThreads, s, v, u);
+        }
     }
-    return cudaGetLastError();
 }
 
 cudaError_t launch_group(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
                          cudaStream_t s) {
     const uint32_t n_slots = (uint32_t)a.n * (2u * (uint32_t)v.steps + 1u);
     if (n_slots == 0) return cudaSuccess;
-    const uint32_t per_cta = kGroupThreads * 4u;
-    group_kernel<<<(n_slots + per_cta - 1u) / per_cta, kGroupThreads, 0, s>>>(u, n_slots);
-    return cudaGetLastError();
+    const uint32_t per_cta = kGroupThreads * (uint32_t)kGroupPerThread;
+    return launch_after(group_kernel, (n_slots + per_cta - 1u) / per_cta, kGroupThreads, s, u, n_slots);
 }
 
-cudaError_t launch_deferred(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
-                            int n_ctas, cudaStream_t s) {
+cudaError_t launch_values(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u, int n_ctas,
+                          cudaStream_t s) {
     switch (v.storage) {
-        case kStoreF16U16: deferred_kernel<kStoreF16U16><<<n_ctas, kDeferThreads, 0, s>>>(v, a, u); break;
-        case kStoreF64: deferred_kernel<kStoreF64><<<n_ctas, kDeferThreads, 0, s>>>(v, a, u); break;
-        default: deferred_kernel<kStoreF32><<<n_ctas, kDeferThreads, 0, s>>>(v, a, u); break;
+        case kStoreF16U16: return launch_after(values_kernel<kStoreF16U16>, n_ctas, kGroupThreads, s, v, a, u);
+        case kStoreF64: return launch_after(values_kernel<kStoreF64>, n_ctas, kGroupThreads, s, v, a, u);
+        default: return launch_after(values_kernel<kStoreF32>, n_ctas, kGroupThreads, s, v, a, u);
     }
-    return cudaGetLastError();
+}
+
+cudaError_t launch_deferred(const DevVolume& v, const UpdateScratch& u, int sm_count, cudaStream_t s) {
+    switch (v.storage) {
+        case kStoreF16U16: {
+            return launch_after(deferred_kernel<kStoreF16U16>, resident_grid<deferred_kernel<kStoreF16U16>>(kDeferThreads, sm_count),
+                                kDeferThreads, s, v, u);
+        }
+        case kStoreF64: {
+            return launch_after(deferred_kernel<kStoreF64>, resident_grid<deferred_kernel<kStoreF64>>(kDeferThreads, sm_count),
+                                kDeferThreads, s, v, u);
+        }
+        default: {
+            return launch_after(deferred_kernel<kStoreF32>, resident_grid<deferred_kernel<kStoreF32>>(kDeferThreads, sm_count),
+                                kDeferThreads, s, v, u);
+        }
+    }
 }
 
 }  // namespace osn_b200

@@ -371,6 +371,16 @@ __device__ __forceinline__ float add_fix(float t0, long long sum) {
     return __double2float_rn((double)t0 + (double)sum * kFixInv);
 }
 
+// Programmatic dependent launch. A kernel launched with programmatic stream
+// serialisation may start before its predecessor on the stream has finished;
+// it waits here, before reading anything the predecessor wrote, until that
+// grid has completed and its writes are visible. Each kernel lets its own
+// dependents launch as soon as all of its CTAs are running, so their launch
+// overlaps its execution. Both are no-ops for kernels launched without the
+// attribute.
+__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void launch_dependents() { asm volatile("griddepcontrol.launch_dependents;"); }
+
 __device__ __forceinline__ unsigned lanemask_lt() {
     unsigned m;
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));

@@ -12,9 +12,9 @@
 // with its scratch in one fixed array compiled into the library.
 //
 // The array is a file-scope __device__ variable of kNoAllocScratchBytes
-// (32 MiB + 256 bytes): the control counters, kNoAllocMaxRecords 4-byte band
-// records, as many 4-byte deferred slots, and half as many 16-byte
-// deferred-voxel entries, i.e. batches with
+// (48 MiB + 256 bytes): the control counters, kNoAllocMaxRecords 4-byte band
+// records, as many 4-byte ids and 8-byte values of crossing voxels' records,
+// and half as many 16-byte crossing-voxel entries, i.e. batches with
 // n_points * (2 * steps + 1) <= 2,097,152 (a 480x360 frame at 9 band steps
 // per point fits; a 640x480 frame must be split in two). The per-voxel and
 // per-block state the update also uses belongs to the volume and was
@@ -40,8 +40,9 @@ constexpr int64_t kNoAllocMaxRecords = OSN_TSDF_NOALLOC_MAX_RECORDS;
 constexpr int64_t kNoAllocMaxDeferred = kNoAllocMaxRecords / 2;
 constexpr size_t kNoAllocRecordBytes = (size_t)kNoAllocMaxRecords * sizeof(uint32_t);
 constexpr size_t kNoAllocDeferredBytes = (size_t)kNoAllocMaxRecords * sizeof(uint32_t);
+constexpr size_t kNoAllocFixBytes = (size_t)kNoAllocMaxRecords * sizeof(long long);
 constexpr size_t kNoAllocScratchBytes = kNoAllocHeaderBytes + kNoAllocRecordBytes +
-                                        kNoAllocDeferredBytes +
+                                        kNoAllocDeferredBytes + kNoAllocFixBytes +
                                         (size_t)kNoAllocMaxDeferred * sizeof(int4);
 static_assert(sizeof(UpdateControl) <= kNoAllocHeaderBytes, "control block must fit the header");
 
@@ -81,8 +82,10 @@ cudaError_t Volume::update_static_scratch(const BatchArgs& a, void* scratch) {
     u.ctl = reinterpret_cast<UpdateControl*>(base);
     u.records = reinterpret_cast<uint32_t*>(base + kNoAllocHeaderBytes);
     u.deferred = reinterpret_cast<uint32_t*>(base + kNoAllocHeaderBytes + kNoAllocRecordBytes);
+    u.deferred_fix = reinterpret_cast<long long*>(base + kNoAllocHeaderBytes + kNoAllocRecordBytes +
+                                                  kNoAllocDeferredBytes);
     u.dvox = reinterpret_cast<int4*>(base + kNoAllocHeaderBytes + kNoAllocRecordBytes +
-                                     kNoAllocDeferredBytes);
+                                     kNoAllocDeferredBytes + kNoAllocFixBytes);
     u.record_cap = kNoAllocMaxRecords;
     u.dvox_cap = (int32_t)kNoAllocMaxDeferred;
     // Only the control counters must start at zero (run_update clears them);

@@ -134,6 +134,7 @@ Volume::~Volume() {
     cudaFree(us_.ctl);
     cudaFree(us_.records);
     cudaFree(us_.deferred);
+    cudaFree(us_.deferred_fix);
     cudaFree(us_.dvox);
     cudaFree(mesh_posnor_);
     cudaFree(mesh_rgb_);
@@ -211,17 +212,21 @@ bool Volume::ensure_records(int64_t n_records) {
     cudaStreamSynchronize(stream_);
     cudaFree(us_.records);
     cudaFree(us_.deferred);
+    cudaFree(us_.deferred_fix);
     cudaFree(us_.dvox);
     us_.records = nullptr;
     us_.deferred = nullptr;
+    us_.deferred_fix = nullptr;
     us_.dvox = nullptr;
     us_.record_cap = 0;
     us_.dvox_cap = 0;
-    // A deferred voxel holds at least two records, so half the records bound
-    // the deferred list.
+    // A crossing voxel holds at least two records, so half the records bound
+    // the two crossing-voxel lists together.
     const int64_t n_dvox = n_records / 2 + 1;
     if (cudaMalloc(&us_.records, (size_t)n_records * sizeof(uint32_t)) != cudaSuccess) return false;
     if (cudaMalloc(&us_.deferred, (size_t)n_records * sizeof(uint32_t)) != cudaSuccess) return false;
+    if (cudaMalloc(&us_.deferred_fix, (size_t)n_records * sizeof(long long)) != cudaSuccess)
+        return false;
     if (cudaMalloc(&us_.dvox, (size_t)n_dvox * sizeof(int4)) != cudaSuccess) return false;
     us_.record_cap = n_records;
     us_.dvox_cap = (int32_t)std::min<int64_t>(n_dvox, INT32_MAX);
@@ -244,15 +249,19 @@ cudaError_t Volume::run_update(const BatchArgs& a, const UpdateScratch& scratch,
     mark_end(kKBand);
     if (e != cudaSuccess) return e;
     mark_start(kKFinish);
-    e = launch_finish(dv_, u, sm_count_ * 16, stream_);
+    e = launch_finish(dv_, u, sm_count_, stream_);
     mark_end(kKFinish);
     if (e != cudaSuccess) return e;
     mark_start(kKGroup);
     e = launch_group(dv_, a, u, stream_);
     mark_end(kKGroup);
     if (e != cudaSuccess) return e;
+    mark_start(kKValues);
+    e = launch_values(dv_, a, u, sm_count_ * 4, stream_);
+    mark_end(kKValues);
+    if (e != cudaSuccess) return e;
     mark_start(kKDeferred);
-    e = launch_deferred(dv_, a, u, sm_count_ * 8, stream_);
+    e = launch_deferred(dv_, u, sm_count_, stream_);
     mark_end(kKDeferred);
     return e;
 }
@@ -373,7 +382,7 @@ bool Volume::last_update_stats(int64_t out[4]) {
     out[0] = c.n_updated;
     out[1] = c.n_records;
     out[2] = c.n_touched;
-    out[3] = c.n_deferred;
+    out[3] = (int64_t)(c.def_lists & 0xFFFFFFFFull) + (int64_t)(c.def_lists >> 32);
     return true;
 }
 

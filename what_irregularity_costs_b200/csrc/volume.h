@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cstdint>
+#include <utility>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -19,7 +20,8 @@ enum KernelId : int {
     kKDeferred = 4,      // ordered cap selection of those voxels
     kKExtract = 5,
     kKReset = 6,
-    kNumKernelIds = 7,
+    kKValues = 7,        // ids and values of the grouped records
+    kNumKernelIds = 8,
 };
 
 // Counters an update pass keeps on the device (one small struct, cleared by
@@ -28,9 +30,14 @@ struct UpdateControl {
     int32_t n_records;   // band records counted (contributions that can be accepted)
     int32_t n_touched;   // blocks that received a band sample
     int32_t n_updated;   // voxels whose sums were rewritten
-    int32_t n_deferred;  // voxels that cross the cap inside the batch
+    int32_t pad0;
     uint32_t x_used;     // deferred records reserved
-    int32_t pad[11];
+    int32_t pad1;
+    // Voxels that cross the cap inside the batch, in two lists sharing dvox:
+    // low word = entries of the small list (at most kLaneRecords records,
+    // from the front), high word = entries of the large list (from the back).
+    unsigned long long def_lists;
+    int32_t pad[8];
 };
 static_assert(sizeof(UpdateControl) == 64, "control block is read back as 64 bytes");
 
@@ -39,6 +46,10 @@ static_assert(sizeof(UpdateControl) == 64, "control block is read back as 64 byt
 // dropped or saturated sample.
 constexpr uint32_t kNoVoxel = 0xFFFFFFFFu;
 
+// Cap-crossing voxels with at most this many records are ranked by one lane
+// each (in registers); larger ones by a whole warp.
+constexpr int kLaneRecords = 16;
+
 // Global voxel indices are 32-bit with one value reserved, which bounds the
 // pool at 2^23 - 1 blocks (4 G voxels).
 constexpr int32_t kMaxPoolBlocks = (1 << 23) - 1;
@@ -46,8 +57,9 @@ constexpr int32_t kMaxPoolBlocks = (1 << 23) - 1;
 struct UpdateScratch {
     UpdateControl* ctl = nullptr;
     uint32_t* records = nullptr;  // [record_cap] one per band slot
-    uint32_t* deferred = nullptr; // [record_cap] band slots of crossing voxels' records, grouped per voxel
-    int4* dvox = nullptr;         // [dvox_cap] (voxel, group base, records, accepted)
+    uint32_t* deferred = nullptr;       // [record_cap] canonical ids of crossing voxels' records, grouped per voxel
+    long long* deferred_fix = nullptr;  // [record_cap] their normalised SDFs, 2^-40 fixed point
+    int4* dvox = nullptr;               // [dvox_cap] (voxel, group base, records, accepted)
     int64_t record_cap = 0;
     int32_t dvox_cap = 0;
     // Owned by the volume. Per voxel: zero between updates.
@@ -138,6 +150,25 @@ private:
     int64_t acc_launches_[kNumKernelIds] = {};
 };
 
+// Launch `kernel` with programmatic stream serialisation: it may begin while
+// the previous kernel on the stream is still running, and waits for it in
+// grid_dependency_wait().
+template <typename... KArgs, typename... Args>
+cudaError_t launch_after(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t s,
+                         Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
 // Launchers (one per translation unit).
 cudaError_t launch_allocate(const DevVolume& v, const BatchArgs& a, int mode,
                             unsigned long long* hist, int n_bins, int sm_count, cudaStream_t s);
@@ -146,14 +177,16 @@ cudaError_t launch_reset_voxels(const DevVolume& v, int32_t n_blocks, cudaStream
 cudaError_t launch_extract(const DevVolume& v, int32_t n_blocks, float min_w, float iso,
                            float* posnor, uint8_t* rgb, int32_t cap, int32_t* ctl, cudaStream_t s);
 
-// The update pipeline: band walk (counts, sums, records) -> finish -> group -> deferred.
+// The update pipeline: band walk (counts, sums, records) -> finish -> group
+// -> values -> deferred.
 cudaError_t launch_band_records(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
                                 bool insert, int sm_count, cudaStream_t s);
-cudaError_t launch_finish(const DevVolume& v, const UpdateScratch& u, int n_ctas, cudaStream_t s);
+cudaError_t launch_finish(const DevVolume& v, const UpdateScratch& u, int sm_count, cudaStream_t s);
 cudaError_t launch_group(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
                          cudaStream_t s);
-cudaError_t launch_deferred(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
-                            int n_ctas, cudaStream_t s);
+cudaError_t launch_values(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u, int n_ctas,
+                          cudaStream_t s);
+cudaError_t launch_deferred(const DevVolume& v, const UpdateScratch& u, int sm_count, cudaStream_t s);
 
 }  // namespace osn_b200
 

@@ -17,7 +17,7 @@ import numpy as np
 
 from . import _lib
 
-KERNEL_NAMES = ["allocate", "band", "finish", "group", "deferred", "extract", "reset"]
+KERNEL_NAMES = ["allocate", "band", "finish", "group", "deferred", "extract", "reset", "values"]
 
 # Voxel storage modes (OSN_TSDF_STORAGE_* in include/osn_tsdf_b200.h).
 STORAGE_FP32, STORAGE_FP16_U16, STORAGE_FP64 = 0, 1, 2
