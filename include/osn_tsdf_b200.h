@@ -198,6 +198,62 @@ int32_t osn_tsdf_cuda_update_voxels_noalloc(OsnTsdfCudaVolume* v, const float* d
                                             int32_t n_points, float cam_x, float cam_y,
                                             float cam_z, float radius_m);
 
+/* ---- batched integrate (no counterpart in the reference) ---------------
+ *
+ * Many independent volumes ("scenes", each with its own table, pool, voxel
+ * size and truncation, one storage mode for all) integrate one frame each
+ * per step in one chain of work-queued passes on the batch's stream: a
+ * table of the step's scenes is uploaded, then one pass of each kernel
+ * (band walk, finish, group, values, deferred) covers every scene, its CTAs
+ * taking (scene, tile range) work items from atomic queues. Results are
+ * bit-identical to integrating each scene alone with osn_tsdf_cuda_integrate.
+ *
+ * A volume attached to a batch is integrated only through it; before any
+ * other call on the volume (counters, extraction, reset, device view),
+ * call osn_tsdf_batch_synchronize. At most 64 scenes per batch. */
+typedef struct OsnTsdfBatch OsnTsdfBatch;
+
+/* NULL on max_scenes outside [1, 64] or device allocation failure. */
+OsnTsdfBatch* osn_tsdf_batch_create(int32_t max_scenes);
+void osn_tsdf_batch_destroy(OsnTsdfBatch* b);
+/* Attach a volume that will receive frames of up to max_points points (its
+ * scratch is sized now; no allocation happens in a step). Waits for the
+ * volume's stream. Returns the scene index, or -1 (full, NULL, already
+ * attached, storage mode differs from the other scenes, batch too large). */
+int32_t osn_tsdf_batch_add(OsnTsdfBatch* b, OsnTsdfCudaVolume* v, int32_t max_points);
+/* The next step's frame of one scene: device positions (3 floats per point,
+ * kept alive until the step has run), camera origin, far cutoff. Scenes
+ * without a frame sit the step out. 0 ok, 1 bad arguments. */
+int32_t osn_tsdf_batch_set_frame(OsnTsdfBatch* b, int32_t scene, const float* d_positions,
+                                 int32_t n_points, float cam_x, float cam_y, float cam_z,
+                                 float radius_m);
+/* Queue one step (asynchronous on the batch's stream). 0 ok, 1 bad batch,
+ * 3 launch failure. */
+int32_t osn_tsdf_batch_step(OsnTsdfBatch* b);
+int32_t osn_tsdf_batch_synchronize(OsnTsdfBatch* b);
+/* Replay the step's passes from a CUDA graph (captured on the second step
+ * with the same scenes and shape). */
+int32_t osn_tsdf_batch_set_graph(OsnTsdfBatch* b, int32_t enabled);
+/* Run the next 16 * steps_per_shape steps with each candidate shape
+ * (band tiles per work item 1/2/4/8, warp-grouped or per-lane block
+ * resolution, one or two blocks per finish item), then keep the fastest
+ * median. Shapes change speed only, never results. */
+int32_t osn_tsdf_batch_autotune(OsnTsdfBatch* b, int32_t steps_per_shape);
+/* Fix the shape: tiles_per_item in [1, 8], probe 0 (warp) or 1 (lane),
+ * finish_pair 0 or 1. */
+int32_t osn_tsdf_batch_set_shape(OsnTsdfBatch* b, int32_t tiles_per_item, int32_t probe,
+                                 int32_t finish_pair);
+/* Current shape into out3 (tiles_per_item, probe, finish_pair); returns 1
+ * while tuning, 0 otherwise, -1 on bad arguments. */
+int32_t osn_tsdf_batch_shape(OsnTsdfBatch* b, int32_t* out3);
+/* Autotuner record (waits): median step ms of each candidate (-1 if not run)
+ * and its shape (3 ints each); returns the number of candidates written. */
+int32_t osn_tsdf_batch_tune_results(OsnTsdfBatch* b, double* ms, int32_t* shapes, int32_t n_max);
+/* Status words of the batch and its volumes, OR-ed (waits). */
+uint32_t osn_tsdf_batch_status(OsnTsdfBatch* b);
+void* osn_tsdf_batch_stream(OsnTsdfBatch* b);
+int32_t osn_tsdf_batch_size(OsnTsdfBatch* b);
+
 /* Kernel timing. When enabled, every kernel launch of the volume is
  * bracketed by CUDA events on the volume's stream; kernel_times reads (and
  * waits for) the accumulated per-kernel milliseconds and launch counts.

@@ -9,6 +9,7 @@ from .volume import (CudaVolume, device_tensor, KERNEL_NAMES, STORAGE_FP32,  # n
                      STORAGE_FP16_U16, STORAGE_FP64, STORAGE_NAMES)
 from . import scenes  # noqa: F401
 from . import precision  # noqa: F401
+from .batch import Batch  # noqa: F401
 
-__all__ = ["CudaVolume", "device_tensor", "scenes", "precision", "KERNEL_NAMES", "STORAGE_FP32",
+__all__ = ["CudaVolume", "Batch", "device_tensor", "scenes", "precision", "KERNEL_NAMES", "STORAGE_FP32",
            "STORAGE_FP16_U16", "STORAGE_FP64", "STORAGE_NAMES"]

@@ -69,6 +69,20 @@ _SIG = {
     "osn_tsdf_cuda_set_timing": (_I, [_P, _I]),
     "osn_tsdf_cuda_kernel_times": (_I, [_P, _P, _P, _I]),
     "osn_tsdf_cuda_update_voxels_noalloc": (_I, [_P, _P, _I, _F, _F, _F, _F]),
+    "osn_tsdf_batch_create": (_P, [_I]),
+    "osn_tsdf_batch_destroy": (None, [_P]),
+    "osn_tsdf_batch_add": (_I, [_P, _P, _I]),
+    "osn_tsdf_batch_set_frame": (_I, [_P, _I, _P, _I, _F, _F, _F, _F]),
+    "osn_tsdf_batch_step": (_I, [_P]),
+    "osn_tsdf_batch_synchronize": (_I, [_P]),
+    "osn_tsdf_batch_set_graph": (_I, [_P, _I]),
+    "osn_tsdf_batch_autotune": (_I, [_P, _I]),
+    "osn_tsdf_batch_set_shape": (_I, [_P, _I, _I, _I]),
+    "osn_tsdf_batch_shape": (_I, [_P, _P]),
+    "osn_tsdf_batch_tune_results": (_I, [_P, _P, _P, _I]),
+    "osn_tsdf_batch_status": (C.c_uint32, [_P]),
+    "osn_tsdf_batch_stream": (_P, [_P]),
+    "osn_tsdf_batch_size": (_I, [_P]),
 }
 
 _lib = None
@@ -78,7 +92,7 @@ def declared_symbols() -> list[str]:
     """Every function the public header declares."""
     with open(HEADER) as f:
         text = f.read()
-    return sorted(set(re.findall(r"\b(osn_tsdf_cuda_\w+)\s*\(", text)))
+    return sorted(set(re.findall(r"\b(osn_tsdf_(?:cuda|batch)_\w+)\s*\(", text)))
 
 
 def load(path: str = LIB_PATH):

@@ -44,7 +44,7 @@
 namespace osn_b200 {
 namespace {
 
-constexpr int kBandThreads = 128;
+constexpr int kBandThreads = kBatchTilePoints;
 constexpr int kChunk = 9;  // samples per ray held in registers (the whole band at 4 voxels)
 constexpr int kBandMinBlocks = 8;  // resident CTAs per SM the register budget is sized for
 
@@ -147,17 +147,167 @@ __device__ __forceinline__ void red_add(unsigned long long* p, unsigned long lon
     asm volatile("red.global.add.u64 [%0], %1;" ::"l"(p), "l"(x));
 }
 
-template <int MODE, bool RECORDS, int S>
-__global__ void __launch_bounds__(kBandThreads, kBandMinBlocks)
-band_kernel(DevVolume v, BatchArgs a, UpdateScratch u, unsigned long long* hist, int n_bins) {
-    // Per-thread columns: run q of thread t at [q][t] (no bank conflicts).
-    __shared__ long long run_key[kChunk][kBandThreads];
-    __shared__ int32_t run_bi[kChunk][kBandThreads];    // written by the run's group leader
-    __shared__ uint8_t run_src[kChunk][kBandThreads];   // leader lane of the run's group
+// Shared memory of one band CTA: per-thread run columns, run q of thread t
+// at [q][t] (no bank conflicts).
+struct BandSmem {
+    long long run_key[kChunk][kBandThreads];
+    int32_t run_bi[kChunk][kBandThreads];   // written by the run's group leader
+    uint8_t run_src[kChunk][kBandThreads];  // leader lane of the run's group
+};
+
+// Walk point i (already loaded into px, py, pz; i >= a.n for lanes without a
+// point) through its band: runs, warp-cooperative block resolution, then
+// the update tail. Called by every thread of the CTA, warp-synchronously.
+// Block resolution schemes of the band walk.
+constexpr int kProbeWarp = 0;  // equal keys grouped across the warp, one leader probes
+constexpr int kProbeLane = 1;  // every lane probes its own runs (L1 shares the loads)
+
+template <int MODE, bool RECORDS, int S, int PROBE = kProbeWarp>
+__device__ __forceinline__ void band_point(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
+                                           int i, float px, float py, float pz, BandSmem& sm,
+                                           uint32_t& drops, uint32_t& counted,
+                                           unsigned long long* hist, int n_bins) {
     const int t = threadIdx.x;
     const int lane = t & 31, wbase = t & ~31;
     const bool counts_drops = MODE != kLookupOnly && MODE != kAllocNoCas && MODE != kAllocCountingCas;
     const bool sat_check = RECORDS && v.weight_cap > 0.0f;
+    auto& run_key = sm.run_key;
+    auto& run_bi = sm.run_bi;
+    auto& run_src = sm.run_src;
+    Ray r;
+    const bool live = i < a.n && ray_setup_at(a, px, py, pz, r);
+    uint32_t* rec = RECORDS ? u.records + i : nullptr;  // slot (s = -steps, i)
+
+    for (int c0 = -v.steps; c0 <= v.steps; c0 += kChunk) {
+        uint32_t st[kChunk];
+        float sd[kChunk];
+        int n_run = 0;
+        long long last = kNoKey;
+
+        // Phase 1: the chunk's samples; runs of equal blocks in walk order.
+#pragma unroll
+        for (int j = 0; j < kChunk; ++j) {
+            st[j] = 0u;
+            sd[j] = 0.0f;
+            const int s = c0 + j;
+            int vx, vy, vz;
+            float sdf;
+            if (live && s <= v.steps && band_sample(v, a, r, s, vx, vy, vz, sdf)) {
+                const int bx = vx >> 3, by = vy >> 3, bz = vz >> 3;  // floor_div(v, 8)
+                const long long key = pack_key(bx, by, bz);
+                // A straight ray leaves a block (a convex box) for good, so
+                // equal consecutive keys are the only repeats.
+                if (key != last) {
+                    last = key;
+                    run_key[n_run][t] = key;
+                    ++n_run;
+                }
+                const uint32_t lv =
+                    (uint32_t)(((vz & 7) * kBlockDim + (vy & 7)) * kBlockDim + (vx & 7));
+                st[j] = kValid | lv | (uint32_t)(n_run - 1) << kRunShift;
+                sd[j] = sdf;
+            }
+        }
+
+        // Phase 2a: group equal keys across the warp, one round per run
+        // index; the lowest lane of a group leads it. (Per-lane probing: every
+        // lane leads its own runs.)
+        uint32_t lead = 0u;
+        if constexpr (PROBE == kProbeWarp) {
+            for (int q = 0; q < kChunk; ++q) {
+                if (!__any_sync(0xffffffffu, q < n_run)) break;
+                const long long key = q < n_run ? run_key[q][t] : kNoKey;
+                const unsigned grp = __match_any_sync(0xffffffffu, key);
+                const int leader = __ffs(grp) - 1;
+                if (q < n_run) run_src[q][t] = (uint8_t)leader;
+                if (key != kNoKey && lane == leader) lead |= 1u << q;
+            }
+        } else {
+            for (int q = 0; q < n_run; ++q) run_src[q][t] = (uint8_t)lane;
+            lead = n_run ? (1u << n_run) - 1u : 0u;
+        }
+        // Phase 2b: each leader resolves its runs two at a time, both
+        // home-slot probes (and then both tag reads) in flight together.
+        while (lead) {
+            const int qa = __ffs(lead) - 1;
+            lead &= lead - 1u;
+            const int qb = lead ? __ffs(lead) - 1 : -1;
+            if (qb >= 0) lead &= lead - 1u;
+            const long long ka = run_key[qa][t];
+            const long long kb = qb >= 0 ? run_key[qb][t] : kNoKey;
+            const int4 ra = home_entry<MODE>(v, ka);
+            const int4 rb = qb >= 0 ? home_entry<MODE>(v, kb) : make_int4(0, 0, -1, 0);
+            const int32_t ba = resolve_from<MODE>(v, ra, ka, hist, n_bins);
+            const int32_t bb = qb >= 0 ? resolve_from<MODE>(v, rb, kb, hist, n_bins) : -1;
+            run_bi[qa][t] = ba;
+            if (qb >= 0) run_bi[qb][t] = bb;
+            if (RECORDS) {
+                const uint32_t sa = ba >= 0 ? __ldca(&u.blk_touch[ba]) : u.tag;
+                const uint32_t sb = bb >= 0 ? __ldca(&u.blk_touch[bb]) : u.tag;
+                tag_touched(u, ba, sa);
+                tag_touched(u, bb, sb);
+            }
+        }
+        __syncwarp();
+
+        // Phase 3: drops; then every sample's weight gather in flight
+        // together; then the saturation gate, counts, sums and records.
+        uint32_t vox[kChunk];
+#pragma unroll
+        for (int j = 0; j < kChunk; ++j) {
+            vox[j] = kNoVoxel;
+            if (st[j] & kValid) {
+                const uint32_t q = (st[j] >> kRunShift) & 15u;
+                const int32_t bi = run_bi[q][wbase + run_src[q][t]];
+                if (bi < 0) {
+                    if (counts_drops) ++drops;
+                } else {
+                    vox[j] = (uint32_t)bi * kBlockVoxels + (st[j] & kLvMask);
+                }
+            }
+        }
+        if (RECORDS) {
+            float w0[kChunk];
+#pragma unroll
+            for (int j = 0; j < kChunk; ++j)
+                w0[j] = (sat_check && vox[j] != kNoVoxel) ? weight_at<S>(v, vox[j]) : 0.0f;
+#pragma unroll
+            for (int j = 0; j < kChunk; ++j) {
+                if (c0 + j > v.steps) break;
+                uint32_t out = kNoVoxel;
+                if (vox[j] != kNoVoxel && !(sat_check && w0[j] >= v.weight_cap)) {
+                    out = vox[j];
+                    long long fix;
+                    if constexpr (S == kStoreF64) {
+                        // The oracle's value of the same sample, in double.
+                        const long long key = run_key[(st[j] >> kRunShift) & 15u][t];
+                        const uint32_t lv = st[j] & kLvMask;
+                        const int vx = unpack_axis(key, 2 * kCoordBits) * kBlockDim + (int)(lv & 7u);
+                        const int vy = unpack_axis(key, kCoordBits) * kBlockDim + (int)((lv >> 3) & 7u);
+                        const int vz = unpack_axis(key, 0) * kBlockDim + (int)(lv >> 6);
+                        fix = to_fix(clamp_sdf_n_f64(sdf_f64(v, a, r.px, r.py, r.pz, vx, vy, vz), v.trunc));
+                    } else {
+                        fix = to_fix(fminf(fmaxf(__fmul_rn(sd[j], v.inv_trunc), -1.0f), 1.0f));
+                    }
+                    red_add(&u.vcnt[out], 1u);
+                    red_add(&u.vacc[out], (unsigned long long)fix);
+                    ++counted;
+                }
+                if (i < a.n) __stcs(rec, out);  // read again only for crossing voxels
+                rec += a.n;
+            }
+        }
+        __syncwarp();  // run columns are rewritten by the next chunk
+    }
+}
+
+template <int MODE, bool RECORDS, int S>
+__global__ void __launch_bounds__(kBandThreads, kBandMinBlocks)
+band_kernel(DevVolume v, BatchArgs a, UpdateScratch u, unsigned long long* hist, int n_bins) {
+    __shared__ BandSmem sm;
+    const int t = threadIdx.x;
+    const int lane = t & 31;
+    const bool counts_drops = MODE != kLookupOnly && MODE != kAllocNoCas && MODE != kAllocCountingCas;
     const int n_tiles = (a.n + kBandThreads - 1) / kBandThreads;
     uint32_t drops = 0, counted = 0;
     __shared__ unsigned s_drops, s_counted;
@@ -187,125 +337,7 @@ band_kernel(DevVolume v, BatchArgs a, UpdateScratch u, unsigned long long* hist,
             ny = a.pos[(size_t)inext * 3 + 1];
             nz = a.pos[(size_t)inext * 3 + 2];
         }
-        Ray r;
-        const bool live = i < a.n && ray_setup_at(a, px, py, pz, r);
-        uint32_t* rec = RECORDS ? u.records + i : nullptr;  // slot (s = -steps, i)
-
-        for (int c0 = -v.steps; c0 <= v.steps; c0 += kChunk) {
-            uint32_t st[kChunk];
-            float sd[kChunk];
-            int n_run = 0;
-            long long last = kNoKey;
-
-            // Phase 1: the chunk's samples; runs of equal blocks in walk order.
-#pragma unroll
-            for (int j = 0; j < kChunk; ++j) {
-                st[j] = 0u;
-                sd[j] = 0.0f;
-                const int s = c0 + j;
-                int vx, vy, vz;
-                float sdf;
-                if (live && s <= v.steps && band_sample(v, a, r, s, vx, vy, vz, sdf)) {
-                    const int bx = vx >> 3, by = vy >> 3, bz = vz >> 3;  // floor_div(v, 8)
-                    const long long key = pack_key(bx, by, bz);
-                    // A straight ray leaves a block (a convex box) for good, so
-                    // equal consecutive keys are the only repeats.
-                    if (key != last) {
-                        last = key;
-                        run_key[n_run][t] = key;
-                        ++n_run;
-                    }
-                    const uint32_t lv =
-                        (uint32_t)(((vz & 7) * kBlockDim + (vy & 7)) * kBlockDim + (vx & 7));
-                    st[j] = kValid | lv | (uint32_t)(n_run - 1) << kRunShift;
-                    sd[j] = sdf;
-                }
-            }
-
-            // Phase 2a: group equal keys across the warp, one round per run
-            // index; the lowest lane of a group leads it.
-            uint32_t lead = 0u;
-            for (int q = 0; q < kChunk; ++q) {
-                if (!__any_sync(0xffffffffu, q < n_run)) break;
-                const long long key = q < n_run ? run_key[q][t] : kNoKey;
-                const unsigned grp = __match_any_sync(0xffffffffu, key);
-                const int leader = __ffs(grp) - 1;
-                if (q < n_run) run_src[q][t] = (uint8_t)leader;
-                if (key != kNoKey && lane == leader) lead |= 1u << q;
-            }
-            // Phase 2b: each leader resolves its runs two at a time, both
-            // home-slot probes (and then both tag reads) in flight together.
-            while (lead) {
-                const int qa = __ffs(lead) - 1;
-                lead &= lead - 1u;
-                const int qb = lead ? __ffs(lead) - 1 : -1;
-                if (qb >= 0) lead &= lead - 1u;
-                const long long ka = run_key[qa][t];
-                const long long kb = qb >= 0 ? run_key[qb][t] : kNoKey;
-                const int4 ra = home_entry<MODE>(v, ka);
-                const int4 rb = qb >= 0 ? home_entry<MODE>(v, kb) : make_int4(0, 0, -1, 0);
-                const int32_t ba = resolve_from<MODE>(v, ra, ka, hist, n_bins);
-                const int32_t bb = qb >= 0 ? resolve_from<MODE>(v, rb, kb, hist, n_bins) : -1;
-                run_bi[qa][t] = ba;
-                if (qb >= 0) run_bi[qb][t] = bb;
-                if (RECORDS) {
-                    const uint32_t sa = ba >= 0 ? __ldca(&u.blk_touch[ba]) : u.tag;
-                    const uint32_t sb = bb >= 0 ? __ldca(&u.blk_touch[bb]) : u.tag;
-                    tag_touched(u, ba, sa);
-                    tag_touched(u, bb, sb);
-                }
-            }
-            __syncwarp();
-
-            // Phase 3: drops; then every sample's weight gather in flight
-            // together; then the saturation gate, counts, sums and records.
-            uint32_t vox[kChunk];
-#pragma unroll
-            for (int j = 0; j < kChunk; ++j) {
-                vox[j] = kNoVoxel;
-                if (st[j] & kValid) {
-                    const uint32_t q = (st[j] >> kRunShift) & 15u;
-                    const int32_t bi = run_bi[q][wbase + run_src[q][t]];
-                    if (bi < 0) {
-                        if (counts_drops) ++drops;
-                    } else {
-                        vox[j] = (uint32_t)bi * kBlockVoxels + (st[j] & kLvMask);
-                    }
-                }
-            }
-            if (RECORDS) {
-                float w0[kChunk];
-#pragma unroll
-                for (int j = 0; j < kChunk; ++j)
-                    w0[j] = (sat_check && vox[j] != kNoVoxel) ? weight_at<S>(v, vox[j]) : 0.0f;
-#pragma unroll
-                for (int j = 0; j < kChunk; ++j) {
-                    if (c0 + j > v.steps) break;
-                    uint32_t out = kNoVoxel;
-                    if (vox[j] != kNoVoxel && !(sat_check && w0[j] >= v.weight_cap)) {
-                        out = vox[j];
-                        long long fix;
-                        if constexpr (S == kStoreF64) {
-                            // The oracle's value of the same sample, in double.
-                            const long long key = run_key[(st[j] >> kRunShift) & 15u][t];
-                            const uint32_t lv = st[j] & kLvMask;
-                            const int vx = unpack_axis(key, 2 * kCoordBits) * kBlockDim + (int)(lv & 7u);
-                            const int vy = unpack_axis(key, kCoordBits) * kBlockDim + (int)((lv >> 3) & 7u);
-                            const int vz = unpack_axis(key, 0) * kBlockDim + (int)(lv >> 6);
-                            fix = to_fix(clamp_sdf_n_f64(sdf_f64(v, a, r.px, r.py, r.pz, vx, vy, vz), v.trunc));
-                        } else {
-                            fix = to_fix(fminf(fmaxf(__fmul_rn(sd[j], v.inv_trunc), -1.0f), 1.0f));
-                        }
-                        red_add(&u.vcnt[out], 1u);
-                        red_add(&u.vacc[out], (unsigned long long)fix);
-                        ++counted;
-                    }
-                    if (i < a.n) __stcs(rec, out);  // read again only for crossing voxels
-                    rec += a.n;
-                }
-            }
-            __syncwarp();  // run columns are rewritten by the next chunk
-        }
+        band_point<MODE, RECORDS, S>(v, a, u, i, px, py, pz, sm, drops, counted, hist, n_bins);
     }
 
     // Counters: one global atomic per CTA (per-warp atomics on one line serialise).
@@ -316,6 +348,105 @@ band_kernel(DevVolume v, BatchArgs a, UpdateScratch u, unsigned long long* hist,
     __syncthreads();
     if (t == 0 && s_drops) atomicAdd(v.drop_count, (unsigned long long)s_drops);
     if (t == 0 && s_counted) atomicAdd(&u.ctl->n_records, (int)s_counted);
+}
+
+// ---- batched steps -----------------------------------------------------
+
+// Copy a POD descriptor into shared memory with the whole CTA.
+template <typename T>
+__device__ __forceinline__ void cta_copy(T* dst, const T* src) {
+    static_assert(sizeof(T) % 4 == 0, "descriptor copies go by words");
+    const uint32_t* s = reinterpret_cast<const uint32_t*>(src);
+    uint32_t* d = reinterpret_cast<uint32_t*>(dst);
+    for (int k = threadIdx.x; k < (int)(sizeof(T) / 4); k += blockDim.x) d[k] = s[k];
+}
+
+// Scene of global work item `item` given the per-scene item prefix `begin`
+// (n + 1 entries, begin[0] = 0): the last scene whose range starts at or
+// before it.
+__device__ __forceinline__ int scene_of(const int* begin, int n, int item) {
+    int lo = 0, hi = n;  // begin[lo] <= item < begin[hi]
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (begin[mid] <= item) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Allocate + count-and-sum walk of every scene of a step. Work items are
+// runs of tiles_per_item consecutive 128-point tiles of one scene, handed
+// out by an atomic queue to a persistent grid; the CTA keeps the current
+// item's scene descriptor in shared memory and flushes its per-scene
+// counters whenever it moves to another scene.
+template <int S, int PROBE>
+__global__ void __launch_bounds__(kBandThreads, kBandMinBlocks)
+band_multi_kernel(StepWork w) {
+    __shared__ BandSmem sm;
+    __shared__ SceneWork sw;
+    __shared__ int s_begin[kMaxBatchScenes + 1];
+    __shared__ int s_item;
+    __shared__ unsigned s_drops, s_counted;
+    const int t = threadIdx.x, lane = t & 31;
+    launch_dependents();
+    grid_dependency_wait();
+    if (t == 0) {
+        int acc = 0;
+        s_begin[0] = 0;
+        for (int k = 0; k < w.n_scenes; ++k) {
+            acc += (w.scenes[k].band_tiles + w.band_tiles_per_item - 1) / w.band_tiles_per_item;
+            s_begin[k + 1] = acc;
+        }
+        s_drops = 0u;
+        s_counted = 0u;
+    }
+    __syncthreads();
+    const int total = s_begin[w.n_scenes];
+    int cur = -1;
+    uint32_t drops = 0u, counted = 0u;
+    for (;;) {
+        if (t == 0) s_item = (int)atomicAdd(&w.queues[kQBand], 1u);
+        __syncthreads();
+        const int item = s_item;
+        const bool done = item >= total;  // also on a CTA's first pull when items are few
+        const int sc = done ? -1 : scene_of(s_begin, w.n_scenes, item);
+        if (sc != cur || done) {
+            // Flush the counters of the scene left behind, then load the next one.
+            const unsigned wd = __reduce_add_sync(0xffffffffu, drops);
+            const unsigned wc = __reduce_add_sync(0xffffffffu, counted);
+            if (lane == 0 && wd) atomicAdd(&s_drops, wd);
+            if (lane == 0 && wc) atomicAdd(&s_counted, wc);
+            __syncthreads();
+            if (t == 0 && cur >= 0) {
+                if (s_drops) atomicAdd(sw.v.drop_count, (unsigned long long)s_drops);
+                if (s_counted) atomicAdd(&sw.u.ctl->n_records, (int)s_counted);
+            }
+            __syncthreads();
+            if (t == 0) {
+                s_drops = 0u;
+                s_counted = 0u;
+            }
+            drops = counted = 0u;
+            if (done) break;
+            cta_copy(&sw, &w.scenes[sc]);
+            __syncthreads();
+            cur = sc;
+        }
+        const int first = (item - s_begin[sc]) * w.band_tiles_per_item;
+        const int last = min(first + w.band_tiles_per_item, sw.band_tiles);
+        for (int tile = first; tile < last; ++tile) {
+            const int i = tile * kBandThreads + t;
+            float px = 0.0f, py = 0.0f, pz = 0.0f;
+            if (i < sw.a.n) {
+                px = sw.a.pos[(size_t)i * 3 + 0];
+                py = sw.a.pos[(size_t)i * 3 + 1];
+                pz = sw.a.pos[(size_t)i * 3 + 2];
+            }
+            band_point<kAllocInsert, true, S, PROBE>(sw.v, sw.a, sw.u, i, px, py, pz, sm, drops, counted,
+                                                    nullptr, 0);
+        }
+        __syncthreads();  // s_item and the descriptor are rewritten next
+    }
 }
 
 template <int MODE, bool RECORDS, int S = kStoreF32>
@@ -367,6 +498,36 @@ cudaError_t launch_band_records(const DevVolume& v, const BatchArgs& a, const Up
         default:
             return insert ? launch<kAllocInsert, true>(v, a, u, nullptr, 0, sm_count, s)
                           : launch<kLookupOnly, true>(v, a, u, nullptr, 0, sm_count, s);
+    }
+}
+
+namespace {
+template <int S, int PROBE>
+cudaError_t launch_band_multi_t(const StepWork& w, int sm_count, cudaStream_t s) {
+    static int per_sm = 0;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, band_multi_kernel<S, PROBE>,
+                                                          kBandThreads, 0) != cudaSuccess ||
+            per_sm < 1)
+            per_sm = 1;
+    });
+    return launch_after(band_multi_kernel<S, PROBE>, per_sm * sm_count, kBandThreads, s, w);
+}
+}  // namespace
+
+cudaError_t launch_band_multi(const StepWork& w, int storage, int probe, int sm_count, cudaStream_t s) {
+    const bool lane = probe == kProbeLane;
+    switch (storage) {
+        case kStoreF16U16:
+            return lane ? launch_band_multi_t<kStoreF16U16, kProbeLane>(w, sm_count, s)
+                        : launch_band_multi_t<kStoreF16U16, kProbeWarp>(w, sm_count, s);
+        case kStoreF64:
+            return lane ? launch_band_multi_t<kStoreF64, kProbeLane>(w, sm_count, s)
+                        : launch_band_multi_t<kStoreF64, kProbeWarp>(w, sm_count, s);
+        default:
+            return lane ? launch_band_multi_t<kStoreF32, kProbeLane>(w, sm_count, s)
+                        : launch_band_multi_t<kStoreF32, kProbeWarp>(w, sm_count, s);
     }
 }
 

@@ -316,6 +316,10 @@ template <int S>
 __device__ __forceinline__ uint32_t slot_record(const DevVolume& v, const BatchArgs& a, uint32_t slot,
                                                 long long& fix) {
     const uint32_t n_steps = 2u * (uint32_t)v.steps + 1u;
+    if (a.n <= 0) {  // no batch: nothing to recompute (never a valid record)
+        fix = 0;
+        return 0xFFFFFFFFu;
+    }
     const uint32_t s = slot / (uint32_t)a.n, i = slot - s * (uint32_t)a.n;
     Ray r;
     int vx = 0, vy = 0, vz = 0;
@@ -332,16 +336,13 @@ __device__ __forceinline__ uint32_t slot_record(const DevVolume& v, const BatchA
 
 constexpr int kGroupPerThread = 8;  // records per thread (two 128-bit loads)
 
-__global__ void __launch_bounds__(kGroupThreads)
-group_kernel(UpdateScratch u, uint32_t n_slots) {
-    launch_dependents();
-    grid_dependency_wait();
-    if (u.ctl->def_lists == 0ull) return;  // no voxel crossed the cap in this batch
+// Eight band slots from `first` of one batch: records of voxels that
+// reserved a group take the next place of the group.
+__device__ __forceinline__ void group_slots(const UpdateScratch& u, uint32_t first, uint32_t n_slots) {
     // Eight consecutive band slots per thread (same step, neighbouring points,
     // so mostly the same block): the block-tag gathers of distinct blocks in
     // flight together, then the (rare) records of crossing voxels take the
     // next place of their voxel's group with their band slot.
-    const uint32_t first = (blockIdx.x * kGroupThreads + threadIdx.x) * kGroupPerThread;
     if (first >= n_slots) return;
     uint32_t vi[kGroupPerThread];
     if (first + kGroupPerThread <= n_slots) {
@@ -376,6 +377,14 @@ group_kernel(UpdateScratch u, uint32_t n_slots) {
         if (tk < u.vcnt[vi[m]]) u.deferred[(size_t)(hi[m] - 1u) + tk] = first + m;
         else atomicOr(u.status, kStatusScratchOverflow);  // state left by a failed update
     }
+}
+
+__global__ void __launch_bounds__(kGroupThreads)
+group_kernel(UpdateScratch u, uint32_t n_slots) {
+    launch_dependents();
+    grid_dependency_wait();
+    if (u.ctl->def_lists == 0ull) return;  // no voxel crossed the cap in this batch
+    group_slots(u, (blockIdx.x * kGroupThreads + threadIdx.x) * kGroupPerThread, n_slots);
 }
 
 // ---- values --------------------------------------------------------------
@@ -575,6 +584,261 @@ deferred_kernel(DevVolume v, UpdateScratch u) {
     cta_add(&s_updated, updated, &u.ctl->n_updated);
 }
 
+// ---- batched steps -----------------------------------------------------
+
+template <typename T>
+__device__ __forceinline__ void cta_copy(T* dst, const T* src) {
+    static_assert(sizeof(T) % 4 == 0, "descriptor copies go by words");
+    const uint32_t* a = reinterpret_cast<const uint32_t*>(src);
+    uint32_t* d = reinterpret_cast<uint32_t*>(dst);
+    for (int k = threadIdx.x; k < (int)(sizeof(T) / 4); k += blockDim.x) d[k] = a[k];
+}
+
+// Scene of global work item `item` given the per-scene item prefix `begin`
+// (n + 1 entries, begin[0] = 0).
+__device__ __forceinline__ int scene_of(const int* begin, int n, int item) {
+    int lo = 0, hi = n;  // begin[lo] <= item < begin[hi]
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (begin[mid] <= item) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Start of a step: every scene's update counters and the step's queues to
+// zero (one CTA).
+__global__ void batch_prepare_kernel(StepWork w) {
+    grid_dependency_wait();
+    constexpr int kWords = (int)(sizeof(UpdateControl) / 4);
+    for (int k = threadIdx.x; k < w.n_scenes * kWords; k += blockDim.x) {
+        const SceneWork& sw = w.scenes[k / kWords];
+        if (sw.band_tiles > 0)  // idle scenes keep their last update's counters
+            reinterpret_cast<uint32_t*>(sw.u.ctl)[k % kWords] = 0u;
+    }
+    if (threadIdx.x < kNumBatchQueues) w.queues[threadIdx.x] = 0u;
+    __syncthreads();
+    launch_dependents();
+}
+
+// Work items a pass has in one scene (read by thread 0 after the previous
+// pass completed).
+enum MultiPass : int { kPassFinishPairs, kPassFinishSingle, kPassGroup, kPassValues, kPassDeferred };
+
+template <int PASS>
+__device__ __forceinline__ int scene_items(const SceneWork& sw) {
+    // A scene sitting this step out still holds its previous update's
+    // counters (and an empty batch): it has no work in any pass.
+    if (sw.band_tiles <= 0) return 0;
+    const UpdateControl* c = sw.u.ctl;
+    if (PASS == kPassFinishPairs || PASS == kPassFinishSingle) {
+        const int nt = min(c->n_touched, sw.v.pool_capacity);
+        return PASS == kPassFinishPairs ? (nt + 1) / 2 : nt;
+    }
+    if (c->def_lists == 0ull) return 0;  // no voxel crossed the cap in this scene
+    if (PASS == kPassGroup)
+        return (int)(((uint32_t)sw.n_slots + kGroupThreads * kGroupPerThread - 1) /
+                     (kGroupThreads * kGroupPerThread));
+    if (PASS == kPassValues) {
+        const long long x = min((long long)c->x_used, (long long)sw.u.record_cap);
+        return (int)((x + kGroupThreads - 1) / kGroupThreads);
+    }
+    // Deferred: one warp item per large group and per pair of small groups.
+    const int n_small = (int)(c->def_lists & 0xFFFFFFFFull), n_large = (int)(c->def_lists >> 32);
+    if ((long long)n_small + n_large > (long long)sw.u.dvox_cap) return 0;  // overflowed
+    return n_large + (n_small + 1) / 2;
+}
+
+template <int PASS>
+__device__ __forceinline__ void scene_prefix(const StepWork& w, int* begin) {
+    if (threadIdx.x == 0) {
+        int acc = 0;
+        begin[0] = 0;
+        for (int k = 0; k < w.n_scenes; ++k) {
+            acc += scene_items<PASS>(w.scenes[k]);
+            begin[k + 1] = acc;
+        }
+    }
+    __syncthreads();
+}
+
+// Finish every touched block of every scene: work items of one or two
+// blocks from an atomic queue, the item's scene descriptor staged in shared
+// memory (reloaded when the CTA moves to another scene).
+template <int S, bool PAIR>
+__global__ void __launch_bounds__(kFinishThreads)
+finish_multi_kernel(StepWork w) {
+    __shared__ SceneWork sw;
+    __shared__ int s_begin[kMaxBatchScenes + 1];
+    __shared__ int s_item, s_updated;
+    const int t = threadIdx.x, lane = t & 31;
+    launch_dependents();
+    grid_dependency_wait();
+    if (t == 0) s_updated = 0;
+    scene_prefix<PAIR ? kPassFinishPairs : kPassFinishSingle>(w, s_begin);
+    const int total = s_begin[w.n_scenes];
+    int cur = -1, updated = 0;
+    for (;;) {
+        if (t == 0) s_item = (int)atomicAdd(&w.queues[kQFinish], 1u);
+        __syncthreads();
+        const int item = s_item;
+        const bool done = item >= total;  // also on a CTA's first pull when items are few
+        const int sc = done ? -1 : scene_of(s_begin, w.n_scenes, item);
+        if (sc != cur || done) {
+            // Statistics of the scene left behind, then the next descriptor.
+            const int wsum = __reduce_add_sync(0xffffffffu, updated);
+            if (lane == 0 && wsum) atomicAdd(&s_updated, wsum);
+            __syncthreads();
+            if (t == 0 && cur >= 0 && s_updated) atomicAdd(&sw.u.ctl->n_updated, s_updated);
+            __syncthreads();
+            if (t == 0) s_updated = 0;
+            updated = 0;
+            if (done) break;
+            cta_copy(&sw, &w.scenes[sc]);
+            __syncthreads();
+            cur = sc;
+        }
+        const int n_touched = min(sw.u.ctl->n_touched, sw.v.pool_capacity);
+        const int local = item - s_begin[sc];
+        const int ia = PAIR ? 2 * local : local;
+        const int ib = ia + 1;
+        const bool has_b = PAIR && ib < n_touched;  // uniform across the CTA
+        const int32_t ba = sw.u.touched[ia];
+        const int32_t bb = has_b ? sw.u.touched[ib] : ba;
+        const size_t qa = (size_t)ba * (kBlockVoxels / 4) + t;
+        const size_t qb = (size_t)bb * (kBlockVoxels / 4) + t;
+        uint4 ca, cb;
+        Quad<S> xa, xb;
+        ulonglong2 a01, a23, b01, b23;
+        load_item<S>(sw.v, sw.u, qa, ca, xa, a01, a23);
+        if (has_b) load_item<S>(sw.v, sw.u, qb, cb, xb, b01, b23);
+        finish_quad<S>(sw.v, sw.u, ba, qa, t, lane, ca, xa, a01, a23, updated);
+        if (has_b) finish_quad<S>(sw.v, sw.u, bb, qb, t, lane, cb, xb, b01, b23, updated);
+        __syncthreads();  // s_item and the descriptor are rewritten next
+    }
+}
+
+// Group the records of every scene that has cap-crossing voxels.
+__global__ void __launch_bounds__(kGroupThreads)
+group_multi_kernel(StepWork w) {
+    __shared__ UpdateScratch su;
+    __shared__ int s_begin[kMaxBatchScenes + 1];
+    __shared__ int s_item;
+    __shared__ uint32_t s_slots;
+    const int t = threadIdx.x;
+    launch_dependents();
+    grid_dependency_wait();
+    scene_prefix<kPassGroup>(w, s_begin);
+    const int total = s_begin[w.n_scenes];
+    int cur = -1;
+    for (;;) {
+        if (t == 0) s_item = (int)atomicAdd(&w.queues[kQGroup], 1u);
+        __syncthreads();
+        const int item = s_item;
+        if (item >= total) break;
+        const int sc = scene_of(s_begin, w.n_scenes, item);
+        if (sc != cur) {
+            cta_copy(&su, &w.scenes[sc].u);
+            if (t == 0) s_slots = (uint32_t)w.scenes[sc].n_slots;
+            __syncthreads();
+            cur = sc;
+        }
+        const uint32_t first = ((uint32_t)(item - s_begin[sc]) * kGroupThreads + t) * kGroupPerThread;
+        group_slots(su, first, s_slots);
+        __syncthreads();
+    }
+}
+
+// Ids and values of every scene's grouped records.
+template <int S>
+__global__ void __launch_bounds__(kGroupThreads)
+values_multi_kernel(StepWork w) {
+    __shared__ SceneWork sw;
+    __shared__ int s_begin[kMaxBatchScenes + 1];
+    __shared__ int s_item;
+    const int t = threadIdx.x;
+    launch_dependents();
+    grid_dependency_wait();
+    scene_prefix<kPassValues>(w, s_begin);
+    const int total = s_begin[w.n_scenes];
+    int cur = -1;
+    for (;;) {
+        if (t == 0) s_item = (int)atomicAdd(&w.queues[kQValues], 1u);
+        __syncthreads();
+        const int item = s_item;
+        if (item >= total) break;
+        const int sc = scene_of(s_begin, w.n_scenes, item);
+        if (sc != cur) {
+            cta_copy(&sw, &w.scenes[sc]);
+            __syncthreads();
+            cur = sc;
+        }
+        const uint32_t n = (uint32_t)min((long long)sw.u.ctl->x_used, (long long)sw.u.record_cap);
+        const uint32_t k = (uint32_t)(item - s_begin[sc]) * kGroupThreads + t;
+        if (k < n) {
+            long long fix;
+            const uint32_t id = slot_record<S>(sw.v, sw.a, sw.u.deferred[k], fix);
+            sw.u.deferred[k] = id;
+            sw.u.deferred_fix[k] = fix;
+        }
+        __syncthreads();
+    }
+}
+
+// Select and finish every scene's cap-crossing voxels: warp work items, one
+// per large group and one per pair of small groups.
+template <int S>
+__global__ void __launch_bounds__(kDeferThreads)
+deferred_multi_kernel(StepWork w) {
+    __shared__ uint32_t hist[kDeferWarps][256];
+    __shared__ int s_begin[kMaxBatchScenes + 1];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    launch_dependents();
+    grid_dependency_wait();
+    scene_prefix<kPassDeferred>(w, s_begin);
+    const int total = s_begin[w.n_scenes];
+    for (;;) {
+        int item = 0;
+        if (lane == 0) item = (int)atomicAdd(&w.queues[kQDeferred], 1u);
+        item = __shfl_sync(0xffffffffu, item, 0);
+        if (item >= total) break;
+        const int sc = scene_of(s_begin, w.n_scenes, item);
+        const SceneWork& sw = w.scenes[sc];
+        const DevVolume& v = sw.v;
+        const UpdateScratch& u = sw.u;
+        const unsigned long long lists = u.ctl->def_lists;
+        const int n_small = (int)(lists & 0xFFFFFFFFull), n_large = (int)(lists >> 32);
+        const int local = item - s_begin[sc];
+        int done = 0;
+        if (local < n_large) {
+            const int4 e = u.dvox[u.dvox_cap - 1 - local];
+            const long long fix = warp_select(u.deferred + (uint32_t)e.y, u.deferred_fix + (uint32_t)e.y,
+                                              e.z, e.w, hist[warp], lane);
+            if (lane == 0) finish_voxel<S>(v, u, (uint32_t)e.x, e.w, fix);
+            done = 1;
+        } else {
+            const int half = lane >> 4, hl = lane & 15;
+            const int d0 = 2 * (local - n_large);
+            const int d = d0 + half;
+            const bool live = d < n_small;
+            const int4 e = live ? u.dvox[d] : make_int4(0, 0, 0, 0);
+            const int n = e.z, keep = e.w;
+            const bool mine = live && hl < n;
+            const uint32_t id = mine ? u.deferred[(uint32_t)e.y + hl] : 0xFFFFFFFFu;
+            const long long val = mine ? u.deferred_fix[(uint32_t)e.y + hl] : 0ll;
+            int rank = 0;
+#pragma unroll
+            for (int src = 0; src < 16; ++src) rank += __shfl_sync(0xffffffffu, id, src, 16) < id ? 1 : 0;
+            long long fix = (mine && rank < keep) ? val : 0ll;
+#pragma unroll
+            for (int o = 8; o > 0; o >>= 1) fix += __shfl_xor_sync(0xffffffffu, fix, o, 16);
+            if (live && hl == 0) finish_voxel<S>(v, u, (uint32_t)e.x, keep, fix);
+            done = d0 + 1 < n_small ? 2 : 1;
+        }
+        if (lane == 0) atomicAdd(&u.ctl->n_updated, done);
+    }
+}
+
 }  // namespace
 
 // CTAs of Kernel resident at once on the device (one wave), queried once
@@ -639,6 +903,65 @@ cudaError_t launch_deferred(const DevVolume& v, const UpdateScratch& u, int sm_c
             return launch_after(deferred_kernel<kStoreF32>, resident_grid<deferred_kernel<kStoreF32>>(kDeferThreads, sm_count),
                                 kDeferThreads, s, v, u);
         }
+    }
+}
+
+cudaError_t launch_batch_prepare(const StepWork& w, cudaStream_t s) {
+    return launch_after(batch_prepare_kernel, 1, 256, s, w);
+}
+
+namespace {
+template <int S, bool P>
+cudaError_t finish_multi_t(const StepWork& w, int sm_count, cudaStream_t s) {
+    return launch_after(finish_multi_kernel<S, P>,
+                        resident_grid<finish_multi_kernel<S, P>>(kFinishThreads, sm_count),
+                        kFinishThreads, s, w);
+}
+template <int S>
+cudaError_t values_multi_t(const StepWork& w, int sm_count, cudaStream_t s) {
+    return launch_after(values_multi_kernel<S>, resident_grid<values_multi_kernel<S>>(kGroupThreads, sm_count),
+                        kGroupThreads, s, w);
+}
+template <int S>
+cudaError_t deferred_multi_t(const StepWork& w, int sm_count, cudaStream_t s) {
+    return launch_after(deferred_multi_kernel<S>,
+                        resident_grid<deferred_multi_kernel<S>>(kDeferThreads, sm_count), kDeferThreads, s,
+                        w);
+}
+}  // namespace
+
+cudaError_t launch_finish_multi(const StepWork& w, int storage, int pair, int sm_count, cudaStream_t s) {
+    switch (storage) {
+        case kStoreF16U16:
+            return pair ? finish_multi_t<kStoreF16U16, true>(w, sm_count, s)
+                        : finish_multi_t<kStoreF16U16, false>(w, sm_count, s);
+        case kStoreF64:
+            return pair ? finish_multi_t<kStoreF64, true>(w, sm_count, s)
+                        : finish_multi_t<kStoreF64, false>(w, sm_count, s);
+        default:
+            return pair ? finish_multi_t<kStoreF32, true>(w, sm_count, s)
+                        : finish_multi_t<kStoreF32, false>(w, sm_count, s);
+    }
+}
+
+cudaError_t launch_group_multi(const StepWork& w, int sm_count, cudaStream_t s) {
+    return launch_after(group_multi_kernel, resident_grid<group_multi_kernel>(kGroupThreads, sm_count),
+                        kGroupThreads, s, w);
+}
+
+cudaError_t launch_values_multi(const StepWork& w, int storage, int sm_count, cudaStream_t s) {
+    switch (storage) {
+        case kStoreF16U16: return values_multi_t<kStoreF16U16>(w, sm_count, s);
+        case kStoreF64: return values_multi_t<kStoreF64>(w, sm_count, s);
+        default: return values_multi_t<kStoreF32>(w, sm_count, s);
+    }
+}
+
+cudaError_t launch_deferred_multi(const StepWork& w, int storage, int sm_count, cudaStream_t s) {
+    switch (storage) {
+        case kStoreF16U16: return deferred_multi_t<kStoreF16U16>(w, sm_count, s);
+        case kStoreF64: return deferred_multi_t<kStoreF64>(w, sm_count, s);
+        default: return deferred_multi_t<kStoreF32>(w, sm_count, s);
     }
 }
 

@@ -332,6 +332,27 @@ int32_t Volume::extract(float* posnor, uint8_t* rgb, int32_t cap, float min_w, f
     return n;
 }
 
+bool Volume::reserve_batch(int32_t max_points) {
+    return max_points > 0 && ensure_records(batch_records(max_points, dv_.steps));
+}
+
+SceneWork Volume::batch_work(const BatchArgs& a, cudaStream_t s) {
+    // Block tags are update numbers; at the (theoretical) wrap, clear them.
+    if (++update_tag_ == 0u) {
+        cudaMemsetAsync(us_.blk_touch, 0, (size_t)dv_.pool_capacity * sizeof(uint32_t), s);
+        cudaMemsetAsync(us_.blk_cross, 0, (size_t)dv_.pool_capacity * sizeof(uint32_t), s);
+        update_tag_ = 1u;
+    }
+    SceneWork w{};
+    w.v = dv_;
+    w.a = a;
+    w.u = us_;
+    w.u.tag = update_tag_;
+    w.band_tiles = (a.n + kBatchTilePoints - 1) / kBatchTilePoints;
+    w.n_slots = (int32_t)batch_records(a.n, dv_.steps);
+    return w;
+}
+
 cudaError_t Volume::reset() {
     const int32_t n_blocks = std::min(block_count(), dv_.pool_capacity);
     mark_start(kKReset);

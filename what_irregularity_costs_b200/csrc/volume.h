@@ -11,6 +11,8 @@
 
 namespace osn_b200 {
 
+struct SceneWork;  // one volume's part of a batched step (below)
+
 // Kernel ids for the timing table (documented in include/osn_tsdf_b200.h).
 enum KernelId : int {
     kKAllocate = 0,      // allocate-only band walk
@@ -108,6 +110,12 @@ public:
     void synchronize() { cudaStreamSynchronize(stream_); }
     bool last_update_stats(int64_t out[4]);
 
+    // Batched steps: make room for batches of up to max_points points (call
+    // before any stream capture), then describe one batch for a batched
+    // step on stream s (takes the next update number).
+    bool reserve_batch(int32_t max_points);
+    SceneWork batch_work(const BatchArgs& a, cudaStream_t s);
+
     // Timing.
     void set_timing(bool on) { timing_ = on; }
     int kernel_times(double* ms, int64_t* launches, int n_ids);
@@ -193,3 +201,48 @@ cudaError_t launch_deferred(const DevVolume& v, const UpdateScratch& u, int sm_c
 // The Volume behind a C-ABI handle, or nullptr when the handle is NULL or invalid.
 struct OsnTsdfCudaVolume;
 osn_b200::Volume* osn_tsdf_b200_volume_of(OsnTsdfCudaVolume* v);
+
+namespace osn_b200 {
+
+// ---- batched steps: many volumes integrate one frame each per step -------
+
+constexpr int kMaxBatchScenes = 64;
+constexpr int kBatchTilePoints = 128;  // points per band tile (the band CTA size)
+constexpr int kBandTilesPerItemMax = 8;
+
+// One scene of a batched step (device memory, rewritten every step).
+struct SceneWork {
+    DevVolume v;
+    BatchArgs a;
+    UpdateScratch u;
+    int32_t band_tiles;  // ceil(a.n / kBandThreads); 0 when the scene is idle this step
+    int32_t n_slots;     // band slots a.n * (2 * steps + 1)
+};
+
+// Work queues of one step, one counter per pass (zeroed by the prepare pass).
+enum BatchQueue : int { kQBand = 0, kQFinish, kQGroup, kQValues, kQDeferred, kNumBatchQueues };
+
+// Tunable shape of a batched step (chosen by the batch autotuner).
+struct BatchShape {
+    int band_tiles_per_item = 4;  // band work item: this many 128-point tiles of one scene
+    int probe = 0;                // 0: warp-deduplicated block resolution, 1: per-lane
+    int finish_pair = 1;          // finish work item: 1 = two touched blocks, 0 = one
+};
+
+// Everything a batched pass reads: the scene table and the queues.
+struct StepWork {
+    SceneWork* scenes;     // [n_scenes]
+    int32_t n_scenes;
+    int32_t band_tiles_per_item;
+    uint32_t* queues;      // [kNumBatchQueues]
+    uint32_t* status;      // batch status word (bounded waits, overflows)
+};
+
+cudaError_t launch_batch_prepare(const StepWork& w, cudaStream_t s);
+cudaError_t launch_band_multi(const StepWork& w, int storage, int probe, int sm_count, cudaStream_t s);
+cudaError_t launch_finish_multi(const StepWork& w, int storage, int pair, int sm_count, cudaStream_t s);
+cudaError_t launch_group_multi(const StepWork& w, int sm_count, cudaStream_t s);
+cudaError_t launch_values_multi(const StepWork& w, int storage, int sm_count, cudaStream_t s);
+cudaError_t launch_deferred_multi(const StepWork& w, int storage, int sm_count, cudaStream_t s);
+
+}  // namespace osn_b200
