@@ -487,6 +487,202 @@ def run_ours(args):
     return 0
 
 
+def run_batch32(args):
+    """The 32-scene batched mix (what_irregularity_costs_b200.workloads): every
+    scene advances one frame per step. Arms, each timed with CUDA events over
+    the same steps after the same warm-up frames:
+      value        batched, FP16 TSDF + uint16 weight, autotuned shape, steps
+                   replayed from a CUDA graph (device-resident frames);
+      plain_fp32   each scene integrated alone through osn_tsdf_cuda_integrate
+                   (its own stream), FP32 storage -- the plain drop-in arm;
+      batched_fp32 the batched arm with FP32 storage;
+      e2e          the batched arm with every frame copied from pinned host
+                   memory on the batch stream inside the timed region;
+      precision    max / RMS TSDF error (m) of the FP16 batch against FP64
+                   volumes fed the same frames, first 8 scenes.
+    """
+    from what_irregularity_costs_b200 import workloads
+    specs = workloads.scene_mix(32)
+    n_steps = args.warmup + args.steps
+    frames = workloads.mix_frames(specs, n_steps)  # before any CUDA use
+    import torch
+    from what_irregularity_costs_b200 import (STORAGE_FP16_U16, STORAGE_FP32, STORAGE_FP64, Batch,
+                                              device_tensor, precision)
+    rank, local, world, dist = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    dev = workloads.upload(frames, torch)
+    active = [[s.index for s in specs if k < len(frames[s.index])] for k in range(n_steps)]
+    timed_frames = sum(len(active[k]) for k in range(args.warmup, n_steps))
+
+    def batched(storage, tune, graph=True, e2e=False, shape=None):
+        vols = workloads.make_volumes(specs, storage)
+        b = Batch(len(specs))
+        for v, sp in zip(vols, specs):
+            b.add(v, sp.max_points)
+        if shape is not None:
+            b.set_shape(shape["tiles_per_item"], 1 if shape["probe"] == "lane" else 0,
+                        1 if shape["finish_pair"] else 0)
+        bstream = torch.cuda.ExternalStream(b.stream_handle())
+        tune_res = None
+        if tune:  # live autotuning steps (results do not depend on the shape), then reset
+            b.autotune(1)
+            for k in range(16):
+                kk = k % n_steps
+                for si in active[kk]:
+                    b.set_frame(si, dev[si][kk], frames[si][kk][1])
+                b.step()
+            tune_res = b.tune_results()
+            b.synchronize()
+            for v in vols:
+                v.reset()
+        b.set_graph(graph)
+        stage = host = None
+        if e2e:
+            stage = [torch.empty((sp.max_points, 3), dtype=torch.float32, device="cuda") for sp in specs]
+            host = [[torch.from_numpy(p).pin_memory() for p, _ in fr] for fr in frames]
+            view = vols[0].device_view()
+            bc_dev = device_tensor(view.block_count, (1,), "<i4")
+            bc_host = torch.zeros(1, dtype=torch.int32).pin_memory()
+        h2d = [0]
+
+        def step(k):
+            for si in active[k]:
+                if e2e:
+                    n = host[si][k].shape[0]
+                    with torch.cuda.stream(bstream):
+                        stage[si][:n].copy_(host[si][k], non_blocking=True)
+                    b.set_frame(si, stage[si][:n], frames[si][k][1])
+                    if k >= args.warmup:
+                        h2d[0] += n * 12
+                else:
+                    b.set_frame(si, dev[si][k], frames[si][k][1])
+            b.step()
+            if e2e:
+                with torch.cuda.stream(bstream):
+                    bc_host.copy_(bc_dev, non_blocking=True)
+
+        for k in range(args.warmup):
+            step(k)
+        b.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(bstream)
+        for k in range(args.warmup, n_steps):
+            step(k)
+        e1.record(bstream)
+        b.synchronize()
+        ms = e0.elapsed_time(e1)
+        status = b.status()
+        out = {"value": timed_frames / (ms / 1e3), "unit": "frames/s", "ms_per_step": ms / args.steps,
+               "status": status, "shape": b.shape(), "graph": graph}
+        if e2e:
+            out["h2d_bytes_per_step"] = h2d[0] // args.steps
+            out["d2h_bytes_per_step"] = 4
+        if tune_res is not None:
+            out["tune"] = tune_res
+        return out, vols, b
+
+    # -- batched FP16 (the batched form), autotuned and graph-replayed
+    res16, vols16, b16 = batched(STORAGE_FP16_U16, tune=True)
+    shape = res16["shape"]
+    keep = list(range(8))
+    snap16 = [precision._aligned(vols16[i]) for i in keep]
+    blocks16 = [v.block_count() for v in vols16]
+    del b16, vols16
+    torch.cuda.synchronize()
+
+    # -- e2e: the same batched arm from pinned host buffers
+    res_e2e, v_e2e, b_e2e = batched(STORAGE_FP16_U16, tune=False, e2e=True, shape=shape)
+    del b_e2e, v_e2e
+    torch.cuda.synchronize()
+
+    # -- batched FP32 (same passes, reference storage)
+    res32b, v32b, b32b = batched(STORAGE_FP32, tune=False, shape=shape)
+    blocks32b = [v.block_count() for v in v32b]
+    del b32b, v32b
+    torch.cuda.synchronize()
+
+    # -- plain FP32 arm: every scene alone through the drop-in ABI, own streams
+    vols = workloads.make_volumes(specs, STORAGE_FP32)
+    streams = [torch.cuda.ExternalStream(v.stream_handle()) for v in vols]
+    join = torch.cuda.Stream()
+
+    def plain_step(k):
+        for si in active[k]:
+            vols[si].integrate(dev[si][k], frames[si][k][1])
+
+    for k in range(args.warmup):
+        plain_step(k)
+    torch.cuda.synchronize()
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0.record(join)
+    for st in streams:
+        st.wait_event(p0)
+    for k in range(args.warmup, n_steps):
+        plain_step(k)
+    for st in streams:
+        ev = torch.cuda.Event()
+        ev.record(st)
+        join.wait_event(ev)
+    p1.record(join)
+    torch.cuda.synchronize()
+    plain_ms = p0.elapsed_time(p1)
+    plain = {"value": timed_frames / (plain_ms / 1e3), "unit": "frames/s",
+             "ms_per_step": plain_ms / args.steps}
+    blocks_plain = [v.block_count() for v in vols]
+    snap32 = [precision._aligned(vols[i]) for i in keep]
+    del vols
+    torch.cuda.synchronize()
+
+    # -- FP64 oracle for the first 8 scenes (alone), same frames
+    errs16, errs32 = [], []
+    for i in keep:
+        sp = specs[i]
+        o = workloads.make_volumes([sp], STORAGE_FP64)[0]
+        for k in range(len(frames[i])):
+            o.integrate(dev[i][k], frames[i][k][1])
+        co, mo, wo = precision._aligned(o)
+        for snap, errs in ((snap16[i], errs16), (snap32[i], errs32)):
+            c, m, w = snap
+            if c.shape != co.shape or not np.array_equal(c, co) or not np.array_equal(w, wo):
+                errs.append({"scene": i, "mismatch": True})
+                continue
+            seen = wo > 0
+            e = np.abs(m[seen] - mo[seen]) * sp.trunc
+            errs.append({"scene": i, "max_m": float(e.max()) if e.size else 0.0,
+                         "rms_m": float(np.sqrt(np.mean(e * e))) if e.size else 0.0})
+        del o
+
+    if rank == 0:
+        line = {
+            "metric": "frames/s (32-scene batched integrate)", "value": res16["value"],
+            "unit": "frames/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": res16["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f16 tsdf / u16 weight storage, f32 running average",
+            "data": "synthetic: 32 seeded room scenes (scene_mix seed 4)",
+            "config": {"workload": "32-scene mix: tables 2^14-2^20 (log-uniform), voxels 1-4 cm "
+                                   "(log-uniform), 160x120..1280x720, 8-256 frames, cap 64; step = "
+                                   "every active scene integrates its next frame",
+                       "scenes": [s.__dict__ for s in specs], "frames_in_window": timed_frames,
+                       "l2": "inputs larger than L2: %.0f MB of points in the timed steps"
+                             % (sum(dev[si][k].numel() * 4 for k in range(args.warmup, n_steps)
+                                    for si in active[k]) / 1e6)},
+            "shape": shape, "graph": True, "status": res16["status"],
+            "plain_fp32": plain, "batched_fp32": res32b,
+            "speedup_vs_plain": res16["value"] / plain["value"],
+            "blocks_identical": blocks16 == blocks32b == blocks_plain,
+            "precision_vs_fp64": {"fp16_u16": errs16, "fp32": errs32},
+            "e2e": {"value": res_e2e["value"], "unit": "frames/s",
+                    "h2d_bytes_per_step": res_e2e["h2d_bytes_per_step"],
+                    "d2h_bytes_per_step": res_e2e["d2h_bytes_per_step"]},
+            "autotune": res16.get("tune"),
+        }
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -501,8 +697,13 @@ def main():
     ap.add_argument("--frames", type=int, default=N_FRAMES,
                     help="frames of the trajectory per step (fewer: a small profiling case)")
     ap.add_argument("--pool", type=int, default=POOL, help="pool capacity in blocks")
+    ap.add_argument("--workload", choices=["room", "batch32"], default="room",
+                    help="room: the single-scene trajectory (default); batch32: the 32-scene "
+                         "batched mix")
     args = ap.parse_args()
     set_workload(args.frames, args.pool)
+    if args.workload == "batch32" and args.impl == "ours":
+        return run_batch32(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)
