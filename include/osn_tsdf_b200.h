@@ -221,6 +221,10 @@ void osn_tsdf_batch_destroy(OsnTsdfBatch* b);
  * volume's stream. Returns the scene index, or -1 (full, NULL, already
  * attached, storage mode differs from the other scenes, batch too large). */
 int32_t osn_tsdf_batch_add(OsnTsdfBatch* b, OsnTsdfCudaVolume* v, int32_t max_points);
+/* Detach a scene once the steps queued so far have run (waits for the batch
+ * stream); the volume stays valid and its slot is reused by the next add.
+ * 0 ok, 1 no such scene, 3 CUDA error. */
+int32_t osn_tsdf_batch_remove(OsnTsdfBatch* b, int32_t scene);
 /* The next step's frame of one scene: device positions (3 floats per point,
  * kept alive until the step has run), camera origin, far cutoff. Scenes
  * without a frame sit the step out. 0 ok, 1 bad arguments. */

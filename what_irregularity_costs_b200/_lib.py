@@ -72,6 +72,7 @@ _SIG = {
     "osn_tsdf_batch_create": (_P, [_I]),
     "osn_tsdf_batch_destroy": (None, [_P]),
     "osn_tsdf_batch_add": (_I, [_P, _P, _I]),
+    "osn_tsdf_batch_remove": (_I, [_P, _I]),
     "osn_tsdf_batch_set_frame": (_I, [_P, _I, _P, _I, _F, _F, _F, _F]),
     "osn_tsdf_batch_step": (_I, [_P]),
     "osn_tsdf_batch_synchronize": (_I, [_P]),

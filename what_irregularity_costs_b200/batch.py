@@ -25,7 +25,7 @@ class Batch:
         self.h = self.lib.osn_tsdf_batch_create(int(max_scenes))
         if not self.h:
             raise ValueError("osn_tsdf_batch_create failed (max_scenes must be in [1, 64])")
-        self.scenes: list[CudaVolume] = []
+        self.scenes: list[CudaVolume | None] = []  # by scene slot
         self._keep = []
 
     def close(self):
@@ -45,8 +45,19 @@ class Batch:
         if idx < 0:
             raise ValueError("osn_tsdf_batch_add rejected the volume (full, already attached, "
                              "storage mode differs, or max_points too large)")
-        self.scenes.append(vol)
+        while len(self.scenes) <= idx:
+            self.scenes.append(None)
+        self.scenes[idx] = vol
         return idx
+
+    def remove(self, scene: int):
+        """Detach a scene after the queued steps ran (its slot is reused)."""
+        rc = self.lib.osn_tsdf_batch_remove(self.h, int(scene))
+        if rc:
+            raise ValueError(f"remove: no scene {scene}" if rc == 1 else "remove: CUDA error")
+        vol = self.scenes[scene]
+        self.scenes[scene] = None
+        return vol
 
     def set_frame(self, scene: int, positions, cam: Sequence[float], radius_m: float = 0.0, n=None):
         count = _count(positions, n)

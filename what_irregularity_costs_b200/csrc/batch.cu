@@ -71,29 +71,60 @@ public:
 
     bool ok() const { return ok_; }
     cudaStream_t stream() const { return stream_; }
-    int size() const { return (int)vols_.size(); }
+    int size() const { return live_; }
 
-    // Attach a volume; every scene of a batch shares one storage mode.
+    // Attach a volume (into the first free scene slot); every scene of a
+    // batch shares one storage mode.
     int add(Volume* v, int32_t max_points) {
-        if (!v || max_points <= 0 || (int)vols_.size() >= max_scenes_) return -1;
-        if (storage_ >= 0 && v->storage() != storage_) return -1;
+        if (!v || max_points <= 0) return -1;
+        if (storage_ >= 0 && live_ > 0 && v->storage() != storage_) return -1;
         if ((int64_t)max_points * (2 * (int64_t)v->dev().steps + 1) >= (int64_t(1) << 32)) return -1;
         for (Volume* o : vols_)
             if (o == v) return -1;
+        int slot = -1;
+        for (int k = 0; k < (int)vols_.size(); ++k)
+            if (!vols_[k]) {
+                slot = k;
+                break;
+            }
+        if (slot < 0 && (int)vols_.size() >= max_scenes_) return -1;
         // Room for the largest frame now (no allocation during a step), and
         // the volume's own queued work done before the batch stream uses it.
         if (!v->reserve_batch(max_points)) return -1;
         v->synchronize();
         storage_ = v->storage();
-        vols_.push_back(v);
-        max_points_.push_back(max_points);
-        pending_.push_back(BatchArgs{});
-        drop_graph();  // the table grew
-        return (int)vols_.size() - 1;
+        if (slot < 0) {
+            slot = (int)vols_.size();
+            vols_.push_back(nullptr);
+            max_points_.push_back(0);
+            pending_.push_back(BatchArgs{});
+            drop_graph();  // the table grew
+        }
+        vols_[slot] = v;
+        max_points_[slot] = max_points;
+        pending_[slot] = BatchArgs{};
+        ++live_;
+        return slot;
+    }
+
+    // Detach a scene after the steps queued so far have run; its slot is
+    // reused by the next add.
+    int remove(int scene) {
+        if (scene < 0 || scene >= (int)vols_.size() || !vols_[scene]) return 1;
+        if (cudaStreamSynchronize(stream_) != cudaSuccess) return 3;
+        vols_[scene] = nullptr;
+        pending_[scene] = BatchArgs{};
+        --live_;
+        return 0;
+    }
+
+    Volume* volume(int scene) const {
+        return scene >= 0 && scene < (int)vols_.size() ? vols_[scene] : nullptr;
     }
 
     int set_frame(int scene, const BatchArgs& a) {
-        if (scene < 0 || scene >= (int)vols_.size() || !a.pos || a.n <= 0 || a.n > max_points_[scene])
+        if (scene < 0 || scene >= (int)vols_.size() || !vols_[scene] || !a.pos || a.n <= 0 ||
+            a.n > max_points_[scene])
             return 1;
         pending_[scene] = a;
         return 0;
@@ -109,6 +140,10 @@ public:
         if (e != cudaSuccess) return e;
         SceneWork* table = h_table_[k];
         for (int s = 0; s < n; ++s) {
+            if (!vols_[s]) {  // free slot: no work, nothing to point at
+                table[s] = SceneWork{};
+                continue;
+            }
             if (pending_[s].n > 0) {
                 table[s] = vols_[s]->batch_work(pending_[s], stream_);
             } else {
@@ -162,7 +197,8 @@ public:
                 cudaSuccess &&
             cudaStreamSynchronize(stream_) == cudaSuccess)
             st = *h_status_;
-        for (Volume* v : vols_) st |= v->status();
+        for (Volume* v : vols_)
+            if (v) st |= v->status();
         return st;
     }
 
@@ -290,6 +326,7 @@ private:
     int max_scenes_;
     int sm_count_ = 148;
     int storage_ = -1;
+    int live_ = 0;  // attached scenes
     cudaStream_t stream_ = nullptr;
     std::vector<Volume*> vols_;
     std::vector<int32_t> max_points_;
@@ -348,6 +385,12 @@ int32_t osn_tsdf_batch_add(OsnTsdfBatch* b, OsnTsdfCudaVolume* v, int32_t max_po
     osn_b200::Volume* vol = osn_tsdf_b200_volume_of(v);
     if (!x || !vol) return -1;
     return x->add(vol, max_points);
+}
+
+int32_t osn_tsdf_batch_remove(OsnTsdfBatch* b, int32_t scene) {
+    osn_b200::Batch* x = batch_of(b);
+    if (!x) return 1;
+    return x->remove(scene);
 }
 
 int32_t osn_tsdf_batch_set_frame(OsnTsdfBatch* b, int32_t scene, const float* d_positions,

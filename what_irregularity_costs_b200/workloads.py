@@ -37,6 +37,7 @@ class SceneSpec:
     width: int
     height: int
     frames: int
+    cap: float = CAP
 
     @property
     def pool(self) -> int:
@@ -92,7 +93,7 @@ def mix_frames(specs, n_steps: int, workers: int | None = None):
 
 def make_volumes(specs, storage: int):
     from .volume import CudaVolume
-    return [CudaVolume(s.voxel, s.pool, s.trunc, CAP, s.hash_slots, storage=storage) for s in specs]
+    return [CudaVolume(s.voxel, s.pool, s.trunc, s.cap, s.hash_slots, storage=storage) for s in specs]
 
 
 def upload(frames, torch):
