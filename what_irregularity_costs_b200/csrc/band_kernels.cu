@@ -45,6 +45,7 @@ namespace osn_b200 {
 namespace {
 
 constexpr int kBandThreads = kBatchTilePoints;
+static_assert(kBandThreads >= kMaxBatchScenes, "one thread per scene builds the item prefix");
 constexpr int kChunk = 9;  // samples per ray held in registers (the whole band at 4 voxels)
 constexpr int kBandMinBlocks = 8;  // resident CTAs per SM the register budget is sized for
 
@@ -390,16 +391,17 @@ band_multi_kernel(StepWork w) {
     const int t = threadIdx.x, lane = t & 31;
     launch_dependents();
     grid_dependency_wait();
+    // Item prefix: one thread per scene, then a scan (n <= 64 <= blockDim.x).
+    if (t < w.n_scenes)
+        s_begin[t + 1] = (w.scenes[t].band_tiles + w.band_tiles_per_item - 1) / w.band_tiles_per_item;
     if (t == 0) {
-        int acc = 0;
         s_begin[0] = 0;
-        for (int k = 0; k < w.n_scenes; ++k) {
-            acc += (w.scenes[k].band_tiles + w.band_tiles_per_item - 1) / w.band_tiles_per_item;
-            s_begin[k + 1] = acc;
-        }
         s_drops = 0u;
         s_counted = 0u;
     }
+    __syncthreads();
+    if (t == 0)
+        for (int k = 1; k <= w.n_scenes; ++k) s_begin[k] += s_begin[k - 1];
     __syncthreads();
     const int total = s_begin[w.n_scenes];
     int cur = -1;

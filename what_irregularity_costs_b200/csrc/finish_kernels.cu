@@ -56,7 +56,10 @@ constexpr int kFinishThreads = 128;  // 4 voxels per thread, one block per CTA p
 constexpr int kGroupThreads = 256;
 constexpr int kDeferThreads = 128;
 constexpr int kDeferWarps = kDeferThreads / 32;
-constexpr int kRankRegs = 8;  // crossing voxels of up to 256 records are ranked in registers
+constexpr int kRankRegs = 8;
+static_assert(kFinishThreads >= kMaxBatchScenes && kGroupThreads >= kMaxBatchScenes &&
+                  kDeferThreads >= kMaxBatchScenes,
+              "one thread per scene builds the item prefix");  // crossing voxels of up to 256 records are ranked in registers
 
 // Contributions a voxel accepts given its weight w0 before the batch and n
 // unit-weight records: the j-th record (0-based, canonical order) is accepted
@@ -649,16 +652,17 @@ __device__ __forceinline__ int scene_items(const SceneWork& sw) {
     return n_large + (n_small + 1) / 2;
 }
 
+// Exclusive item prefix of the scenes into begin[0..n]: one thread per scene
+// reads its counts (all in flight together), then a scan in shared memory
+// (n <= 64 <= blockDim.x).
 template <int PASS>
 __device__ __forceinline__ void scene_prefix(const StepWork& w, int* begin) {
-    if (threadIdx.x == 0) {
-        int acc = 0;
-        begin[0] = 0;
-        for (int k = 0; k < w.n_scenes; ++k) {
-            acc += scene_items<PASS>(w.scenes[k]);
-            begin[k + 1] = acc;
-        }
-    }
+    const int t = threadIdx.x;
+    if (t < w.n_scenes) begin[t + 1] = scene_items<PASS>(w.scenes[t]);
+    if (t == 0) begin[0] = 0;
+    __syncthreads();
+    if (t == 0)
+        for (int k = 1; k <= w.n_scenes; ++k) begin[k] += begin[k - 1];
     __syncthreads();
 }
 

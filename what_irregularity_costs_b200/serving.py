@@ -9,14 +9,16 @@ One host thread drives one ``Batch`` (at most 64 attached sessions):
   ``footprint_bytes``) fits both the HBM budget ledger and the device's free
   memory (``torch.cuda.mem_get_info`` minus a headroom); sessions are
   admitted first come, first served. An admitted session's volume stays
-  resident in HBM until its last request is done, then it is detached and
-  freed, which admits the next waiting sessions.
+  resident in HBM until its last request is done, then it is detached; its
+  memory is freed when a waiting session needs the room (freeing synchronises
+  the device, so it is not done while nothing waits).
 * Continuous batching. Every step takes the oldest integrate request of each
   admitted session (one frame per session per step; a session's requests
-  run in arrival order), copies the frames from pinned host memory on the
-  batch stream and queues one batched step; at most ``max_inflight`` steps
-  are on the GPU while the host forms the next, so requests that arrive
-  during a step join the next one.
+  run in arrival order), copies the frames from pinned host memory on a
+  copy stream into the session's other staging buffer (so the upload
+  overlaps the step still running) and queues one batched step after the
+  copies; at most ``max_inflight`` steps are on the GPU while the host forms
+  the next, so requests that arrive during a step join the next one.
 * Extraction. A session whose oldest request is an extract, with none of
   its frames in flight, extracts its mesh into its device buffer on its own
   stream, concurrently with the batch steps of the other sessions.
@@ -40,8 +42,16 @@ from .batch import Batch
 from .volume import CudaVolume
 
 SCRATCH_SLOTS = 1 << 20
-MESH_CAP_PER_POINT = 4  # initial extraction buffer: 4 vertices per point of the largest frame
-MESH_CAP_MAX = 1 << 26  # vertices; the buffer doubles up to this on overflow
+MESH_CAP_MAX = 1 << 26  # vertices; the extraction buffer doubles up to this on overflow
+
+
+def mesh_capacity(spec) -> int:
+    """Initial extraction buffer (vertices): a block crossed by a surface holds
+    about 64 surface cubes of ~6 vertices each; sized for the pool, between 4
+    vertices per point of the largest frame and 16M vertices. Allocating it at
+    admission keeps allocation (a device-wide synchronisation) out of the
+    serving loop; a mesh that does not fit doubles the buffer."""
+    return int(min(max(spec.pool * 384, spec.max_points * 4), 1 << 24))
 
 
 def footprint_bytes(spec, storage: int) -> int:
@@ -53,8 +63,8 @@ def footprint_bytes(spec, storage: int) -> int:
     table = (spec.hash_slots + SCRATCH_SLOTS) * 16
     pool = spec.pool * (512 * per_voxel + 12 + 4 * 3)
     scratch = n_records * (4 + 4 + 8) + (n_records // 2 + 1) * 16
-    stage = spec.max_points * 12
-    mesh = spec.max_points * MESH_CAP_PER_POINT * 24
+    stage = 2 * spec.max_points * 12  # double-buffered frame staging
+    mesh = mesh_capacity(spec) * 24
     return int(table + pool + scratch + stage + mesh)
 
 
@@ -75,7 +85,9 @@ class _Session:
     queue: deque = field(default_factory=deque)
     vol: CudaVolume | None = None
     slot: int = -1
-    stage: object = None
+    stage: object = None      # two staging buffers, alternated per frame
+    stage_ev: list = field(default_factory=lambda: [None, None])  # last step reading each
+    flip: int = 0
     mesh: object = None
     inflight: int = 0
     remaining: int = 0  # requests not yet done
@@ -100,18 +112,22 @@ class Server:
             self.batch.set_shape(*shape)
         self.autotune_steps = autotune_steps
         self.stream = torch.cuda.ExternalStream(self.batch.stream_handle())
+        self.copy_stream = torch.cuda.Stream()  # frame uploads overlap the running step
         self.ledger = 0
         self.peak_ledger = 0
         self.peak_sessions = 0
         self.steps = 0
         self.keep_volumes = False  # tests keep finished volumes for comparison
         self.finished: dict[int, CudaVolume] = {}
+        self.graveyard: list = []  # closed sessions' memory, freed lazily
 
     # -- admission -----------------------------------------------------------
     def _try_admit(self, s: _Session, now: float) -> bool:
         if self.batch is None or len([x for x in self.sessions if x.vol is not None and not x.closed]) >= 64:
             return False
         fp = footprint_bytes(s.spec, self.storage)
+        if self.ledger + fp > self.budget and self.graveyard:
+            self._bury(fp)  # release finished sessions only when the room is needed
         if self.ledger + fp > self.budget:
             return False
         free, _ = self.torch.cuda.mem_get_info()
@@ -120,9 +136,9 @@ class Server:
         sp = s.spec
         s.vol = CudaVolume(sp.voxel, sp.pool, sp.trunc, sp.cap, sp.hash_slots, storage=self.storage)
         s.slot = self.batch.add(s.vol, sp.max_points)
-        s.stage = self.torch.empty((sp.max_points, 3), dtype=self.torch.float32, device="cuda")
-        s.mesh = self.torch.empty((sp.max_points * MESH_CAP_PER_POINT, 6), dtype=self.torch.float32,
-                                  device="cuda")
+        s.stage = [self.torch.empty((sp.max_points, 3), dtype=self.torch.float32, device="cuda")
+                   for _ in range(2)]
+        s.mesh = self.torch.empty((mesh_capacity(sp), 6), dtype=self.torch.float32, device="cuda")
         s.footprint = fp
         s.admitted_at = now
         self.ledger += fp
@@ -146,21 +162,37 @@ class Server:
             self.peak_ledger = max(self.peak_ledger, self.ledger)
 
     def _close(self, s: _Session):
+        """Detach a finished session. Its memory is released lazily: freeing
+        multi-GB buffers synchronises the whole device, so the volume goes to
+        a graveyard (still on the ledger) that is emptied only when a waiting
+        session needs the room, or at the end of the run."""
         self.batch.remove(s.slot)
         if self.keep_volumes:
             self.finished[s.spec.index] = s.vol
-        else:
-            s.vol.close()
+        self.graveyard.append((s.vol, s.stage, s.mesh, s.footprint))
         s.stage = s.mesh = None
+        s.stage_ev = [None, None]
         s.closed = True
-        self.ledger -= s.footprint
+
+    def _bury(self, need_bytes: float = float("inf")):
+        """Free graveyard volumes (oldest first) until need_bytes fit the ledger."""
+        while self.graveyard and self.ledger + need_bytes > self.budget:
+            vol, stage, mesh, fp = self.graveyard.pop(0)
+            if not self.keep_volumes:
+                vol.close()
+            del stage, mesh
+            self.ledger -= fp
 
     # -- the loop ------------------------------------------------------------
-    def run(self, specs, frames, requests: list[Request], realtime: bool = True) -> dict:
+    def run(self, specs, frames, requests: list[Request], realtime: bool = True,
+            open_first: bool = False) -> dict:
         """Serve `requests` (sorted or not) for sessions `specs` whose frames
         are `frames[i]` (host (n, 3) float32 arrays and cams; frame k of a
         request uses frames[i][k % len]). realtime: requests become visible at
-        their arrival time; otherwise all at once (throughput at saturation)."""
+        their arrival time; otherwise all at once (throughput at saturation).
+        open_first: the sessions open before the first frame arrives, so every
+        session that fits is admitted before the clock starts (the time this
+        takes is reported as open_s); the rest wait for memory as usual."""
         torch = self.torch
         reqs = sorted(requests, key=lambda r: r.arrival)
         self.sessions = []
@@ -171,6 +203,16 @@ class Server:
             self.sessions[r.session].remaining += 1
         waiting: deque[_Session] = deque()
         inflight: deque = deque()  # (event, [requests])
+        self.t_tuned = 0.0
+        self.t_admitted = 0.0  # last admission
+        self.open_s = 0.0
+        if open_first:
+            t_open = time.perf_counter()
+            for sess in self.sessions:
+                if not self._try_admit(sess, 0.0):
+                    break  # first come, first served: later sessions wait their turn
+            self.batch.synchronize()
+            self.open_s = time.perf_counter() - t_open
         nxt = 0
         t0 = time.perf_counter()
         tuned = self.autotune_steps <= 0
@@ -182,13 +224,14 @@ class Server:
                 if not realtime:
                     r.arrival = now
                 s = self.sessions[r.session]
-                if s.vol is None and not s.queue and s not in waiting:
+                if s.vol is None and not s.closed and not s.queue and s not in waiting:
                     waiting.append(s)
                 s.queue.append(r)
                 nxt += 1
             # Admission, first come first served.
             while waiting and self._try_admit(waiting[0], now):
                 waiting.popleft()
+                self.t_admitted = now
             # Completed steps.
             while inflight and inflight[0][0].query():
                 _, rs = inflight.popleft()
@@ -212,29 +255,39 @@ class Server:
                     self._close(s)
             # Next step: the oldest integrate request of every admitted session.
             if len(inflight) < self.max_inflight:
-                members = []
-                with torch.cuda.stream(self.stream):
+                members, used = [], []
+                with torch.cuda.stream(self.copy_stream):
                     for s in self.sessions:
                         if s.vol is None or s.closed or not s.queue or s.queue[0].kind != "integrate":
                             continue
-                        # The copy is stream-ordered after every queued step,
-                        # so it never overwrites a frame still being read.
                         r = s.queue.popleft()
                         host, cam = s.frames[r.frame % len(s.frames)]
                         n = host.shape[0]
-                        s.stage[:n].copy_(host, non_blocking=True)
-                        self.batch.set_frame(s.slot, s.stage[:n], cam)
+                        buf = s.flip
+                        s.flip ^= 1
+                        if s.stage_ev[buf] is not None:  # the step that last read it
+                            self.copy_stream.wait_event(s.stage_ev[buf])
+                        s.stage[buf][:n].copy_(host, non_blocking=True)
+                        self.batch.set_frame(s.slot, s.stage[buf][:n], cam)
                         s.inflight += 1
                         members.append(r)
+                        used.append((s, buf))
                 if members:
+                    copied = torch.cuda.Event()
+                    copied.record(self.copy_stream)
+                    self.stream.wait_event(copied)
                     if not tuned:
                         self.batch.autotune(self.autotune_steps)
                         tuned = True
                     self.batch.step()
                     ev = torch.cuda.Event()
                     ev.record(self.stream)
+                    for s, buf in used:
+                        s.stage_ev[buf] = ev
                     inflight.append((ev, members))
                     self.steps += 1
+                    if self.steps == 16 * max(self.autotune_steps, 0):
+                        self.t_tuned = time.perf_counter() - t0
                     continue
             if inflight:
                 inflight[0][0].synchronize() if not realtime else time.sleep(0)
@@ -244,6 +297,7 @@ class Server:
                     time.sleep(min(wait, 0.0005))
         self.batch.synchronize()
         t_end = time.perf_counter() - t0
+        self._bury()
         return self._stats(reqs, t_end)
 
     def _stats(self, reqs, t_end) -> dict:
@@ -255,6 +309,10 @@ class Server:
 
         lat_i = [r.done - r.arrival for r in integ]
         lat_e = [r.done - r.arrival for r in ext]
+        # Steady state: arrivals after start-up (autotuning steps, and the
+        # admissions of sessions that arrived together at the start).
+        start = max(self.t_tuned, min(self.t_admitted, 1.0))
+        lat_s = [r.done - r.arrival for r in integ if r.arrival >= start]
         first = min((r.arrival for r in reqs), default=0.0)
         last = max((r.done for r in reqs), default=0.0)
         return {
@@ -262,8 +320,10 @@ class Server:
             "frames_per_s": len(integ) / max(last - first, 1e-9),
             "frames_per_step": len(integ) / max(self.steps, 1),
             "integrate_latency_ms": {"p50": pct(lat_i, 50), "p99": pct(lat_i, 99), "max": pct(lat_i, 100)},
+            "integrate_latency_ms_steady": {"p50": pct(lat_s, 50), "p99": pct(lat_s, 99),
+                                            "from_s": start, "requests": len(lat_s)},
             "extract_latency_ms": {"p50": pct(lat_e, 50), "p99": pct(lat_e, 99)},
-            "wall_s": t_end, "peak_sessions": self.peak_sessions,
+            "wall_s": t_end, "open_s": self.open_s, "peak_sessions": self.peak_sessions,
             "peak_ledger_gb": self.peak_ledger / 1e9, "budget_gb": self.budget / 1e9,
             "shape": self.batch.shape(),
         }
@@ -279,7 +339,9 @@ class Server:
                 self._close(s)
             s.frames = []
             s.stage = s.mesh = None
+            s.stage_ev = [None, None]
         self.sessions = []
+        self._bury()
         self.torch.cuda.synchronize()
         self.batch.close()
         self.batch = None
