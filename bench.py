@@ -53,17 +53,22 @@ def _frame_points(args):
     from what_irregularity_costs_b200 import scenes
     scene = scenes.RoomScene.make(seed)
     f = scenes.room_frame(scene, k)
-    return scenes.frame_points(f), f.cam
+    return scenes.frame_points(f), f.cam, (f.depth, f.R, f.t)
+
+
+_DEPTH = []  # depth frames and poses of the last make_trajectory call
 
 
 def make_trajectory(n_frames=N_FRAMES, seed=SEED, workers=None):
-    """Points of every frame (generated in spawned workers, before any CUDA use)."""
+    """Points of every frame (generated in spawned workers, before any CUDA use);
+    the depth images and poses they came from are kept in _DEPTH."""
     workers = workers or min(16, os.cpu_count() or 1)
     ctx = mp.get_context("spawn")
     with ProcessPoolExecutor(max_workers=workers, mp_context=ctx) as ex:
         out = list(ex.map(_frame_points, [(seed, k) for k in range(n_frames)]))
-    pts = [p for p, _ in out]
-    cams = [c for _, c in out]
+    pts = [p for p, _, _ in out]
+    cams = [c for _, c, _ in out]
+    _DEPTH[:] = [d for _, _, d in out]
     return pts, cams
 
 
@@ -376,6 +381,40 @@ def run_ours(args):
     e2e_ms = max_over_ranks(e0.elapsed_time(e1), dist, torch)
     e2e_value = frames_total / (e2e_ms / 1e3)
 
+    # -- e2e from depth images: 4 B per pixel uploaded, unprojected on the GPU
+    from what_irregularity_costs_b200 import scenes as _scenes
+    K = _scenes.ROOM_K
+    depth_host = [torch.from_numpy(d).pin_memory() for d, _, _ in _DEPTH]
+    dstage = [torch.empty(depth_host[0].shape, dtype=torch.float32, device="cuda") for _ in range(2)]
+    dbytes = int(sum(d.nbytes for d, _, _ in _DEPTH))
+
+    def step_e2e_depth():
+        vol.reset()
+        for k in range(N_FRAMES):
+            s_ = k & 1
+            with torch.cuda.stream(cstream):
+                cstream.wait_event(free[s_])
+                dstage[s_].copy_(depth_host[k], non_blocking=True)
+                copied[s_].record(cstream)
+            vstream.wait_event(copied[s_])
+            _, R_, t_ = _DEPTH[k]
+            vol.integrate_depth(dstage[s_], K, R_, t_)
+            free[s_].record(vstream)
+        result[0] = vol.block_count()
+        result[1] = vol.drop_count()
+
+    for _ in range(args.warmup):
+        step_e2e_depth()
+    barrier(dist, torch)
+    d0, d1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    d0.record(vstream)
+    for _ in range(args.steps):
+        step_e2e_depth()
+    d1.record(vstream)
+    barrier(dist, torch)
+    e2e_depth_ms = max_over_ranks(d0.elapsed_time(d1), dist, torch)
+    blocks_depth = vol.block_count()
+
     # -- one instrumented step: per-kernel CUDA-event times (every launch of
     # the volume bracketed on its stream; no synchronisation between frames)
     vol.set_timing(True)
@@ -468,6 +507,10 @@ def run_ours(args):
             "reference_gpu_arm": a3,
             "e2e": {"value": e2e_value, "unit": "frames/s",
                     "h2d_bytes_per_step": int(all_pts.nbytes), "d2h_bytes_per_step": 16},
+            "e2e_depth": {"value": frames_total / (e2e_depth_ms / 1e3), "unit": "frames/s",
+                          "h2d_bytes_per_step": dbytes, "d2h_bytes_per_step": 16,
+                          "path": "osn_tsdf_cuda_integrate_depth (unprojection in the band walk)",
+                          "blocks": blocks_depth},
             "gpu_launches": int(launches_per_step * args.steps),
             "clocks": clocks.summary(),
             "alloc_mrays_per_s": n_points / t_alloc / 1e6 if t_alloc else None,

@@ -144,6 +144,21 @@ OsnTsdfCudaVolume* osn_tsdf_cuda_create_ex(float voxel_size_m, int32_t pool_capa
 int32_t osn_tsdf_cuda_integrate(OsnTsdfCudaVolume* v, const float* d_positions, int32_t n_points,
                                 float cam_x, float cam_y, float cam_z, float radius_m);
 
+/* integrate from a depth image, unprojected inside the band walk: pixel
+ * (u, v) with depth z (metres along the optical axis, d_depth is a DEVICE
+ * float array of height * width in raster order) becomes the world point
+ * R [(u - cx) z / fx, (v - cy) z / fy, z] + t in FP64, rounded to float, as
+ * crates/tartanair/src/lib.rs:307-340 does on the host; pixels whose depth is
+ * non-finite, <= 0 or beyond max_range_m (when > 0) have no point. R (row-
+ * major 3x3) and t are the camera-to-world pose (HOST arrays); the camera
+ * origin of the walk is (float)t. Results equal integrate() of the host-
+ * backprojected valid points in raster order. 4 bytes per pixel cross the
+ * bus instead of 12 per point. Return codes as integrate. */
+int32_t osn_tsdf_cuda_integrate_depth(OsnTsdfCudaVolume* v, const float* d_depth, int32_t width,
+                                      int32_t height, double fx, double fy, double cx, double cy,
+                                      const double* cam_to_world_R, const double* cam_to_world_t,
+                                      float max_range_m);
+
 /* Extraction into DEVICE buffers (same layout as extract_mesh), skipping the
  * host copy. Returns the vertex count or -1 (overflow / bad arguments).
  * Waits for the count only. */

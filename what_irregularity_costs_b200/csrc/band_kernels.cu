@@ -165,7 +165,7 @@ constexpr int kProbeLane = 1;  // every lane probes its own runs (L1 shares the 
 
 template <int MODE, bool RECORDS, int S, int PROBE = kProbeWarp>
 __device__ __forceinline__ void band_point(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
-                                           int i, float px, float py, float pz, BandSmem& sm,
+                                           int i, bool has, float px, float py, float pz, BandSmem& sm,
                                            uint32_t& drops, uint32_t& counted,
                                            unsigned long long* hist, int n_bins) {
     const int t = threadIdx.x;
@@ -176,7 +176,7 @@ __device__ __forceinline__ void band_point(const DevVolume& v, const BatchArgs& 
     auto& run_bi = sm.run_bi;
     auto& run_src = sm.run_src;
     Ray r;
-    const bool live = i < a.n && ray_setup_at(a, px, py, pz, r);
+    const bool live = i < a.n && has && ray_setup_at(a, px, py, pz, r);
     uint32_t* rec = RECORDS ? u.records + i : nullptr;  // slot (s = -steps, i)
 
     for (int c0 = -v.steps; c0 <= v.steps; c0 += kChunk) {
@@ -302,9 +302,10 @@ __device__ __forceinline__ void band_point(const DevVolume& v, const BatchArgs& 
     }
 }
 
-template <int MODE, bool RECORDS, int S>
+template <int MODE, bool RECORDS, int S, bool DEPTH = false>
 __global__ void __launch_bounds__(kBandThreads, kBandMinBlocks)
 band_kernel(DevVolume v, BatchArgs a, UpdateScratch u, unsigned long long* hist, int n_bins) {
+    constexpr int kSource = DEPTH ? 1 : 0;
     __shared__ BandSmem sm;
     const int t = threadIdx.x;
     const int lane = t & 31;
@@ -321,24 +322,19 @@ band_kernel(DevVolume v, BatchArgs a, UpdateScratch u, unsigned long long* hist,
 
     // The point of the next tile is loaded one tile ahead.
     float nx = 0.0f, ny = 0.0f, nz = 0.0f;
+    bool nhas = false;
     {
         const int i0 = blockIdx.x * kBandThreads + t;
-        if (blockIdx.x < n_tiles && i0 < a.n) {
-            nx = a.pos[(size_t)i0 * 3 + 0];
-            ny = a.pos[(size_t)i0 * 3 + 1];
-            nz = a.pos[(size_t)i0 * 3 + 2];
-        }
+        if (blockIdx.x < n_tiles && i0 < a.n) nhas = load_point<kSource>(a, i0, nx, ny, nz);
     }
     for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
         const int i = tile * kBandThreads + t;
         const float px = nx, py = ny, pz = nz;
+        const bool has = nhas;
         const int inext = i + gridDim.x * kBandThreads;
-        if (inext < a.n) {
-            nx = a.pos[(size_t)inext * 3 + 0];
-            ny = a.pos[(size_t)inext * 3 + 1];
-            nz = a.pos[(size_t)inext * 3 + 2];
-        }
-        band_point<MODE, RECORDS, S>(v, a, u, i, px, py, pz, sm, drops, counted, hist, n_bins);
+        nhas = false;
+        if (inext < a.n) nhas = load_point<kSource>(a, inext, nx, ny, nz);
+        band_point<MODE, RECORDS, S>(v, a, u, i, has, px, py, pz, sm, drops, counted, hist, n_bins);
     }
 
     // Counters: one global atomic per CTA (per-warp atomics on one line serialise).
@@ -439,19 +435,15 @@ band_multi_kernel(StepWork w) {
         for (int tile = first; tile < last; ++tile) {
             const int i = tile * kBandThreads + t;
             float px = 0.0f, py = 0.0f, pz = 0.0f;
-            if (i < sw.a.n) {
-                px = sw.a.pos[(size_t)i * 3 + 0];
-                py = sw.a.pos[(size_t)i * 3 + 1];
-                pz = sw.a.pos[(size_t)i * 3 + 2];
-            }
-            band_point<kAllocInsert, true, S, PROBE>(sw.v, sw.a, sw.u, i, px, py, pz, sm, drops, counted,
-                                                    nullptr, 0);
+            const bool has = i < sw.a.n && load_point(sw.a, i, px, py, pz);
+            band_point<kAllocInsert, true, S, PROBE>(sw.v, sw.a, sw.u, i, has, px, py, pz, sm, drops,
+                                                    counted, nullptr, 0);
         }
         __syncthreads();  // s_item and the descriptor are rewritten next
     }
 }
 
-template <int MODE, bool RECORDS, int S = kStoreF32>
+template <int MODE, bool RECORDS, int S = kStoreF32, bool DEPTH = false>
 cudaError_t launch(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
                    unsigned long long* hist, int n_bins, int sm_count, cudaStream_t s) {
     if (a.n <= 0) return cudaSuccess;
@@ -460,14 +452,14 @@ cudaError_t launch(const DevVolume& v, const BatchArgs& a, const UpdateScratch& 
     static int per_sm = 0;
     static std::once_flag once;
     std::call_once(once, [] {
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, band_kernel<MODE, RECORDS, S>,
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, band_kernel<MODE, RECORDS, S, DEPTH>,
                                                           kBandThreads, 0) != cudaSuccess ||
             per_sm < 1)
             per_sm = 1;
     });
     const int tiles = (a.n + kBandThreads - 1) / kBandThreads;
     const int grid = std::min(tiles, per_sm * sm_count);
-    band_kernel<MODE, RECORDS, S><<<grid, kBandThreads, 0, s>>>(v, a, u, hist, n_bins);
+    band_kernel<MODE, RECORDS, S, DEPTH><<<grid, kBandThreads, 0, s>>>(v, a, u, hist, n_bins);
     return cudaGetLastError();
 }
 
@@ -490,6 +482,17 @@ cudaError_t launch_allocate(const DevVolume& v, const BatchArgs& a, int mode,
 
 cudaError_t launch_band_records(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
                                 bool insert, int sm_count, cudaStream_t s) {
+    if (a.depth.depth != nullptr) {  // integrate from a depth image (allocates)
+        if (!insert) return cudaErrorInvalidValue;
+        switch (v.storage) {
+            case kStoreF16U16:
+                return launch<kAllocInsert, true, kStoreF16U16, true>(v, a, u, nullptr, 0, sm_count, s);
+            case kStoreF64:
+                return launch<kAllocInsert, true, kStoreF64, true>(v, a, u, nullptr, 0, sm_count, s);
+            default:
+                return launch<kAllocInsert, true, kStoreF32, true>(v, a, u, nullptr, 0, sm_count, s);
+        }
+    }
     switch (v.storage) {
         case kStoreF16U16:
             return insert ? launch<kAllocInsert, true, kStoreF16U16>(v, a, u, nullptr, 0, sm_count, s)

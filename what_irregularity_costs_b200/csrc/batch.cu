@@ -398,7 +398,7 @@ int32_t osn_tsdf_batch_set_frame(OsnTsdfBatch* b, int32_t scene, const float* d_
                                  float radius_m) {
     osn_b200::Batch* x = batch_of(b);
     if (!x) return 1;
-    osn_b200::BatchArgs a;
+    osn_b200::BatchArgs a{};
     a.pos = d_positions;
     a.n = n_points;
     a.cam_x = cam_x;

@@ -1,6 +1,7 @@
 // The C ABI: the reference's CUDA section of cpp/include/osn_tsdf/c_api.h
 // (implemented there by cpp/src/c_api_cuda.cu) plus this library's
 // extensions, declared in include/osn_tsdf_b200.h.
+#include <climits>
 #include <cstring>
 
 #include "../../include/osn_tsdf_b200.h"
@@ -21,7 +22,7 @@ struct OsnTsdfCudaVolume {
 namespace {
 
 BatchArgs batch(const float* pos, int32_t n, float cx, float cy, float cz, float radius) {
-    BatchArgs a;
+    BatchArgs a{};
     a.pos = pos;
     a.n = n;
     a.cam_x = cx;
@@ -133,6 +134,31 @@ int32_t osn_tsdf_cuda_integrate(OsnTsdfCudaVolume* v, const float* d_positions, 
                    cudaSuccess
                ? 0
                : 3;
+}
+
+int32_t osn_tsdf_cuda_integrate_depth(OsnTsdfCudaVolume* v, const float* d_depth, int32_t width,
+                                      int32_t height, double fx, double fy, double cx, double cy,
+                                      const double* cam_to_world_R, const double* cam_to_world_t,
+                                      float max_range_m) {
+    if (!usable(v) || !d_depth || width <= 0 || height <= 0 || !cam_to_world_R || !cam_to_world_t ||
+        !(fx != 0.0) || !(fy != 0.0))
+        return 1;
+    const int64_t n = (int64_t)width * height;
+    if (n > INT32_MAX || !batch_fits(v, (int32_t)n)) return 1;
+    // The camera origin of the walk is the pose translation as float, as a
+    // caller passing backprojected points would pass it.
+    BatchArgs a = batch(nullptr, (int32_t)n, (float)cam_to_world_t[0], (float)cam_to_world_t[1],
+                        (float)cam_to_world_t[2], 0.0f);
+    a.depth.depth = d_depth;
+    a.depth.width = width;
+    a.depth.max_range = max_range_m;
+    a.depth.fx = fx;
+    a.depth.fy = fy;
+    a.depth.cx = cx;
+    a.depth.cy = cy;
+    for (int k = 0; k < 9; ++k) a.depth.R[k] = cam_to_world_R[k];
+    for (int k = 0; k < 3; ++k) a.depth.t[k] = cam_to_world_t[k];
+    return v->vol.integrate(a) == cudaSuccess ? 0 : 3;
 }
 
 int32_t osn_tsdf_cuda_extract_mesh(OsnTsdfCudaVolume* v, float* buffer_posnor, uint8_t* buffer_rgb,

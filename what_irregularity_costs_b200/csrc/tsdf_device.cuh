@@ -120,13 +120,61 @@ __device__ __forceinline__ float mean_at(const DevVolume& v, size_t i, float w) 
         return __fmul_rn(v.tsdf[i], __fdiv_rn(1.0f, w));  // marching_tets.cpp: sum * (1/w)
 }
 
-// One batch: camera origin and squared far cutoff (0 disables).
+// A depth image as the point source of a batch: pixel i = v * width + u
+// with depth z (metres along the optical axis) becomes the world point
+// R [ (u - cx) z / fx, (v - cy) z / fy, z ] + t, evaluated in FP64 and
+// rounded to float (crates/tartanair/src/lib.rs:307-340); pixels with a
+// non-finite, non-positive or out-of-range depth have no point.
+struct DepthSource {
+    const float* depth;  // [height * width], device
+    int32_t width;
+    float max_range;     // <= 0: no limit
+    double fx, fy, cx, cy;
+    double R[9];         // camera-to-world rotation, row-major
+    double t[3];         // camera origin in world
+};
+
+// One batch: camera origin and squared far cutoff (0 disables). Points come
+// from pos (3 floats each) or, when depth.depth is set, from a depth image
+// (n = width * height pixels, in raster order).
 struct BatchArgs {
     const float* pos;
     int32_t n;
     float cam_x, cam_y, cam_z;
     float radius_sq;
+    DepthSource depth;
 };
+
+// Point i of a batch; false when it has none (an invalid depth pixel).
+// SOURCE: 0 = xyz positions, 1 = depth image, -1 = whichever the batch has.
+template <int SOURCE = -1>
+__device__ __forceinline__ bool load_point(const BatchArgs& a, int i, float& px, float& py, float& pz) {
+    if (SOURCE == 0 || (SOURCE < 0 && a.depth.depth == nullptr)) {
+        px = a.pos[(size_t)i * 3 + 0];
+        py = a.pos[(size_t)i * 3 + 1];
+        pz = a.pos[(size_t)i * 3 + 2];
+        return true;
+    }
+    const DepthSource& d = a.depth;
+    const float z = d.depth[i];
+    px = py = pz = 0.0f;
+    if (!isfinite(z) || !(z > 0.0f) || (d.max_range > 0.0f && z > d.max_range)) return false;
+    const int v = i / d.width, u = i - v * d.width;
+    const double zd = (double)z;
+    const double x = __ddiv_rn(__dmul_rn(__dsub_rn((double)u, d.cx), zd), d.fx);
+    const double y = __ddiv_rn(__dmul_rn(__dsub_rn((double)v, d.cy), zd), d.fy);
+    float w[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+        w[k] = __double2float_rn(__dadd_rn(
+            __dadd_rn(__dadd_rn(__dmul_rn(d.R[3 * k], x), __dmul_rn(d.R[3 * k + 1], y)),
+                      __dmul_rn(d.R[3 * k + 2], zd)),
+            d.t[k]));
+    px = w[0];
+    py = w[1];
+    pz = w[2];
+    return true;
+}
 
 __device__ __forceinline__ long long pack_key(int32_t x, int32_t y, int32_t z) {
     return (((long long)x + kCoordBias) << (2 * kCoordBits)) |
@@ -188,8 +236,9 @@ __device__ __forceinline__ bool ray_setup_at(const BatchArgs& a, float px, float
 }
 
 __device__ __forceinline__ bool ray_setup(const BatchArgs& a, int i, Ray& r) {
-    return ray_setup_at(a, a.pos[(size_t)i * 3 + 0], a.pos[(size_t)i * 3 + 1], a.pos[(size_t)i * 3 + 2],
-                        r);
+    float px, py, pz;
+    if (!load_point(a, i, px, py, pz)) return false;
+    return ray_setup_at(a, px, py, pz, r);
 }
 
 // Band sample s in [-steps, steps]: voxel index and signed distance at the

@@ -114,7 +114,7 @@ extern "C" int32_t osn_tsdf_cuda_update_voxels_noalloc(OsnTsdfCudaVolume* v,
     if (cudaGetDevice(&device) != cudaSuccess) return 3;
     void* scratch = osn_b200::scratch_address(device);
     if (!scratch) return 3;
-    osn_b200::BatchArgs a;
+    osn_b200::BatchArgs a{};
     a.pos = d_positions;
     a.n = n_points;
     a.cam_x = cam_x;

@@ -141,6 +141,24 @@ class CudaVolume:
     def integrate(self, positions, cam: Sequence[float], radius_m: float = 0.0, n=None):
         self._batch(self.lib.osn_tsdf_cuda_integrate, positions, cam, radius_m, n, "integrate")
 
+    def integrate_depth(self, depth, K, R, t, max_range_m: float = 0.0):
+        """integrate() from a device depth image (H, W) float32, unprojected on
+        the GPU with intrinsics K (fx, fy, cx, cy attributes) and the
+        camera-to-world pose R (3x3), t (3,) in FP64; equals integrating the
+        host-backprojected points (scenes.backproject)."""
+        if not (hasattr(depth, "is_cuda") and depth.is_cuda and depth.dim() == 2 and depth.is_contiguous()):
+            raise ValueError("depth must be a contiguous (H, W) CUDA tensor")
+        import torch
+        if depth.dtype != torch.float32:
+            raise ValueError("depth must be float32")
+        Rh = np.ascontiguousarray(np.asarray(R, dtype=np.float64).reshape(9))
+        th = np.ascontiguousarray(np.asarray(t, dtype=np.float64).reshape(3))
+        self._keep.append(depth)
+        rc = self.lib.osn_tsdf_cuda_integrate_depth(
+            self.h, _addr(depth), int(depth.shape[1]), int(depth.shape[0]), float(K.fx), float(K.fy),
+            float(K.cx), float(K.cy), Rh.ctypes.data, th.ctypes.data, float(max_range_m))
+        self._check(rc, "integrate_depth")
+
     def allocate_counting_cas(self, positions, cam, radius_m=0.0, n=None):
         self._batch(self.lib.osn_tsdf_cuda_allocate_counting_cas, positions, cam, radius_m, n,
                     "allocate_counting_cas")
