@@ -788,6 +788,116 @@ def run_serve64(args):
     return 0
 
 
+def run_sweep(args):
+    """Irregularity and precision sweep on the room trajectory (640x480 frames):
+    voxel sizes 5 mm, 1, 2, 4 cm (trunc 4 voxels, cap 64) on a 2^18-slot table
+    (the smallest of the 2^18-2^22 range, so the most load factors are
+    reachable), pool = slots. An FP64 volume integrates frames until the block
+    count reaches 0.9 of the table (or the frames run out); FP32 and FP16/u16
+    volumes then integrate exactly those frames, so all three hold the same
+    blocks. In the FP32/FP16 runs, the frame at which the load factor first
+    reaches 0.25 / 0.5 / 0.75 / 0.9 runs as: allocate (timed: Mrays/s), a
+    probe-histogram pass over the same points (now lookups: the probe depth of
+    finding each block at that load factor), update (timed: GB/s of 12 B per
+    point + tsdf and weight of every touched block read and written). Load
+    factors the trajectory cannot reach at a voxel size are reported as the
+    largest reached. Errors of FP32 and FP16 against FP64: max / RMS mean-TSDF
+    error (m) and the Chamfer distance of the extracted meshes."""
+    n_frames = min(args.frames, N_FRAMES)
+    pts, cams = make_trajectory(n_frames)  # before any CUDA use
+    import torch
+    from what_irregularity_costs_b200 import (STORAGE_FP16_U16, STORAGE_FP32, STORAGE_FP64, CudaVolume,
+                                              precision)
+    rank, local, world, dist = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    dev = [torch.from_numpy(p).cuda() for p in pts]
+    slots = 1 << 18
+    targets = [0.25, 0.5, 0.75, 0.9]
+    mesh_cap = 1 << 25
+    cells = []
+    for voxel in (0.005, 0.01, 0.02, 0.04):
+        trunc = 4 * voxel
+        o = CudaVolume(voxel, slots, trunc, CAP, slots, storage=STORAGE_FP64)
+        n_stop = 0
+        for k in range(n_frames):
+            if o.block_count() >= 0.9 * slots:
+                break
+            o.integrate(dev[k], cams[k])
+            n_stop = k + 1
+        mo = o.extract_mesh(mesh_cap)
+        row = {"voxel_m": voxel, "slots": slots, "frames": n_stop, "blocks": o.block_count(),
+               "lf_reached": o.block_count() / slots, "fp64_drops": int(o.drop_count())}
+        for storage, name in ((STORAGE_FP32, "fp32"), (STORAGE_FP16_U16, "fp16_u16")):
+            vol = CudaVolume(voxel, slots, trunc, CAP, slots, storage=storage)
+            vs = torch.cuda.ExternalStream(vol.stream_handle())
+            # Pass 1 (timed): every frame, one event pair, no polling in between.
+            for _ in range(2):  # the first pass warms up (allocations, caches)
+                vol.reset()
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(vs)
+                for k in range(n_stop):
+                    vol.integrate(dev[k], cams[k])
+                e1.record(vs)
+                torch.cuda.synchronize()
+            fps = n_stop / (e0.elapsed_time(e1) / 1e3) if n_stop else None
+            # Pass 2: the same frames with the load-factor checkpoints.
+            vol.reset()
+            marks, ti, t_frames = [], 0, []
+            for k in range(n_stop):
+                lf = vol.block_count() / slots
+                if ti < len(targets) and lf >= targets[ti]:
+                    e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+                    e[0].record(vs)
+                    vol.allocate_blocks(dev[k], cams[k])
+                    e[1].record(vs)
+                    hist = vol.allocate_probe_histogram(dev[k], cams[k], n_bins=32)
+                    e[2].record(vs)
+                    vol.update_voxels(dev[k], cams[k])
+                    e[3].record(vs)
+                    torch.cuda.synchronize()
+                    st = vol.last_update_stats()
+                    t_alloc, t_upd = e[0].elapsed_time(e[1]), e[2].elapsed_time(e[3])
+                    tb = 4 if storage == STORAGE_FP32 else 2
+                    ub = 12 * pts[k].shape[0] + st["touched_blocks"] * 512 * 2 * 2 * tb
+                    nz = np.nonzero(hist)[0]
+                    marks.append({"target_lf": targets[ti], "lf": lf, "frame": k,
+                                  "alloc_mrays_per_s": pts[k].shape[0] / t_alloc / 1e3,
+                                  "update_gbps": ub / t_upd / 1e6, "update_ms": t_upd,
+                                  "touched_blocks": st["touched_blocks"],
+                                  "probe_hist": hist[: int(nz.max()) + 1].tolist() if nz.size else [],
+                                  "mean_probes": float((hist * np.arange(hist.size)).sum() / max(hist.sum(), 1))})
+                    while ti < len(targets) and lf >= targets[ti]:
+                        ti += 1
+                else:
+                    vol.integrate(dev[k], cams[k])
+            torch.cuda.synchronize()
+            try:
+                err = precision.tsdf_errors(vol, o, trunc)
+            except AssertionError as ex:  # block sets or weights differ: reported, not hidden
+                err = {"mismatch": str(ex)}
+            mesh = vol.extract_mesh(mesh_cap)
+            row[name] = {"frames_per_s": fps, "marks": marks,
+                         "drops": int(vol.drop_count()), "status": vol.status(),
+                         "tsdf_error_vs_fp64": err, "mesh_vs_fp64": precision.mesh_errors(mesh, mo, stride=4)}
+            vol.close()
+        o.close()
+        cells.append(row)
+    if rank == 0:
+        print(json.dumps({
+            "metric": "irregularity and precision sweep (room trajectory 640x480)",
+            "value": None, "unit": None, "n_gpus": world, "steps": n_frames, "warmup": 0,
+            "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 and f16/u16 storage vs f64 oracle", "data": "synthetic room trajectory seed 0",
+            "config": {"workload": "voxels 5 mm-4 cm x load factor 0.25-0.9 on 2^18 slots x storage",
+                       "frames": n_frames, "slots": slots},
+            "cells": cells}))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -802,15 +912,18 @@ def main():
     ap.add_argument("--frames", type=int, default=N_FRAMES,
                     help="frames of the trajectory per step (fewer: a small profiling case)")
     ap.add_argument("--pool", type=int, default=POOL, help="pool capacity in blocks")
-    ap.add_argument("--workload", choices=["room", "batch32", "serve64"], default="room",
+    ap.add_argument("--workload", choices=["room", "batch32", "serve64", "sweep"], default="room",
                     help="room: the single-scene trajectory (default); batch32: the 32-scene "
-                         "batched mix; serve64: the 64-session serving loop")
+                         "batched mix; serve64: the 64-session serving loop; sweep: voxel size x "
+                         "load factor x storage precision")
     args = ap.parse_args()
     set_workload(args.frames, args.pool)
     if args.workload == "batch32" and args.impl == "ours":
         return run_batch32(args)
     if args.workload == "serve64" and args.impl == "ours":
         return run_serve64(args)
+    if args.workload == "sweep" and args.impl == "ours":
+        return run_sweep(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

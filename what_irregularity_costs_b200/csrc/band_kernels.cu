@@ -46,8 +46,14 @@ namespace {
 
 constexpr int kBandThreads = kBatchTilePoints;
 static_assert(kBandThreads >= kMaxBatchScenes, "one thread per scene builds the item prefix");
-constexpr int kChunk = 9;  // samples per ray held in registers (the whole band at 4 voxels)
-constexpr int kBandMinBlocks = 8;  // resident CTAs per SM the register budget is sized for
+#ifndef OSN_BAND_CHUNK
+#define OSN_BAND_CHUNK 9
+#endif
+constexpr int kChunk = OSN_BAND_CHUNK;  // samples per ray held in registers (9: the whole band at 4 voxels)
+#ifndef OSN_BAND_MIN_BLOCKS
+#define OSN_BAND_MIN_BLOCKS 8
+#endif
+constexpr int kBandMinBlocks = OSN_BAND_MIN_BLOCKS;  // resident CTAs per SM the register budget is sized for
 
 // Per-sample state: voxel within block (9 bits), run index (4 bits), valid.
 constexpr uint32_t kLvMask = 0x1FFu;
