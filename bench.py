@@ -141,31 +141,45 @@ class ClockSampler:
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
 
 
-def dist_setup(n_gpus):
+def dist_setup(n_gpus, backend="nccl"):
+    """Rank, local rank, world size and the process group module (None alone).
+    One process per GPU; the data path has no collective (replicas): the
+    group only carries the timing barrier and the max over ranks. The short
+    timeout ends a collective with an error when a rank is gone."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=None)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
         return rank, local, world, dist
     return 0, 0, 1, None
 
 
+def _device(dist):
+    return "cuda" if dist is None or dist.get_backend() == "nccl" else "cpu"
+
+
 def barrier(dist, torch):
-    torch.cuda.synchronize()
+    if torch.cuda.is_available():
+        torch.cuda.synchronize()
     if dist is not None:
         dist.barrier()
 
 
 def max_over_ranks(x, dist, torch):
+    """The job's time is the slowest rank's."""
     if dist is None:
         return x
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=_device(dist))
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_work(frames_per_rank, world):
+    """Frames the whole job integrates: every rank runs its own replica."""
+    return frames_per_rank * world
 
 
 # ---------------------------------------------------------------------------
@@ -341,7 +355,7 @@ def run_ours(args):
     blocks = vol.block_count()
     drops = vol.drop_count()
     status = vol.status()
-    frames_total = N_FRAMES * args.steps * world
+    frames_total = replica_work(N_FRAMES * args.steps, world)
     value = frames_total / (ms / 1e3)
 
     # -- e2e: pinned host buffers, copies inside the timed region ------------
