@@ -165,6 +165,22 @@ int32_t osn_tsdf_cuda_integrate_depth(OsnTsdfCudaVolume* v, const float* d_depth
 int32_t osn_tsdf_cuda_extract_mesh_device(OsnTsdfCudaVolume* v, float* d_posnor, uint8_t* d_rgb,
                                           int32_t vert_cap, float min_weight, float iso);
 
+/* Snapshot and restore through host memory (checkpoint a volume, or move an
+ * idle session out of HBM and back). A snapshot holds the allocated blocks'
+ * coordinates and voxel arrays (pool order) and the drop counter; the table
+ * is rebuilt on restore, so slot positions may differ while every lookup,
+ * update and extraction continues as on the original.
+ * snapshot_bytes: bytes a snapshot needs now (waits), -1 on a bad volume.
+ * snapshot: writes into host_buffer (capacity bytes); returns the bytes
+ * written or -1 (too small, bad volume, CUDA error).
+ * restore: replaces the volume's contents with a snapshot taken from a
+ * volume with the same voxel size, truncation, weight cap and storage mode;
+ * its pool and table must hold the snapshot's blocks. 0 ok, 1 bad snapshot or
+ * arguments, 3 CUDA error. All three wait for the volume's stream. */
+int64_t osn_tsdf_cuda_snapshot_bytes(OsnTsdfCudaVolume* v);
+int64_t osn_tsdf_cuda_snapshot(OsnTsdfCudaVolume* v, void* host_buffer, int64_t capacity);
+int32_t osn_tsdf_cuda_restore(OsnTsdfCudaVolume* v, const void* host_buffer, int64_t size);
+
 /* Device error word, after waiting for the stream: 0 when every bounded
  * wait in the kernels finished in time; bit 0 = a publication wait gave up,
  * bit 1 = an update batch exceeded its scratch. */

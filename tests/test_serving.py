@@ -118,3 +118,40 @@ def test_admission_by_memory_budget(cuda):
         _check(cuda, specs, frames, reqs, server)
     finally:
         server.close()
+
+
+def test_eviction_to_host_and_back(cuda):
+    """Four sessions taking turns under a budget that holds two: idle
+    sessions are snapshotted to host and restored on their next request,
+    and every result still equals the lone volume."""
+    specs = _specs()[:4]
+    frames = [_frames(sp, 2) for sp in specs]
+    reqs = []
+    t = 0.0
+    for turn in range(3):  # each session gets a burst of frames, then waits for the others
+        for sp in specs:
+            for j in range(2):
+                k = 2 * turn + j
+                if k < sp.frames:
+                    reqs.append(Request("integrate", sp.index, k, t))
+                    t += 0.004
+            t += 0.02
+    fps = sorted(footprint_bytes(sp, STORAGE_FP16_U16) for sp in specs)
+    budget = fps[-1] + fps[-2] + 1
+    server = Server(budget_bytes=budget, graph=False, evict=True)
+    server.keep_volumes = True
+    try:
+        stats = server.run(specs, frames, reqs, realtime=True)
+        assert stats["frames"] == len(reqs)
+        assert stats["evictions"] > 0 and stats["restores"] > 0
+        assert stats["peak_ledger_gb"] * 1e9 <= budget
+        for sp in specs:
+            used = [r for r in reqs if r.session == sp.index]
+            sp2 = SceneSpec(sp.index, sp.seed, sp.hash_slots, sp.voxel, sp.width, sp.height,
+                            len(used), cap=sp.cap)
+            alone, _ = _alone(cuda, sp2, frames[sp.index], set())
+            ca, ma, wa = precision._aligned(alone)
+            cs, ms, ws = precision._aligned(server.finished[sp.index])
+            assert np.array_equal(ca, cs) and np.array_equal(wa, ws) and np.array_equal(ma, ms)
+    finally:
+        server.close()

@@ -67,6 +67,9 @@ _SIG = {
     "osn_tsdf_cuda_status": (C.c_uint32, [_P]),
     "osn_tsdf_cuda_stream": (_P, [_P]),
     "osn_tsdf_cuda_storage": (_I, [_P]),
+    "osn_tsdf_cuda_snapshot_bytes": (C.c_int64, [_P]),
+    "osn_tsdf_cuda_snapshot": (C.c_int64, [_P, _P, C.c_int64]),
+    "osn_tsdf_cuda_restore": (_I, [_P, _P, C.c_int64]),
     "osn_tsdf_cuda_last_update_stats": (_I, [_P, _P]),
     "osn_tsdf_cuda_set_timing": (_I, [_P, _I]),
     "osn_tsdf_cuda_kernel_times": (_I, [_P, _P, _P, _I]),

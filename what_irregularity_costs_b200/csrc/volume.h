@@ -110,6 +110,14 @@ public:
     void synchronize() { cudaStreamSynchronize(stream_); }
     bool last_update_stats(int64_t out[4]);
 
+    // Snapshot of the allocated blocks through host memory (snapshot.cu):
+    // bytes needed, write (returns bytes or -1), restore into this volume
+    // (same voxel size, truncation, cap and storage; 0 ok, 1 bad snapshot,
+    // 3 CUDA error). All wait for the stream.
+    int64_t snapshot_bytes();
+    int64_t snapshot(void* host, int64_t cap);
+    int32_t restore(const void* host, int64_t size);
+
     // Batched steps: make room for batches of up to max_points points (call
     // before any stream capture), then describe one batch for a batched
     // step on stream s (takes the next update number).

@@ -19,6 +19,10 @@ One host thread drives one ``Batch`` (at most 64 attached sessions):
   overlaps the step still running) and queues one batched step after the
   copies; at most ``max_inflight`` steps are on the GPU while the host forms
   the next, so requests that arrive during a step join the next one.
+* Eviction. When a waiting session does not fit, admitted sessions with
+  nothing queued or in flight are moved to host snapshots (least recently
+  active first) and freed; an evicted session waits for admission again on
+  its next request and is restored from its snapshot, exactly as it was.
 * Extraction. A session whose oldest request is an extract, with none of
   its frames in flight, extracts its mesh into its device buffer on its own
   stream, concurrently with the batch steps of the other sessions.
@@ -94,12 +98,15 @@ class _Session:
     footprint: int = 0
     admitted_at: float = -1.0
     closed: bool = False
+    snapshot: object = None   # host copy while evicted
+    last_active: float = 0.0
+    evictions: int = 0
 
 
 class Server:
     def __init__(self, budget_bytes: float = 120e9, storage: int = _vol.STORAGE_FP16_U16,
                  graph: bool = True, max_inflight: int = 2, headroom_bytes: float = 2e9,
-                 shape=None, autotune_steps: int = 0):
+                 shape=None, autotune_steps: int = 0, evict: bool = True):
         import torch
         self.torch = torch
         self.budget = float(budget_bytes)
@@ -120,6 +127,9 @@ class Server:
         self.keep_volumes = False  # tests keep finished volumes for comparison
         self.finished: dict[int, CudaVolume] = {}
         self.graveyard: list = []  # closed sessions' memory, freed lazily
+        self.evict = evict          # snapshot idle sessions to host when others wait
+        self.evictions = 0
+        self.restores = 0
 
     # -- admission -----------------------------------------------------------
     def _try_admit(self, s: _Session, now: float) -> bool:
@@ -128,6 +138,8 @@ class Server:
         fp = footprint_bytes(s.spec, self.storage)
         if self.ledger + fp > self.budget and self.graveyard:
             self._bury(fp)  # release finished sessions only when the room is needed
+        if self.ledger + fp > self.budget and self.evict:
+            self._evict_for(fp, now)
         if self.ledger + fp > self.budget:
             return False
         free, _ = self.torch.cuda.mem_get_info()
@@ -135,7 +147,13 @@ class Server:
             return False
         sp = s.spec
         s.vol = CudaVolume(sp.voxel, sp.pool, sp.trunc, sp.cap, sp.hash_slots, storage=self.storage)
+        if s.snapshot is not None:  # back from eviction
+            s.vol.restore(s.snapshot)
+            s.snapshot = None
+            self.restores += 1
         s.slot = self.batch.add(s.vol, sp.max_points)
+        s.inflight = 0
+        s.stage_ev = [None, None]
         s.stage = [self.torch.empty((sp.max_points, 3), dtype=self.torch.float32, device="cuda")
                    for _ in range(2)]
         s.mesh = self.torch.empty((mesh_capacity(sp), 6), dtype=self.torch.float32, device="cuda")
@@ -146,6 +164,26 @@ class Server:
         live = sum(1 for x in self.sessions if x.vol is not None and not x.closed)
         self.peak_sessions = max(self.peak_sessions, live)
         return True
+
+    def _evict_for(self, need: int, now: float) -> bool:
+        """Move idle sessions (nothing queued or in flight) to host snapshots,
+        least recently active first, until `need` bytes fit the budget."""
+        idle = [x for x in self.sessions
+                if x.vol is not None and not x.closed and not x.queue and not x.inflight and x.remaining]
+        idle.sort(key=lambda x: x.last_active)
+        for x in idle:
+            if self.ledger + need <= self.budget:
+                break
+            self.batch.remove(x.slot)  # waits for the queued steps
+            x.snapshot = x.vol.snapshot()
+            x.vol.close()
+            x.vol = None
+            x.stage = x.mesh = None
+            x.stage_ev = [None, None]
+            self.ledger -= x.footprint
+            x.evictions += 1
+            self.evictions += 1
+        return self.ledger + need <= self.budget
 
     def _extract(self, s: _Session) -> int:
         """Mesh into the session's device buffer; a full buffer is doubled
@@ -241,6 +279,7 @@ class Server:
                     s = self.sessions[r.session]
                     s.inflight -= 1
                     s.remaining -= 1
+                    s.last_active = t
             # Extractions of sessions with nothing in flight.
             for s in self.sessions:
                 if s.vol is None or s.closed or s.inflight or not s.queue or s.queue[0].kind != "extract":
@@ -249,6 +288,7 @@ class Server:
                 r.vertices = self._extract(s)
                 r.done = time.perf_counter() - t0
                 s.remaining -= 1
+                s.last_active = r.done
             # Sessions with every request done leave; their memory admits others.
             for s in self.sessions:
                 if s.vol is not None and not s.closed and s.remaining == 0 and not s.queue:
@@ -324,6 +364,7 @@ class Server:
                                             "from_s": start, "requests": len(lat_s)},
             "extract_latency_ms": {"p50": pct(lat_e, 50), "p99": pct(lat_e, 99)},
             "wall_s": t_end, "open_s": self.open_s, "peak_sessions": self.peak_sessions,
+            "evictions": self.evictions, "restores": self.restores,
             "peak_ledger_gb": self.peak_ledger / 1e9, "budget_gb": self.budget / 1e9,
             "shape": self.batch.shape(),
         }

@@ -159,6 +159,24 @@ class CudaVolume:
             float(K.cx), float(K.cy), Rh.ctypes.data, th.ctypes.data, float(max_range_m))
         self._check(rc, "integrate_depth")
 
+    def snapshot(self) -> np.ndarray:
+        """The volume's allocated blocks and voxels as a host byte array."""
+        n = self.lib.osn_tsdf_cuda_snapshot_bytes(self.h)
+        if n < 0:
+            raise RuntimeError("snapshot_bytes failed")
+        buf = np.empty(int(n), dtype=np.uint8)
+        wrote = self.lib.osn_tsdf_cuda_snapshot(self.h, buf.ctypes.data, int(n))
+        if wrote != n:
+            raise RuntimeError("snapshot failed")
+        return buf
+
+    def restore(self, snap: np.ndarray):
+        """Replace the contents with a snapshot (same voxel size, truncation,
+        cap and storage; pool and table large enough)."""
+        snap = np.ascontiguousarray(snap, dtype=np.uint8)
+        rc = self.lib.osn_tsdf_cuda_restore(self.h, snap.ctypes.data, int(snap.nbytes))
+        self._check(rc, "restore")
+
     def allocate_counting_cas(self, positions, cam, radius_m=0.0, n=None):
         self._batch(self.lib.osn_tsdf_cuda_allocate_counting_cas, positions, cam, radius_m, n,
                     "allocate_counting_cas")
