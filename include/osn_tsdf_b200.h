@@ -186,8 +186,27 @@ int32_t osn_tsdf_cuda_restore(OsnTsdfCudaVolume* v, const void* host_buffer, int
  * bit 1 = an update batch exceeded its scratch. */
 uint32_t osn_tsdf_cuda_status(const OsnTsdfCudaVolume* v);
 
-/* The volume's cudaStream_t, for callers that order their own work after it. */
+/* The volume's cudaStream_t, for callers that order their own work after it.
+ * In pipelined mode (below) the last calls' update tails may still run on an
+ * internal stream: call osn_tsdf_cuda_join first to order work after them. */
 void* osn_tsdf_cuda_stream(const OsnTsdfCudaVolume* v);
+
+/* Pipelined updates. When enabled, an integrate/update call's band walk is
+ * queued on the volume's stream as usual but its update tail (finish, group,
+ * values, deferred) runs on an internal stream, so the next call's walk
+ * overlaps this call's tail; the per-call scratch alternates between two sets
+ * (twice the per-voxel batch state: +12 bytes per voxel). Results are
+ * identical. The positions (or depth image) of a call may be reused once the
+ * volume's stream has passed the call, as in serial mode; every waiting
+ * reader of results (counters, extraction, reset, snapshot, status,
+ * synchronize) first waits for the queued tails. Work a caller orders on the
+ * volume's stream sees the tails only after osn_tsdf_cuda_join. Returns 0,
+ * 1 on a bad volume, 2 for the FP64 oracle storage (not supported: its tail
+ * re-reads the points), 3 on an allocation failure (mode unchanged). Waits. */
+int32_t osn_tsdf_cuda_set_pipelined(OsnTsdfCudaVolume* v, int32_t enabled);
+/* Make the volume's stream wait for every queued update tail (pipelined
+ * mode; a no-op otherwise). 0 ok, 1 bad volume. */
+int32_t osn_tsdf_cuda_join(OsnTsdfCudaVolume* v);
 
 /* The volume's OSN_TSDF_STORAGE_* mode, or -1 for a NULL or invalid volume. */
 int32_t osn_tsdf_cuda_storage(const OsnTsdfCudaVolume* v);
@@ -218,7 +237,7 @@ int32_t osn_tsdf_cuda_last_update_stats(const OsnTsdfCudaVolume* v, int64_t* out
  * (no allocation during stream capture), serving loops that budget device
  * memory up front, latency-critical threads that cannot absorb the implied
  * synchronisation -- call this instead. Same results as update_voxels.
- * Its scratch is one fixed 48 MiB array inside the library, held on every
+ * Its scratch is one fixed 56 MiB array inside the library, held on every
  * GPU where the library's code is loaded until the process exits, and shared
  * by all calls: calls whose work overlaps on the GPU race and must be
  * serialised. The first call on a device resolves the array's address and

@@ -66,6 +66,8 @@ _SIG = {
     "osn_tsdf_cuda_synchronize": (None, [_P]),
     "osn_tsdf_cuda_status": (C.c_uint32, [_P]),
     "osn_tsdf_cuda_stream": (_P, [_P]),
+    "osn_tsdf_cuda_set_pipelined": (_I, [_P, _I]),
+    "osn_tsdf_cuda_join": (_I, [_P]),
     "osn_tsdf_cuda_storage": (_I, [_P]),
     "osn_tsdf_cuda_snapshot_bytes": (C.c_int64, [_P]),
     "osn_tsdf_cuda_snapshot": (C.c_int64, [_P, _P, C.c_int64]),

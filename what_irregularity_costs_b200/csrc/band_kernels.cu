@@ -294,7 +294,11 @@ __device__ __forceinline__ void band_point(const DevVolume& v, const BatchArgs& 
                         const int vz = unpack_axis(key, 0) * kBlockDim + (int)(lv >> 6);
                         fix = to_fix(clamp_sdf_n_f64(sdf_f64(v, a, r.px, r.py, r.pz, vx, vy, vz), v.trunc));
                     } else {
-                        fix = to_fix(fminf(fmaxf(__fmul_rn(sd[j], v.inv_trunc), -1.0f), 1.0f));
+                        const float sdf_n = fminf(fmaxf(__fmul_rn(sd[j], v.inv_trunc), -1.0f), 1.0f);
+                        fix = to_fix(sdf_n);
+                        // Kept for the records of voxels that cross the cap, so the
+                        // update tail never reads the batch's points again.
+                        __stcs(u.slot_val + (rec - u.records), sdf_n);
                     }
                     red_add(&u.vcnt[out], 1u);
                     red_add(&u.vacc[out], (unsigned long long)fix);

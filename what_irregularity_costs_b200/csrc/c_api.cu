@@ -234,6 +234,18 @@ uint32_t osn_tsdf_cuda_status(const OsnTsdfCudaVolume* v) {
     return usable(v) ? const_cast<OsnTsdfCudaVolume*>(v)->vol.status() : 0u;
 }
 
+int32_t osn_tsdf_cuda_set_pipelined(OsnTsdfCudaVolume* v, int32_t enabled) {
+    if (!usable(v)) return 1;
+    if (enabled && v->vol.storage() == osn_b200::kStoreF64) return 2;
+    return v->vol.set_pipelined(enabled != 0) ? 0 : 3;
+}
+
+int32_t osn_tsdf_cuda_join(OsnTsdfCudaVolume* v) {
+    if (!usable(v)) return 1;
+    v->vol.join();
+    return 0;
+}
+
 void* osn_tsdf_cuda_stream(const OsnTsdfCudaVolume* v) {
     return usable(v) ? (void*)v->vol.stream() : nullptr;
 }

@@ -32,9 +32,8 @@
 //   group      one pass over the records of the batch, eight per thread: a
 //              record of a tagged block whose voxel reserved a group takes
 //              the next place of the group (a few percent of the records).
-//   values     one thread per grouped record: its canonical id and
-//              normalised SDF, recomputed from its point (the walk's
-//              arithmetic, same rounding).
+//   values     one thread per grouped record: its canonical id (from its
+//              slot) and the normalised SDF the band walk kept for it.
 //   deferred   selects the keep records with the smallest ids of every
 //              crossing voxel and finishes it: one half-warp per small group
 //              (one record per lane, shuffle ranking), one warp per large group
@@ -313,17 +312,22 @@ finish_kernel(DevVolume v, UpdateScratch u) {
 // ---- group ---------------------------------------------------------------
 
 // Canonical id and normalised SDF (2^-40 fixed point) of the record in band
-// slot `slot`: the walk's arithmetic again for this one sample (same
-// rounding; the FP64 oracle's value in double).
+// slot `slot`: the value the band walk kept for the slot (the FP64 oracle
+// recomputes it from the point in double, with the walk's arithmetic).
 template <int S>
-__device__ __forceinline__ uint32_t slot_record(const DevVolume& v, const BatchArgs& a, uint32_t slot,
-                                                long long& fix) {
+__device__ __forceinline__ uint32_t slot_record(const DevVolume& v, const BatchArgs& a,
+                                                const UpdateScratch& u, uint32_t slot, long long& fix) {
     const uint32_t n_steps = 2u * (uint32_t)v.steps + 1u;
     if (a.n <= 0) {  // no batch: nothing to recompute (never a valid record)
         fix = 0;
         return 0xFFFFFFFFu;
     }
     const uint32_t s = slot / (uint32_t)a.n, i = slot - s * (uint32_t)a.n;
+    if constexpr (S != kStoreF64) {
+        // The band walk kept the slot's normalised SDF: no point is read again.
+        fix = to_fix(u.slot_val[slot]);
+        return i * n_steps + s;
+    }
     Ray r;
     int vx = 0, vy = 0, vz = 0;
     float sdf = 0.0f;
@@ -404,7 +408,7 @@ values_kernel(DevVolume v, BatchArgs a, UpdateScratch u) {
     const uint32_t n = (uint32_t)min((long long)u.ctl->x_used, (long long)u.record_cap);
     for (uint32_t k = blockIdx.x * kGroupThreads + threadIdx.x; k < n; k += gridDim.x * kGroupThreads) {
         long long fix;
-        const uint32_t id = slot_record<S>(v, a, u.deferred[k], fix);
+        const uint32_t id = slot_record<S>(v, a, u, u.deferred[k], fix);
         u.deferred[k] = id;
         u.deferred_fix[k] = fix;
     }
@@ -781,7 +785,7 @@ values_multi_kernel(StepWork w) {
         const uint32_t k = (uint32_t)(item - s_begin[sc]) * kGroupThreads + t;
         if (k < n) {
             long long fix;
-            const uint32_t id = slot_record<S>(sw.v, sw.a, sw.u.deferred[k], fix);
+            const uint32_t id = slot_record<S>(sw.v, sw.a, sw.u, sw.u.deferred[k], fix);
             sw.u.deferred[k] = id;
             sw.u.deferred_fix[k] = fix;
         }

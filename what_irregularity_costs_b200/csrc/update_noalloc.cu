@@ -12,9 +12,10 @@
 // with its scratch in one fixed array compiled into the library.
 //
 // The array is a file-scope __device__ variable of kNoAllocScratchBytes
-// (48 MiB + 256 bytes): the control counters, kNoAllocMaxRecords 4-byte band
-// records, as many 4-byte ids and 8-byte values of crossing voxels' records,
-// and half as many 16-byte crossing-voxel entries, i.e. batches with
+// (56 MiB + 256 bytes): the control counters, kNoAllocMaxRecords 4-byte band
+// records and 4-byte slot values, as many 4-byte ids and 8-byte values of
+// crossing voxels' records, and half as many 16-byte crossing-voxel entries,
+// i.e. batches with
 // n_points * (2 * steps + 1) <= 2,097,152 (a 480x360 frame at 9 band steps
 // per point fits; a 640x480 frame must be split in two). The per-voxel and
 // per-block state the update also uses belongs to the volume and was
@@ -41,9 +42,10 @@ constexpr int64_t kNoAllocMaxDeferred = kNoAllocMaxRecords / 2;
 constexpr size_t kNoAllocRecordBytes = (size_t)kNoAllocMaxRecords * sizeof(uint32_t);
 constexpr size_t kNoAllocDeferredBytes = (size_t)kNoAllocMaxRecords * sizeof(uint32_t);
 constexpr size_t kNoAllocFixBytes = (size_t)kNoAllocMaxRecords * sizeof(long long);
+constexpr size_t kNoAllocSlotValBytes = (size_t)kNoAllocMaxRecords * sizeof(float);
 constexpr size_t kNoAllocScratchBytes = kNoAllocHeaderBytes + kNoAllocRecordBytes +
                                         kNoAllocDeferredBytes + kNoAllocFixBytes +
-                                        (size_t)kNoAllocMaxDeferred * sizeof(int4);
+                                        (size_t)kNoAllocMaxDeferred * sizeof(int4) + kNoAllocSlotValBytes;
 static_assert(sizeof(UpdateControl) <= kNoAllocHeaderBytes, "control block must fit the header");
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
@@ -86,6 +88,9 @@ cudaError_t Volume::update_static_scratch(const BatchArgs& a, void* scratch) {
                                                   kNoAllocDeferredBytes);
     u.dvox = reinterpret_cast<int4*>(base + kNoAllocHeaderBytes + kNoAllocRecordBytes +
                                      kNoAllocDeferredBytes + kNoAllocFixBytes);
+    u.slot_val = dv_.storage == kStoreF64
+                     ? nullptr
+                     : reinterpret_cast<float*>(base + kNoAllocScratchBytes - kNoAllocSlotValBytes);
     u.record_cap = kNoAllocMaxRecords;
     u.dvox_cap = (int32_t)kNoAllocMaxDeferred;
     // Only the control counters must start at zero (run_update clears them);

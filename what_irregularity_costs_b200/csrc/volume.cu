@@ -115,6 +115,7 @@ bool Volume::alloc_device(uint32_t hash_slots) {
 }
 
 Volume::~Volume() {
+    if (pipelined_) set_pipelined(false);
     if (stream_) cudaStreamSynchronize(stream_);
     cudaFree(dv_.table);
     cudaFree(dv_.block_count);
@@ -133,6 +134,7 @@ Volume::~Volume() {
     cudaFree(us_.touched);
     cudaFree(us_.ctl);
     cudaFree(us_.records);
+    cudaFree(us_.slot_val);
     cudaFree(us_.deferred);
     cudaFree(us_.deferred_fix);
     cudaFree(us_.dvox);
@@ -150,7 +152,7 @@ Volume::~Volume() {
 
 // ---- timing ------------------------------------------------------------
 
-void Volume::mark_start(int) {
+void Volume::mark_start(int, cudaStream_t s) {
     if (!timing_) return;
     cudaEvent_t e;
     if (!event_pool_.empty()) {
@@ -159,11 +161,11 @@ void Volume::mark_start(int) {
     } else {
         cudaEventCreate(&e);
     }
-    cudaEventRecord(e, stream_);
+    cudaEventRecord(e, s ? s : stream_);
     open_start_ = e;
 }
 
-void Volume::mark_end(int id) {
+void Volume::mark_end(int id, cudaStream_t s) {
     if (!timing_ || !open_start_) return;
     cudaEvent_t e;
     if (!event_pool_.empty()) {
@@ -172,13 +174,13 @@ void Volume::mark_end(int id) {
     } else {
         cudaEventCreate(&e);
     }
-    cudaEventRecord(e, stream_);
+    cudaEventRecord(e, s ? s : stream_);
     pending_.push_back(Pending{id, open_start_, e});
     open_start_ = nullptr;
 }
 
 int Volume::kernel_times(double* ms, int64_t* launches, int n_ids) {
-    cudaStreamSynchronize(stream_);
+    synchronize();
     for (auto& p : pending_) {
         float t = 0.0f;
         if (cudaEventElapsedTime(&t, p.start, p.end) == cudaSuccess) {
@@ -209,12 +211,14 @@ cudaError_t Volume::allocate(const BatchArgs& a, int mode, unsigned long long* h
 bool Volume::ensure_records(int64_t n_records) {
     if (n_records <= us_.record_cap) return true;
     // Grows only; waits for in-flight work that may still read the old buffers.
-    cudaStreamSynchronize(stream_);
+    synchronize();
     cudaFree(us_.records);
+    cudaFree(us_.slot_val);
     cudaFree(us_.deferred);
     cudaFree(us_.deferred_fix);
     cudaFree(us_.dvox);
     us_.records = nullptr;
+    us_.slot_val = nullptr;
     us_.deferred = nullptr;
     us_.deferred_fix = nullptr;
     us_.dvox = nullptr;
@@ -224,46 +228,154 @@ bool Volume::ensure_records(int64_t n_records) {
     // the two crossing-voxel lists together.
     const int64_t n_dvox = n_records / 2 + 1;
     if (cudaMalloc(&us_.records, (size_t)n_records * sizeof(uint32_t)) != cudaSuccess) return false;
+    if (dv_.storage != kStoreF64 &&
+        cudaMalloc(&us_.slot_val, (size_t)n_records * sizeof(float)) != cudaSuccess)
+        return false;
     if (cudaMalloc(&us_.deferred, (size_t)n_records * sizeof(uint32_t)) != cudaSuccess) return false;
     if (cudaMalloc(&us_.deferred_fix, (size_t)n_records * sizeof(long long)) != cudaSuccess)
         return false;
     if (cudaMalloc(&us_.dvox, (size_t)n_dvox * sizeof(int4)) != cudaSuccess) return false;
     us_.record_cap = n_records;
     us_.dvox_cap = (int32_t)std::min<int64_t>(n_dvox, INT32_MAX);
+    if (pipelined_) {  // the second set's records and slot values grow with the first
+        cudaFree(us2_.records);
+        cudaFree(us2_.slot_val);
+        us2_.records = nullptr;
+        us2_.slot_val = nullptr;
+        if (cudaMalloc(&us2_.records, (size_t)n_records * sizeof(uint32_t)) != cudaSuccess) return false;
+        if (cudaMalloc(&us2_.slot_val, (size_t)n_records * sizeof(float)) != cudaSuccess) return false;
+    }
     return true;
 }
 
+// ---- pipelining --------------------------------------------------------
+
+bool Volume::alloc_second_set() {
+    const size_t n_vox = (size_t)dv_.pool_capacity * kBlockVoxels;
+    us2_ = UpdateScratch{};
+    if (cudaMalloc(&us2_.ctl, sizeof(UpdateControl)) != cudaSuccess) return false;
+    if (cudaMalloc(&us2_.vcnt, n_vox * sizeof(uint32_t)) != cudaSuccess) return false;
+    if (cudaMalloc(&us2_.vacc, n_vox * sizeof(unsigned long long)) != cudaSuccess) return false;
+    if (cudaMalloc(&us2_.touched, (size_t)dv_.pool_capacity * sizeof(int32_t)) != cudaSuccess) return false;
+    if (us_.record_cap > 0) {
+        if (cudaMalloc(&us2_.records, (size_t)us_.record_cap * sizeof(uint32_t)) != cudaSuccess) return false;
+        if (cudaMalloc(&us2_.slot_val, (size_t)us_.record_cap * sizeof(float)) != cudaSuccess) return false;
+    }
+    if (cudaMemsetAsync(us2_.ctl, 0, sizeof(UpdateControl), stream_) != cudaSuccess) return false;
+    if (cudaMemsetAsync(us2_.vcnt, 0, n_vox * sizeof(uint32_t), stream_) != cudaSuccess) return false;
+    if (cudaMemsetAsync(us2_.vacc, 0, n_vox * sizeof(unsigned long long), stream_) != cudaSuccess)
+        return false;
+    return cudaStreamSynchronize(stream_) == cudaSuccess;
+}
+
+void Volume::free_second_set() {
+    cudaFree(us2_.ctl);
+    cudaFree(us2_.vcnt);
+    cudaFree(us2_.vacc);
+    cudaFree(us2_.touched);
+    cudaFree(us2_.records);
+    cudaFree(us2_.slot_val);
+    us2_ = UpdateScratch{};
+}
+
+bool Volume::set_pipelined(bool on) {
+    if (on == pipelined_) return true;
+    synchronize();
+    if (!on) {
+        pipelined_ = false;
+        free_second_set();
+        for (int k = 0; k < 2; ++k) {
+            if (band_done_[k]) cudaEventDestroy(band_done_[k]);
+            if (tail_done_[k]) cudaEventDestroy(tail_done_[k]);
+            band_done_[k] = tail_done_[k] = nullptr;
+        }
+        if (tail_) cudaStreamDestroy(tail_);
+        tail_ = nullptr;
+        if (last_ctl_ != us_.ctl && last_ctl_ != nullptr) last_ctl_ = nullptr;  // its set is gone
+        return true;
+    }
+    if (dv_.storage == kStoreF64) return false;  // the oracle's tail reads the points
+    if (cudaStreamCreate(&tail_) != cudaSuccess) return false;
+    for (int k = 0; k < 2; ++k) {
+        if (cudaEventCreateWithFlags(&band_done_[k], cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&tail_done_[k], cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventRecord(tail_done_[k], stream_) != cudaSuccess)
+            return false;
+    }
+    if (!alloc_second_set()) {
+        free_second_set();
+        return false;
+    }
+    n_updates_ = 0;
+    pipelined_ = true;
+    return true;
+}
+
+void Volume::join() {
+    if (pipelined_ && n_updates_ > 0) cudaStreamWaitEvent(stream_, tail_done_[(n_updates_ - 1) & 1], 0);
+}
+
 cudaError_t Volume::run_update(const BatchArgs& a, const UpdateScratch& scratch, bool insert) {
+    // Pipelined: this update's scratch set alternates; its walk waits only for
+    // the tail two updates back (the last user of that set), its tail for its
+    // walk. The walk's saturation filter may read weights the previous tail is
+    // still writing: weights only grow, and finish decides acceptance from the
+    // final weights, so a stale read only lets through a sample finish rejects.
+    const bool pipe = pipelined_ && scratch.ctl == us_.ctl;  // not the fixed no-alloc scratch
+    if (pipelined_ && !pipe) join();
     // Block tags are update numbers; at the (theoretical) wrap, clear them.
     if (++update_tag_ == 0u) {
+        join();
         cudaMemsetAsync(us_.blk_touch, 0, (size_t)dv_.pool_capacity * sizeof(uint32_t), stream_);
         cudaMemsetAsync(us_.blk_cross, 0, (size_t)dv_.pool_capacity * sizeof(uint32_t), stream_);
         update_tag_ = 1u;
     }
     UpdateScratch u = scratch;
+    const int p = (int)(n_updates_ & 1);
+    if (pipe && p == 1) {
+        u.ctl = us2_.ctl;
+        u.records = us2_.records;
+        u.slot_val = us2_.slot_val;
+        u.vcnt = us2_.vcnt;
+        u.vacc = us2_.vacc;
+        u.touched = us2_.touched;
+    }
     u.tag = update_tag_;
-    cudaError_t e = cudaMemsetAsync(u.ctl, 0, sizeof(UpdateControl), stream_);
+    cudaStream_t tail = pipe ? tail_ : stream_;
+    cudaError_t e = cudaSuccess;
+    if (pipe) e = cudaStreamWaitEvent(stream_, tail_done_[p], 0);
+    if (e == cudaSuccess) e = cudaMemsetAsync(u.ctl, 0, sizeof(UpdateControl), stream_);
     if (e != cudaSuccess) return e;
     mark_start(kKBand);
     e = launch_band_records(dv_, a, u, insert, sm_count_, stream_);
     mark_end(kKBand);
     if (e != cudaSuccess) return e;
-    mark_start(kKFinish);
-    e = launch_finish(dv_, u, sm_count_, stream_);
-    mark_end(kKFinish);
+    if (pipe) {
+        if ((e = cudaEventRecord(band_done_[p], stream_)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(tail_, band_done_[p], 0)) != cudaSuccess) return e;
+    }
+    last_ctl_ = u.ctl;
+    mark_start(kKFinish, tail);
+    e = launch_finish(dv_, u, sm_count_, tail);
+    mark_end(kKFinish, tail);
     if (e != cudaSuccess) return e;
-    mark_start(kKGroup);
-    e = launch_group(dv_, a, u, stream_);
-    mark_end(kKGroup);
+    mark_start(kKGroup, tail);
+    e = launch_group(dv_, a, u, tail);
+    mark_end(kKGroup, tail);
     if (e != cudaSuccess) return e;
-    mark_start(kKValues);
-    e = launch_values(dv_, a, u, sm_count_ * 4, stream_);
-    mark_end(kKValues);
+    mark_start(kKValues, tail);
+    e = launch_values(dv_, a, u, sm_count_ * 4, tail);
+    mark_end(kKValues, tail);
     if (e != cudaSuccess) return e;
-    mark_start(kKDeferred);
-    e = launch_deferred(dv_, u, sm_count_, stream_);
-    mark_end(kKDeferred);
-    return e;
+    mark_start(kKDeferred, tail);
+    e = launch_deferred(dv_, u, sm_count_, tail);
+    mark_end(kKDeferred, tail);
+    if (e != cudaSuccess) return e;
+    if (pipe) {
+        if ((e = cudaEventRecord(tail_done_[p], tail_)) != cudaSuccess) return e;
+        ++n_updates_;
+    }
+    return cudaSuccess;
 }
 
 // Records a batch of n points needs: one per band slot.
@@ -297,6 +409,7 @@ bool Volume::ensure_mesh(int32_t cap, bool rgb) {
 
 int32_t Volume::extract(float* posnor, uint8_t* rgb, int32_t cap, float min_w, float iso,
                         bool host_out) {
+    join();
     const int32_t n_blocks = block_count();  // waits for the stream
     if (n_blocks <= 0) return 0;
     float* d_pos = posnor;
@@ -333,6 +446,8 @@ int32_t Volume::extract(float* posnor, uint8_t* rgb, int32_t cap, float min_w, f
 }
 
 bool Volume::reserve_batch(int32_t max_points) {
+    // A batch drives the volume's updates with its own scratch use: serial.
+    if (pipelined_) set_pipelined(false);
     return max_points > 0 && ensure_records(batch_records(max_points, dv_.steps));
 }
 
@@ -354,6 +469,7 @@ SceneWork Volume::batch_work(const BatchArgs& a, cudaStream_t s) {
 }
 
 cudaError_t Volume::reset() {
+    join();
     const int32_t n_blocks = std::min(block_count(), dv_.pool_capacity);
     mark_start(kKReset);
     cudaError_t e = launch_reset_table(dv_.table, dv_.hash_mask + 1, kEmptyKey, stream_);
@@ -368,11 +484,15 @@ cudaError_t Volume::reset() {
     if (e == cudaSuccess) e = cudaMemsetAsync(us_.vcnt, 0, n_vox * sizeof(uint32_t), stream_);
     if (e == cudaSuccess)
         e = cudaMemsetAsync(us_.vacc, 0, n_vox * sizeof(unsigned long long), stream_);
+    if (pipelined_ && e == cudaSuccess) e = cudaMemsetAsync(us2_.vcnt, 0, n_vox * sizeof(uint32_t), stream_);
+    if (pipelined_ && e == cudaSuccess)
+        e = cudaMemsetAsync(us2_.vacc, 0, n_vox * sizeof(unsigned long long), stream_);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
     return e;
 }
 
 int32_t Volume::block_count() {
+    join();
     int32_t* hs = reinterpret_cast<int32_t*>(host_small_);
     cudaMemcpyAsync(hs, dv_.block_count, sizeof(int32_t), cudaMemcpyDeviceToHost, stream_);
     cudaStreamSynchronize(stream_);
@@ -380,6 +500,7 @@ int32_t Volume::block_count() {
 }
 
 uint64_t Volume::drop_count() {
+    join();
     uint64_t* hs = reinterpret_cast<uint64_t*>(host_small_);
     cudaMemcpyAsync(hs, dv_.drop_count, sizeof(uint64_t), cudaMemcpyDeviceToHost, stream_);
     cudaStreamSynchronize(stream_);
@@ -387,6 +508,7 @@ uint64_t Volume::drop_count() {
 }
 
 uint32_t Volume::status() {
+    join();
     uint32_t* hs = reinterpret_cast<uint32_t*>(host_small_);
     cudaMemcpyAsync(hs, dv_.status, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_);
     cudaStreamSynchronize(stream_);
@@ -394,8 +516,10 @@ uint32_t Volume::status() {
 }
 
 bool Volume::last_update_stats(int64_t out[4]) {
+    join();
     UpdateControl c{};
-    if (cudaMemcpyAsync(host_small_, us_.ctl, sizeof(UpdateControl), cudaMemcpyDeviceToHost,
+    if (cudaMemcpyAsync(host_small_, last_ctl_ ? last_ctl_ : us_.ctl, sizeof(UpdateControl),
+                        cudaMemcpyDeviceToHost,
                         stream_) != cudaSuccess ||
         cudaStreamSynchronize(stream_) != cudaSuccess)
         return false;

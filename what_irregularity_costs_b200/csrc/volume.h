@@ -59,6 +59,8 @@ constexpr int32_t kMaxPoolBlocks = (1 << 23) - 1;
 struct UpdateScratch {
     UpdateControl* ctl = nullptr;
     uint32_t* records = nullptr;  // [record_cap] one per band slot
+    float* slot_val = nullptr;    // [record_cap] normalised SDF of each counted slot (FP32 / FP16
+                                  // storage; null for the FP64 oracle, which recomputes it)
     uint32_t* deferred = nullptr;       // [record_cap] canonical ids of crossing voxels' records, grouped per voxel
     long long* deferred_fix = nullptr;  // [record_cap] their normalised SDFs, 2^-40 fixed point
     int4* dvox = nullptr;               // [dvox_cap] (voxel, group base, records, accepted)
@@ -107,8 +109,21 @@ public:
     int32_t block_count();
     uint64_t drop_count();
     uint32_t status();
-    void synchronize() { cudaStreamSynchronize(stream_); }
+    void synchronize() {
+        join();
+        cudaStreamSynchronize(stream_);
+    }
     bool last_update_stats(int64_t out[4]);
+
+    // Pipelined updates. When on, an update's band walk runs on stream() and
+    // its tail (finish, group, values, deferred) on an internal stream, so the
+    // next update's walk overlaps this one's tail; the per-update scratch
+    // alternates between two sets. Every reader of results joins first.
+    // Not available for the FP64 oracle storage (its tail reads the points).
+    bool set_pipelined(bool on);
+    bool pipelined() const { return pipelined_; }
+    // Make stream() wait for every queued update tail.
+    void join();
 
     // Snapshot of the allocated blocks through host memory (snapshot.cu):
     // bytes needed, write (returns bytes or -1), restore into this volume
@@ -127,8 +142,8 @@ public:
     // Timing.
     void set_timing(bool on) { timing_ = on; }
     int kernel_times(double* ms, int64_t* launches, int n_ids);
-    void mark_start(int id);
-    void mark_end(int id);
+    void mark_start(int id, cudaStream_t s = nullptr);
+    void mark_end(int id, cudaStream_t s = nullptr);
 
 private:
     bool alloc_device(uint32_t hash_slots);
@@ -142,6 +157,18 @@ private:
     cudaStream_t stream_ = nullptr;
     UpdateScratch us_{};
     uint32_t update_tag_ = 0;  // number of the last update (block tags)
+
+    // Pipelining: the second scratch set (its ctl, records, slot_val, vcnt,
+    // vacc and touched), the tail stream and the hand-over events.
+    bool pipelined_ = false;
+    cudaStream_t tail_ = nullptr;
+    UpdateScratch us2_{};
+    cudaEvent_t band_done_[2] = {nullptr, nullptr};
+    cudaEvent_t tail_done_[2] = {nullptr, nullptr};
+    uint64_t n_updates_ = 0;
+    UpdateControl* last_ctl_ = nullptr;  // counters of the last update
+    bool alloc_second_set();
+    void free_second_set();
     int sm_count_ = 148;
 
     // Extraction scratch (device output for the host-copy path, counters).
