@@ -32,8 +32,10 @@
 //   group      one pass over the records of the batch, eight per thread: a
 //              record of a tagged block whose voxel reserved a group takes
 //              the next place of the group (a few percent of the records).
-//   values     one thread per grouped record: its canonical id (from its
-//              slot) and the normalised SDF the band walk kept for it.
+//   values     (FP64 oracle only) one thread per grouped record: its
+//              canonical id and its normalised SDF recomputed in double from
+//              its point. FP32 / FP16 records carry their band slot, from
+//              which deferred reads the id and the value the walk kept.
 //   deferred   selects the keep records with the smallest ids of every
 //              crossing voxel and finishes it: one half-warp per small group
 //              (one record per lane, shuffle ranking), one warp per large group
@@ -493,6 +495,39 @@ __device__ uint32_t radix_select(const uint32_t* ids, int n, int keep, uint32_t*
     return prefix;
 }
 
+// Id and fixed-point value of the record at group position pos: as the values
+// pass left them (the FP64 oracle), or from the record's band slot (FP32 /
+// FP16 storage: id from the slot's point and step, value kept by the walk).
+template <int S>
+__device__ __forceinline__ void group_record(const UpdateScratch& u, uint32_t n_pts, uint32_t n_steps,
+                                             uint32_t pos, uint32_t& id, long long& fix) {
+    if constexpr (S == kStoreF64) {
+        id = u.deferred[pos];
+        fix = u.deferred_fix[pos];
+    } else {
+        const uint32_t slot = u.deferred[pos];
+        const uint32_t st = slot / n_pts;
+        id = (slot - st * n_pts) * n_steps + st;
+        fix = to_fix(u.slot_val[slot]);
+    }
+}
+
+// A large group's records as (id, value) arrays in place, by the whole warp.
+template <int S>
+__device__ __forceinline__ void group_to_ids(const UpdateScratch& u, uint32_t n_pts, uint32_t n_steps,
+                                             uint32_t base, int n, int lane) {
+    if constexpr (S != kStoreF64) {
+        for (int k = lane; k < n; k += 32) {
+            uint32_t id;
+            long long fix;
+            group_record<S>(u, n_pts, n_steps, base + (uint32_t)k, id, fix);
+            u.deferred[base + k] = id;
+            u.deferred_fix[base + k] = fix;
+        }
+        __syncwarp();
+    }
+}
+
 // One warp per voxel of the large list: up to 8 records per lane ranked by id
 // against all others in registers, a radix select of the keep-th id beyond
 // 256 records. Returns the sum of the accepted values (on every lane).
@@ -540,7 +575,7 @@ __device__ long long warp_select(const uint32_t* ids, const long long* vals, int
 
 template <int S>
 __global__ void __launch_bounds__(kDeferThreads)
-deferred_kernel(DevVolume v, UpdateScratch u) {
+deferred_kernel(DevVolume v, BatchArgs a, UpdateScratch u) {
     __shared__ uint32_t hist[kDeferWarps][256];
     __shared__ int s_updated;
     if (threadIdx.x == 0) s_updated = 0;
@@ -548,6 +583,7 @@ deferred_kernel(DevVolume v, UpdateScratch u) {
     launch_dependents();
     grid_dependency_wait();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t n_steps = 2u * (uint32_t)v.steps + 1u;
     const unsigned long long lists = u.ctl->def_lists;
     int n_small = (int)(lists & 0xFFFFFFFFull), n_large = (int)(lists >> 32);
     if ((long long)n_small + n_large > (long long)u.dvox_cap) n_small = n_large = 0;  // overflowed
@@ -557,6 +593,7 @@ deferred_kernel(DevVolume v, UpdateScratch u) {
     const int gw = blockIdx.x * kDeferWarps + warp, nw = gridDim.x * kDeferWarps;
     for (int d = gw; d < n_large; d += nw) {
         const int4 e = u.dvox[u.dvox_cap - 1 - d];  // (voxel, group base, records, accepted)
+        group_to_ids<S>(u, (uint32_t)a.n, n_steps, (uint32_t)e.y, e.z, lane);
         const long long fix = warp_select(u.deferred + (uint32_t)e.y, u.deferred_fix + (uint32_t)e.y,
                                           e.z, e.w, hist[warp], lane);
         if (lane == 0) {
@@ -575,8 +612,9 @@ deferred_kernel(DevVolume v, UpdateScratch u) {
         const int4 e = live ? u.dvox[d] : make_int4(0, 0, 0, 0);
         const int n = e.z, keep = e.w;
         const bool mine = live && hl < n;
-        const uint32_t id = mine ? u.deferred[(uint32_t)e.y + hl] : 0xFFFFFFFFu;
-        const long long val = mine ? u.deferred_fix[(uint32_t)e.y + hl] : 0ll;
+        uint32_t id = 0xFFFFFFFFu;
+        long long val = 0ll;
+        if (mine) group_record<S>(u, (uint32_t)a.n, n_steps, (uint32_t)e.y + hl, id, val);
         int rank = 0;
 #pragma unroll
         for (int src = 0; src < 16; ++src) rank += __shfl_sync(0xffffffffu, id, src, 16) < id ? 1 : 0;
@@ -814,12 +852,14 @@ deferred_multi_kernel(StepWork w) {
         const SceneWork& sw = w.scenes[sc];
         const DevVolume& v = sw.v;
         const UpdateScratch& u = sw.u;
+        const uint32_t n_steps = 2u * (uint32_t)v.steps + 1u;
         const unsigned long long lists = u.ctl->def_lists;
         const int n_small = (int)(lists & 0xFFFFFFFFull), n_large = (int)(lists >> 32);
         const int local = item - s_begin[sc];
         int done = 0;
         if (local < n_large) {
-            const int4 e = u.dvox[u.dvox_cap - 1 - local];
+                const int4 e = u.dvox[u.dvox_cap - 1 - local];
+            group_to_ids<S>(u, (uint32_t)sw.a.n, n_steps, (uint32_t)e.y, e.z, lane);
             const long long fix = warp_select(u.deferred + (uint32_t)e.y, u.deferred_fix + (uint32_t)e.y,
                                               e.z, e.w, hist[warp], lane);
             if (lane == 0) finish_voxel<S>(v, u, (uint32_t)e.x, e.w, fix);
@@ -832,8 +872,9 @@ deferred_multi_kernel(StepWork w) {
             const int4 e = live ? u.dvox[d] : make_int4(0, 0, 0, 0);
             const int n = e.z, keep = e.w;
             const bool mine = live && hl < n;
-            const uint32_t id = mine ? u.deferred[(uint32_t)e.y + hl] : 0xFFFFFFFFu;
-            const long long val = mine ? u.deferred_fix[(uint32_t)e.y + hl] : 0ll;
+            uint32_t id = 0xFFFFFFFFu;
+            long long val = 0ll;
+            if (mine) group_record<S>(u, (uint32_t)sw.a.n, n_steps, (uint32_t)e.y + hl, id, val);
             int rank = 0;
 #pragma unroll
             for (int src = 0; src < 16; ++src) rank += __shfl_sync(0xffffffffu, id, src, 16) < id ? 1 : 0;
@@ -890,6 +931,9 @@ cudaError_t launch_group(const DevVolume& v, const BatchArgs& a, const UpdateScr
 
 cudaError_t launch_values(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u, int n_ctas,
                           cudaStream_t s) {
+    // FP32 / FP16: the deferred pass reads each record's id and value from its
+    // band slot itself; only the FP64 oracle recomputes values from points.
+    if (v.storage != kStoreF64) return cudaSuccess;
     switch (v.storage) {
         case kStoreF16U16: return launch_after(values_kernel<kStoreF16U16>, n_ctas, kGroupThreads, s, v, a, u);
         case kStoreF64: return launch_after(values_kernel<kStoreF64>, n_ctas, kGroupThreads, s, v, a, u);
@@ -897,19 +941,20 @@ cudaError_t launch_values(const DevVolume& v, const BatchArgs& a, const UpdateSc
     }
 }
 
-cudaError_t launch_deferred(const DevVolume& v, const UpdateScratch& u, int sm_count, cudaStream_t s) {
+cudaError_t launch_deferred(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u, int sm_count,
+                            cudaStream_t s) {
     switch (v.storage) {
         case kStoreF16U16: {
             return launch_after(deferred_kernel<kStoreF16U16>, resident_grid<deferred_kernel<kStoreF16U16>>(kDeferThreads, sm_count),
-                                kDeferThreads, s, v, u);
+                                kDeferThreads, s, v, a, u);
         }
         case kStoreF64: {
             return launch_after(deferred_kernel<kStoreF64>, resident_grid<deferred_kernel<kStoreF64>>(kDeferThreads, sm_count),
-                                kDeferThreads, s, v, u);
+                                kDeferThreads, s, v, a, u);
         }
         default: {
             return launch_after(deferred_kernel<kStoreF32>, resident_grid<deferred_kernel<kStoreF32>>(kDeferThreads, sm_count),
-                                kDeferThreads, s, v, u);
+                                kDeferThreads, s, v, a, u);
         }
     }
 }
@@ -958,6 +1003,7 @@ cudaError_t launch_group_multi(const StepWork& w, int sm_count, cudaStream_t s) 
 }
 
 cudaError_t launch_values_multi(const StepWork& w, int storage, int sm_count, cudaStream_t s) {
+    if (storage != kStoreF64) return cudaSuccess;  // deferred_multi reads the band slots itself
     switch (storage) {
         case kStoreF16U16: return values_multi_t<kStoreF16U16>(w, sm_count, s);
         case kStoreF64: return values_multi_t<kStoreF64>(w, sm_count, s);

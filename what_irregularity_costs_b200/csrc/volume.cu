@@ -368,7 +368,7 @@ cudaError_t Volume::run_update(const BatchArgs& a, const UpdateScratch& scratch,
     mark_end(kKValues, tail);
     if (e != cudaSuccess) return e;
     mark_start(kKDeferred, tail);
-    e = launch_deferred(dv_, u, sm_count_, tail);
+    e = launch_deferred(dv_, a, u, sm_count_, tail);
     mark_end(kKDeferred, tail);
     if (e != cudaSuccess) return e;
     if (pipe) {

@@ -229,7 +229,8 @@ cudaError_t launch_group(const DevVolume& v, const BatchArgs& a, const UpdateScr
                          cudaStream_t s);
 cudaError_t launch_values(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u, int n_ctas,
                           cudaStream_t s);
-cudaError_t launch_deferred(const DevVolume& v, const UpdateScratch& u, int sm_count, cudaStream_t s);
+cudaError_t launch_deferred(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u, int sm_count,
+                            cudaStream_t s);
 
 }  // namespace osn_b200
 
