@@ -98,3 +98,37 @@ def make_volumes(specs, storage: int):
 
 def upload(frames, torch):
     return [[torch.from_numpy(p).cuda() for p, _ in fr] for fr in frames]
+
+
+def _main():
+    """A small batched run of the scene mix (a profiling case): the first
+    --scenes scenes integrate --steps frames each through one batch (FP16
+    storage, the autotuner's shape for the mix), then the batch status is
+    printed."""
+    import argparse
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--scenes", type=int, default=8)
+    ap.add_argument("--steps", type=int, default=6)
+    args = ap.parse_args()
+    specs = scene_mix(32)[: args.scenes]
+    frames = mix_frames(specs, args.steps)
+    import torch
+    from . import STORAGE_FP16_U16, Batch
+    dev = upload(frames, torch)
+    vols = make_volumes(specs, STORAGE_FP16_U16)
+    b = Batch(len(specs))
+    b.set_shape(8, 0, 1)
+    for v, sp in zip(vols, specs):
+        b.add(v, sp.max_points)
+    for k in range(args.steps):
+        for i, fr in enumerate(frames):
+            if k < len(fr):
+                b.set_frame(i, dev[i][k], fr[k][1])
+        b.step()
+    b.synchronize()
+    print(f"batched {args.scenes} scenes x {args.steps} steps: status {b.status()}, "
+          f"blocks {[v.block_count() for v in vols]}")
+
+
+if __name__ == "__main__":
+    _main()
