@@ -363,10 +363,12 @@ cudaError_t Volume::run_update(const BatchArgs& a, const UpdateScratch& scratch,
     e = launch_group(dv_, a, u, tail);
     mark_end(kKGroup, tail);
     if (e != cudaSuccess) return e;
-    mark_start(kKValues, tail);
-    e = launch_values(dv_, a, u, sm_count_ * 4, tail);
-    mark_end(kKValues, tail);
-    if (e != cudaSuccess) return e;
+    if (dv_.storage == kStoreF64) {  // other storages: deferred reads the band slots
+        mark_start(kKValues, tail);
+        e = launch_values(dv_, a, u, sm_count_ * 4, tail);
+        mark_end(kKValues, tail);
+        if (e != cudaSuccess) return e;
+    }
     mark_start(kKDeferred, tail);
     e = launch_deferred(dv_, a, u, sm_count_, tail);
     mark_end(kKDeferred, tail);
