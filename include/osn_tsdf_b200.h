@@ -193,7 +193,7 @@ void* osn_tsdf_cuda_stream(const OsnTsdfCudaVolume* v);
 
 /* Pipelined updates. When enabled, an integrate/update call's band walk is
  * queued on the volume's stream as usual but its update tail (finish, group,
- * values, deferred) runs on an internal stream, so the next call's walk
+ * deferred) runs on an internal stream, so the next call's walk
  * overlaps this call's tail; the per-call scratch alternates between two sets
  * (twice the per-voxel batch state: +12 bytes per voxel). Results are
  * identical. The positions (or depth image) of a call may be reused once the
