@@ -144,6 +144,26 @@ OsnTsdfCudaVolume* osn_tsdf_cuda_create_ex(float voxel_size_m, int32_t pool_capa
 int32_t osn_tsdf_cuda_integrate(OsnTsdfCudaVolume* v, const float* d_positions, int32_t n_points,
                                 float cam_x, float cam_y, float cam_z, float radius_m);
 
+/* integrate of several consecutive frames in one call (no counterpart in the
+ * reference). Frame k's points are d_positions[frame_begin[k] ..
+ * frame_begin[k + 1]) (a DEVICE xyz float array holding all frames' points
+ * back to back), seen from the camera at cams_xyz[3k .. 3k + 2];
+ * frame_begin (n_frames + 1 entries, frame_begin[0] = 0, non-decreasing) and
+ * cams_xyz (3 * n_frames) are HOST arrays, read during the call. At most
+ * OSN_TSDF_MAX_FRAMES frames per call.
+ * The cap keeps the same contributions as n_frames successive integrate
+ * calls (accept while the weight before a contribution is below the cap, in
+ * frame, point, step order), so the block set, the weights and the colour
+ * sums are identical to theirs; a voxel's stored TSDF takes one rounding per
+ * call instead of one per frame. The per-call costs (kernel boundaries, the
+ * update tail's pass over the touched blocks, which consecutive frames
+ * largely share) are paid once for all the call's frames. FP32 and FP16
+ * storage; 2 for the FP64 oracle. Other return codes as integrate. */
+#define OSN_TSDF_MAX_FRAMES 32
+int32_t osn_tsdf_cuda_integrate_frames(OsnTsdfCudaVolume* v, const float* d_positions,
+                                       const int32_t* frame_begin, const float* cams_xyz,
+                                       int32_t n_frames, float radius_m);
+
 /* integrate from a depth image, unprojected inside the band walk: pixel
  * (u, v) with depth z (metres along the optical axis, d_depth is a DEVICE
  * float array of height * width in raster order) becomes the world point

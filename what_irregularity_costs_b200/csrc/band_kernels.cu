@@ -169,11 +169,15 @@ struct BandSmem {
 constexpr int kProbeWarp = 0;  // equal keys grouped across the warp, one leader probes
 constexpr int kProbeLane = 1;  // every lane probes its own runs (L1 shares the loads)
 
-template <int MODE, bool RECORDS, int S, int PROBE = kProbeWarp>
+// FRAMES: the batch holds several frames; (cx, cy, cz) is the camera of
+// point i's frame (otherwise the batch's one camera is used).
+template <int MODE, bool RECORDS, int S, int PROBE = kProbeWarp, bool FRAMES = false>
 __device__ __forceinline__ void band_point(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
                                            int i, bool has, float px, float py, float pz, BandSmem& sm,
                                            uint32_t& drops, uint32_t& counted,
-                                           unsigned long long* hist, int n_bins) {
+                                           unsigned long long* hist, int n_bins, float cx = 0.0f,
+                                           float cy = 0.0f, float cz = 0.0f) {
+    static_assert(!(FRAMES && S == kStoreF64), "the FP64 oracle integrates one frame per batch");
     const int t = threadIdx.x;
     const int lane = t & 31, wbase = t & ~31;
     const bool counts_drops = MODE != kLookupOnly && MODE != kAllocNoCas && MODE != kAllocCountingCas;
@@ -182,7 +186,9 @@ __device__ __forceinline__ void band_point(const DevVolume& v, const BatchArgs& 
     auto& run_bi = sm.run_bi;
     auto& run_src = sm.run_src;
     Ray r;
-    const bool live = i < a.n && has && ray_setup_at(a, px, py, pz, r);
+    const bool live = i < a.n && has &&
+                      (FRAMES ? ray_setup_cam(a.radius_sq, cx, cy, cz, px, py, pz, r)
+                              : ray_setup_at(a, px, py, pz, r));
     uint32_t* rec = RECORDS ? u.records + i : nullptr;  // slot (s = -steps, i)
 
     for (int c0 = -v.steps; c0 <= v.steps; c0 += kChunk) {
@@ -199,7 +205,8 @@ __device__ __forceinline__ void band_point(const DevVolume& v, const BatchArgs& 
             const int s = c0 + j;
             int vx, vy, vz;
             float sdf;
-            if (live && s <= v.steps && band_sample(v, a, r, s, vx, vy, vz, sdf)) {
+            if (live && s <= v.steps &&
+                (FRAMES ? band_sample_ray(v, r, s, vx, vy, vz, sdf) : band_sample(v, a, r, s, vx, vy, vz, sdf))) {
                 const int bx = vx >> 3, by = vy >> 3, bz = vz >> 3;  // floor_div(v, 8)
                 const long long key = pack_key(bx, by, bz);
                 // A straight ray leaves a block (a convex box) for good, so
@@ -312,10 +319,41 @@ __device__ __forceinline__ void band_point(const DevVolume& v, const BatchArgs& 
     }
 }
 
-template <int MODE, bool RECORDS, int S, bool DEPTH = false>
-__global__ void __launch_bounds__(kBandThreads, kBandMinBlocks)
-band_kernel(DevVolume v, BatchArgs a, UpdateScratch u, unsigned long long* hist, int n_bins) {
-    constexpr int kSource = DEPTH ? 1 : 0;
+// The camera of every point of a batch with one camera: nothing to track.
+struct OneCamera {
+    float cx = 0.0f, cy = 0.0f, cz = 0.0f;
+    __device__ __forceinline__ void at(int) {}
+};
+
+// The camera of each point of a batch of several frames. A thread's points
+// only move forward (tile += grid size), so its frame does too: one
+// comparison per tile, and a table read only where the frame changes.
+struct FrameCursor {
+    const FrameCam* frames;
+    int32_t n, f, next;
+    float cx, cy, cz;
+    __device__ __forceinline__ FrameCursor(const FrameCam* fr, int32_t nf) : frames(fr), n(nf), f(0) {
+        load();
+    }
+    __device__ __forceinline__ void load() {
+        cx = __ldg(&frames[f].x);
+        cy = __ldg(&frames[f].y);
+        cz = __ldg(&frames[f].z);
+        next = f + 1 < n ? __ldg(&frames[f + 1].begin) : INT_MAX;
+    }
+    __device__ __forceinline__ void at(int i) {
+        while (i >= next) {  // the last frame's bound is INT_MAX
+            ++f;
+            load();
+        }
+    }
+};
+
+// A persistent CTA's share of a batch: tiles of 128 points, strided by the
+// grid, then the CTA's drop and record counts.
+template <int MODE, bool RECORDS, int S, int SOURCE, bool FRAMES, typename Camera>
+__device__ __forceinline__ void band_tiles(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
+                                           unsigned long long* hist, int n_bins, Camera cam) {
     __shared__ BandSmem sm;
     const int t = threadIdx.x;
     const int lane = t & 31;
@@ -335,7 +373,7 @@ band_kernel(DevVolume v, BatchArgs a, UpdateScratch u, unsigned long long* hist,
     bool nhas = false;
     {
         const int i0 = blockIdx.x * kBandThreads + t;
-        if (blockIdx.x < n_tiles && i0 < a.n) nhas = load_point<kSource>(a, i0, nx, ny, nz);
+        if (blockIdx.x < n_tiles && i0 < a.n) nhas = load_point<SOURCE>(a, i0, nx, ny, nz);
     }
     for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
         const int i = tile * kBandThreads + t;
@@ -343,8 +381,10 @@ band_kernel(DevVolume v, BatchArgs a, UpdateScratch u, unsigned long long* hist,
         const bool has = nhas;
         const int inext = i + gridDim.x * kBandThreads;
         nhas = false;
-        if (inext < a.n) nhas = load_point<kSource>(a, inext, nx, ny, nz);
-        band_point<MODE, RECORDS, S>(v, a, u, i, has, px, py, pz, sm, drops, counted, hist, n_bins);
+        if (inext < a.n) nhas = load_point<SOURCE>(a, inext, nx, ny, nz);
+        cam.at(i);
+        band_point<MODE, RECORDS, S, kProbeWarp, FRAMES>(v, a, u, i, has, px, py, pz, sm, drops, counted,
+                                                         hist, n_bins, cam.cx, cam.cy, cam.cz);
     }
 
     // Counters: one global atomic per CTA (per-warp atomics on one line serialise).
@@ -355,6 +395,32 @@ band_kernel(DevVolume v, BatchArgs a, UpdateScratch u, unsigned long long* hist,
     __syncthreads();
     if (t == 0 && s_drops) atomicAdd(v.drop_count, (unsigned long long)s_drops);
     if (t == 0 && s_counted) atomicAdd(&u.ctl->n_records, (int)s_counted);
+}
+
+template <int MODE, bool RECORDS, int S, bool DEPTH = false>
+__global__ void __launch_bounds__(kBandThreads, kBandMinBlocks)
+band_kernel(DevVolume v, BatchArgs a, UpdateScratch u, unsigned long long* hist, int n_bins) {
+    band_tiles<MODE, RECORDS, S, DEPTH ? 1 : 0, false>(v, a, u, hist, n_bins, OneCamera{});
+}
+
+// Integrate (allocate + count-and-sum) of a batch of several frames: the
+// single-frame walk with each point's camera taken from the frame table.
+template <int S>
+__global__ void __launch_bounds__(kBandThreads, kBandMinBlocks)
+band_frames_kernel(DevVolume v, BatchArgs a, UpdateScratch u, const FrameCam* frames, int32_t n_frames) {
+    band_tiles<kAllocInsert, true, S, 0, true>(v, a, u, nullptr, 0, FrameCursor(frames, n_frames));
+}
+
+// Set-up of a several-frame integrate, in place of the control block's
+// memset: zero the control block and store the frame table where the band
+// walk reads it (one CTA; static indices only, so the table stays in the
+// parameter space).
+__global__ void frames_setup_kernel(UpdateControl* ctl, FrameCam* dst, const FrameTable t) {
+    const int k = threadIdx.x;
+    if (k < (int)(sizeof(UpdateControl) / sizeof(uint32_t))) reinterpret_cast<uint32_t*>(ctl)[k] = 0u;
+#pragma unroll
+    for (int j = 0; j <= kMaxFrames; ++j)
+        if (j == k && j <= t.n) dst[j] = t.f[j];
 }
 
 // ---- batched steps -----------------------------------------------------
@@ -513,6 +579,40 @@ cudaError_t launch_band_records(const DevVolume& v, const BatchArgs& a, const Up
         default:
             return insert ? launch<kAllocInsert, true>(v, a, u, nullptr, 0, sm_count, s)
                           : launch<kLookupOnly, true>(v, a, u, nullptr, 0, sm_count, s);
+    }
+}
+
+namespace {
+template <int S>
+cudaError_t launch_band_frames_t(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
+                                 const FrameCam* frames, int32_t n_frames, int sm_count, cudaStream_t s) {
+    static int per_sm = 0;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, band_frames_kernel<S>, kBandThreads, 0) !=
+                cudaSuccess ||
+            per_sm < 1)
+            per_sm = 1;
+    });
+    const int tiles = (a.n + kBandThreads - 1) / kBandThreads;
+    const int grid = std::min(tiles, per_sm * sm_count);
+    band_frames_kernel<S><<<grid, kBandThreads, 0, s>>>(v, a, u, frames, n_frames);
+    return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t launch_frames_setup(UpdateControl* ctl, FrameCam* d_frames, const FrameTable& t, cudaStream_t s) {
+    frames_setup_kernel<<<1, 64, 0, s>>>(ctl, d_frames, t);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_band_frames(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
+                               const FrameCam* d_frames, int32_t n_frames, int sm_count, cudaStream_t s) {
+    if (a.n <= 0) return cudaSuccess;
+    switch (v.storage) {
+        case kStoreF32: return launch_band_frames_t<kStoreF32>(v, a, u, d_frames, n_frames, sm_count, s);
+        case kStoreF16U16: return launch_band_frames_t<kStoreF16U16>(v, a, u, d_frames, n_frames, sm_count, s);
+        default: return cudaErrorInvalidValue;  // the FP64 oracle integrates one frame per batch
     }
 }
 

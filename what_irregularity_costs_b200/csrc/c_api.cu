@@ -136,6 +136,35 @@ int32_t osn_tsdf_cuda_integrate(OsnTsdfCudaVolume* v, const float* d_positions, 
                : 3;
 }
 
+static_assert(OSN_TSDF_MAX_FRAMES == osn_b200::kMaxFrames, "one frame limit");
+
+int32_t osn_tsdf_cuda_integrate_frames(OsnTsdfCudaVolume* v, const float* d_positions,
+                                       const int32_t* frame_begin, const float* cams_xyz,
+                                       int32_t n_frames, float radius_m) {
+    if (!usable(v) || !d_positions || !frame_begin || !cams_xyz || n_frames < 1 ||
+        n_frames > osn_b200::kMaxFrames || frame_begin[0] != 0)
+        return 1;
+    for (int32_t k = 0; k < n_frames; ++k)
+        if (frame_begin[k + 1] < frame_begin[k]) return 1;
+    const int32_t n = frame_begin[n_frames];
+    if (n <= 0 || !batch_fits(v, n)) return 1;
+    if (v->vol.storage() == osn_b200::kStoreF64) return 2;
+    osn_b200::FrameTable t{};
+    t.n = n_frames;
+    for (int32_t k = 0; k <= n_frames; ++k) {
+        t.f[k].begin = frame_begin[k];
+        if (k < n_frames) {
+            t.f[k].x = cams_xyz[3 * k];
+            t.f[k].y = cams_xyz[3 * k + 1];
+            t.f[k].z = cams_xyz[3 * k + 2];
+        }
+    }
+    // The batch's own camera is not read by the several-frame walk; the
+    // update tail of FP32 / FP16 storage reads no camera.
+    const BatchArgs a = batch(d_positions, n, cams_xyz[0], cams_xyz[1], cams_xyz[2], radius_m);
+    return v->vol.integrate_frames(a, t) == cudaSuccess ? 0 : 3;
+}
+
 int32_t osn_tsdf_cuda_integrate_depth(OsnTsdfCudaVolume* v, const float* d_depth, int32_t width,
                                       int32_t height, double fx, double fy, double cx, double cy,
                                       const double* cam_to_world_R, const double* cam_to_world_t,

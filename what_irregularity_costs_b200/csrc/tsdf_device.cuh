@@ -213,26 +213,36 @@ struct Ray {
     float px, py, pz;
     float ux, uy, uz;
     float dist;
+    float cx, cy, cz;  // the camera origin of the point's frame
 };
 
-// Point set-up for a point already loaded into (px, py, pz). False when the
-// point is gated out by the far cutoff or sits on the camera
-// (volume.cpp:158-166).
-__device__ __forceinline__ bool ray_setup_at(const BatchArgs& a, float px, float py, float pz, Ray& r) {
+// Point set-up for a point already loaded into (px, py, pz), seen from the
+// camera at (cx, cy, cz). False when the point is gated out by the far cutoff
+// or sits on the camera (volume.cpp:158-166).
+__device__ __forceinline__ bool ray_setup_cam(float radius_sq, float cx, float cy, float cz, float px,
+                                              float py, float pz, Ray& r) {
     r.px = px;
     r.py = py;
     r.pz = pz;
-    const float dx = __fsub_rn(r.px, a.cam_x);
-    const float dy = __fsub_rn(r.py, a.cam_y);
-    const float dz = __fsub_rn(r.pz, a.cam_z);
+    r.cx = cx;
+    r.cy = cy;
+    r.cz = cz;
+    const float dx = __fsub_rn(r.px, cx);
+    const float dy = __fsub_rn(r.py, cy);
+    const float dz = __fsub_rn(r.pz, cz);
     const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
-    if (a.radius_sq > 0.0f && d2 > a.radius_sq) return false;
+    if (radius_sq > 0.0f && d2 > radius_sq) return false;
     r.dist = __fsqrt_rn(d2);
     if (!(r.dist > 1e-6f)) return false;
     r.ux = __fdiv_rn(dx, r.dist);
     r.uy = __fdiv_rn(dy, r.dist);
     r.uz = __fdiv_rn(dz, r.dist);
     return true;
+}
+
+// The same for a batch with one camera.
+__device__ __forceinline__ bool ray_setup_at(const BatchArgs& a, float px, float py, float pz, Ray& r) {
+    return ray_setup_cam(a.radius_sq, a.cam_x, a.cam_y, a.cam_z, px, py, pz, r);
 }
 
 __device__ __forceinline__ bool ray_setup(const BatchArgs& a, int i, Ray& r) {
@@ -244,19 +254,31 @@ __device__ __forceinline__ bool ray_setup(const BatchArgs& a, int i, Ray& r) {
 // Band sample s in [-steps, steps]: voxel index and signed distance at the
 // voxel CENTRE. False when the voxel is fully occluded (sdf < -trunc), the
 // gate both passes apply (volume.cpp:185-191, :260-268).
-__device__ __forceinline__ bool band_sample(const DevVolume& v, const BatchArgs& a, const Ray& r,
-                                            int s, int& vx, int& vy, int& vz, float& sdf) {
+__device__ __forceinline__ bool band_sample_from(const DevVolume& v, const Ray& r, float cx, float cy,
+                                                 float cz, int s, int& vx, int& vy, int& vz, float& sdf) {
     const float t = __fmul_rn((float)s, v.voxel_size);
     vx = (int)floorf(__fmul_rn(__fadd_rn(r.px, __fmul_rn(r.ux, t)), v.inv_voxel));
     vy = (int)floorf(__fmul_rn(__fadd_rn(r.py, __fmul_rn(r.uy, t)), v.inv_voxel));
     vz = (int)floorf(__fmul_rn(__fadd_rn(r.pz, __fmul_rn(r.uz, t)), v.inv_voxel));
-    const float ex = __fsub_rn(__fmul_rn(__fadd_rn((float)vx, 0.5f), v.voxel_size), a.cam_x);
-    const float ey = __fsub_rn(__fmul_rn(__fadd_rn((float)vy, 0.5f), v.voxel_size), a.cam_y);
-    const float ez = __fsub_rn(__fmul_rn(__fadd_rn((float)vz, 0.5f), v.voxel_size), a.cam_z);
+    const float ex = __fsub_rn(__fmul_rn(__fadd_rn((float)vx, 0.5f), v.voxel_size), cx);
+    const float ey = __fsub_rn(__fmul_rn(__fadd_rn((float)vy, 0.5f), v.voxel_size), cy);
+    const float ez = __fsub_rn(__fmul_rn(__fadd_rn((float)vz, 0.5f), v.voxel_size), cz);
     const float dv =
         __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(ex, ex), __fmul_rn(ey, ey)), __fmul_rn(ez, ez)));
     sdf = __fsub_rn(r.dist, dv);
     return !(sdf < -v.trunc);
+}
+
+// A batch with one camera (read from the batch's arguments).
+__device__ __forceinline__ bool band_sample(const DevVolume& v, const BatchArgs& a, const Ray& r,
+                                            int s, int& vx, int& vy, int& vz, float& sdf) {
+    return band_sample_from(v, r, a.cam_x, a.cam_y, a.cam_z, s, vx, vy, vz, sdf);
+}
+
+// A batch of several frames: the camera of the point's frame, kept in the ray.
+__device__ __forceinline__ bool band_sample_ray(const DevVolume& v, const Ray& r, int s, int& vx,
+                                                int& vy, int& vz, float& sdf) {
+    return band_sample_from(v, r, r.cx, r.cy, r.cz, s, vx, vy, vz, sdf);
 }
 
 // The FP64 oracle's signed distance of the same band sample: the point's

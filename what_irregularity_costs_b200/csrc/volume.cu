@@ -141,6 +141,7 @@ Volume::~Volume() {
     cudaFree(mesh_posnor_);
     cudaFree(mesh_rgb_);
     cudaFree(mesh_ctl_);
+    cudaFree(d_frames_);
     if (host_small_) cudaFreeHost(host_small_);
     for (auto& p : pending_) {
         cudaEventDestroy(p.start);
@@ -315,7 +316,8 @@ void Volume::join() {
     if (pipelined_ && n_updates_ > 0) cudaStreamWaitEvent(stream_, tail_done_[(n_updates_ - 1) & 1], 0);
 }
 
-cudaError_t Volume::run_update(const BatchArgs& a, const UpdateScratch& scratch, bool insert) {
+cudaError_t Volume::run_update(const BatchArgs& a, const UpdateScratch& scratch, bool insert,
+                               const FrameTable* frames) {
     // Pipelined: this update's scratch set alternates; its walk waits only for
     // the tail two updates back (the last user of that set), its tail for its
     // walk. The walk's saturation filter may read weights the previous tail is
@@ -344,10 +346,13 @@ cudaError_t Volume::run_update(const BatchArgs& a, const UpdateScratch& scratch,
     cudaStream_t tail = pipe ? tail_ : stream_;
     cudaError_t e = cudaSuccess;
     if (pipe) e = cudaStreamWaitEvent(stream_, tail_done_[p], 0);
-    if (e == cudaSuccess) e = cudaMemsetAsync(u.ctl, 0, sizeof(UpdateControl), stream_);
+    if (e == cudaSuccess)
+        e = frames ? launch_frames_setup(u.ctl, d_frames_, *frames, stream_)
+                   : cudaMemsetAsync(u.ctl, 0, sizeof(UpdateControl), stream_);
     if (e != cudaSuccess) return e;
     mark_start(kKBand);
-    e = launch_band_records(dv_, a, u, insert, sm_count_, stream_);
+    e = frames ? launch_band_frames(dv_, a, u, d_frames_, frames->n, sm_count_, stream_)
+               : launch_band_records(dv_, a, u, insert, sm_count_, stream_);
     mark_end(kKBand);
     if (e != cudaSuccess) return e;
     if (pipe) {
@@ -391,6 +396,16 @@ cudaError_t Volume::update(const BatchArgs& a) {
 cudaError_t Volume::integrate(const BatchArgs& a) {
     if (!ensure_records(batch_records(a.n, dv_.steps))) return cudaErrorMemoryAllocation;
     return run_update(a, us_, true);
+}
+
+cudaError_t Volume::integrate_frames(const BatchArgs& a, const FrameTable& t) {
+    if (dv_.storage == kStoreF64) return cudaErrorInvalidValue;  // one frame per oracle batch
+    if (!d_frames_ && cudaMalloc(&d_frames_, sizeof(FrameCam) * (kMaxFrames + 1)) != cudaSuccess) {
+        d_frames_ = nullptr;
+        return cudaErrorMemoryAllocation;
+    }
+    if (!ensure_records(batch_records(a.n, dv_.steps))) return cudaErrorMemoryAllocation;
+    return run_update(a, us_, true, &t);
 }
 
 bool Volume::ensure_mesh(int32_t cap, bool rgb) {

@@ -56,6 +56,19 @@ constexpr int kLaneRecords = 16;
 // pool at 2^23 - 1 blocks (4 G voxels).
 constexpr int32_t kMaxPoolBlocks = (1 << 23) - 1;
 
+// Several consecutive frames integrated as one batch: frame k's points are
+// [f[k].begin, f[k + 1].begin) of the batch, seen from the camera at
+// (f[k].x, f[k].y, f[k].z); f[n].begin is the batch's point count.
+constexpr int kMaxFrames = 32;
+struct FrameCam {
+    int32_t begin;
+    float x, y, z;
+};
+struct FrameTable {
+    int32_t n;
+    FrameCam f[kMaxFrames + 1];
+};
+
 struct UpdateScratch {
     UpdateControl* ctl = nullptr;
     uint32_t* records = nullptr;  // [record_cap] one per band slot
@@ -100,6 +113,10 @@ public:
     cudaError_t update(const BatchArgs& a);
     // allocate + update in one pass over the points (same results).
     cudaError_t integrate(const BatchArgs& a);
+    // integrate() of several consecutive frames as one batch (a.n = all
+    // their points; t gives each frame's first point and camera). FP32 and
+    // FP16 storage.
+    cudaError_t integrate_frames(const BatchArgs& a, const FrameTable& t);
     // update() with its control counters and records in caller-provided
     // device memory instead of the volume's own (grown) buffer.
     cudaError_t update_static_scratch(const BatchArgs& a, void* scratch);
@@ -147,7 +164,8 @@ public:
 
 private:
     bool alloc_device(uint32_t hash_slots);
-    cudaError_t run_update(const BatchArgs& a, const UpdateScratch& u, bool insert);
+    cudaError_t run_update(const BatchArgs& a, const UpdateScratch& u, bool insert,
+                           const FrameTable* frames = nullptr);
     bool ensure_records(int64_t n_records);
     bool ensure_mesh(int32_t cap, bool rgb);
 
@@ -176,6 +194,7 @@ private:
     uint8_t* mesh_rgb_ = nullptr;
     int32_t mesh_cap_ = 0;
     int32_t* mesh_ctl_ = nullptr;  // [0] vertex count, [1] overflow flag
+    FrameCam* d_frames_ = nullptr;  // frame table of the last several-frame integrate
 
     // Pinned host staging for small reads.
     int64_t* host_small_ = nullptr;
@@ -224,6 +243,11 @@ cudaError_t launch_extract(const DevVolume& v, int32_t n_blocks, float min_w, fl
 // -> values -> deferred.
 cudaError_t launch_band_records(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
                                 bool insert, int sm_count, cudaStream_t s);
+// Several-frame integrate: the set-up kernel (control block zeroed, frame
+// table stored) and the band walk with per-frame cameras (FP32 / FP16 storage).
+cudaError_t launch_frames_setup(UpdateControl* ctl, FrameCam* d_frames, const FrameTable& t, cudaStream_t s);
+cudaError_t launch_band_frames(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
+                               const FrameCam* d_frames, int32_t n_frames, int sm_count, cudaStream_t s);
 cudaError_t launch_finish(const DevVolume& v, const UpdateScratch& u, int sm_count, cudaStream_t s);
 cudaError_t launch_group(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
                          cudaStream_t s);

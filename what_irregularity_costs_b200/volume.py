@@ -17,6 +17,7 @@ import numpy as np
 
 from . import _lib
 
+MAX_FRAMES = 32  # OSN_TSDF_MAX_FRAMES: frames per integrate_frames call
 KERNEL_NAMES = ["allocate", "band", "finish", "group", "deferred", "extract", "reset", "values"]
 
 # Voxel storage modes (OSN_TSDF_STORAGE_* in include/osn_tsdf_b200.h).
@@ -140,6 +141,27 @@ class CudaVolume:
 
     def integrate(self, positions, cam: Sequence[float], radius_m: float = 0.0, n=None):
         self._batch(self.lib.osn_tsdf_cuda_integrate, positions, cam, radius_m, n, "integrate")
+
+    def integrate_frames(self, positions, frame_begin, cams, radius_m: float = 0.0):
+        """integrate() of several consecutive frames in one call: frame k is
+        positions[frame_begin[k]:frame_begin[k + 1]] seen from cams[k]
+        (positions: a CUDA (N, 3) float32 tensor of all frames' points back to
+        back; frame_begin: n_frames + 1 offsets from 0 to N; cams: (n_frames, 3)).
+        Same blocks and weights as one integrate() per frame; each voxel's TSDF
+        is rounded once per call instead of once per frame. FP32 and FP16
+        storage; at most MAX_FRAMES frames."""
+        begin = np.ascontiguousarray(np.asarray(frame_begin, dtype=np.int32).reshape(-1))
+        cam = np.ascontiguousarray(np.asarray(cams, dtype=np.float32).reshape(-1, 3))
+        if begin.size != cam.shape[0] + 1:
+            raise ValueError("integrate_frames: frame_begin needs one entry more than cams")
+        if _count(positions, None) < int(begin[-1]):
+            raise ValueError("integrate_frames: frame_begin reaches past the points")
+        self._keep.append(positions)
+        rc = self.lib.osn_tsdf_cuda_integrate_frames(self.h, _addr(positions), begin.ctypes.data,
+                                                     cam.ctypes.data, int(cam.shape[0]), float(radius_m))
+        if rc == 2:
+            raise ValueError("integrate_frames: the FP64 oracle integrates one frame per call")
+        self._check(rc, "integrate_frames")
 
     def integrate_depth(self, depth, K, R, t, max_range_m: float = 0.0):
         """integrate() from a device depth image (H, W) float32, unprojected on
