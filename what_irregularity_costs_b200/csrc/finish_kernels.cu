@@ -528,44 +528,65 @@ __device__ __forceinline__ void group_to_ids(const UpdateScratch& u, uint32_t n_
     }
 }
 
-// One warp per voxel of the large list: up to 8 records per lane ranked by id
-// against all others in registers, a radix select of the keep-th id beyond
-// 256 records. Returns the sum of the accepted values (on every lane).
-__device__ long long warp_select(const uint32_t* ids, const long long* vals, int n, int keep,
-                                 uint32_t* hist, int lane) {
-    long long fix = 0;
-    if (n <= 32 * kRankRegs) {
-        uint32_t id[kRankRegs];
-        long long val[kRankRegs];
-        int rank[kRankRegs];
-        const int rows = (n + 31) / 32;
+// Sum of the accepted values of a group of at most 32 * R records, by one
+// warp: record r * 32 + lane in registers (id and value straight from its
+// band slot), ranked by id against every other record with shuffles; a record
+// is accepted when fewer than keep ids are below its own. Ids are distinct
+// and below 0xFFFFFFFF, so the padding entries never rank below a record.
+template <int S, int R>
+__device__ __forceinline__ long long rank_group(const UpdateScratch& u, uint32_t n_pts, uint32_t n_steps,
+                                                uint32_t base, int n, int keep, int lane) {
+    uint32_t id[R];
+    long long val[R];
+    int rank[R];
 #pragma unroll
-        for (int r = 0; r < kRankRegs; ++r) {
-            const int k = r * 32 + lane;
-            id[r] = 0xFFFFFFFFu;
-            val[r] = 0ll;
-            rank[r] = 0;
-            if (r < rows && k < n) {
-                id[r] = ids[k];
-                val[r] = vals[k];
-            }
+    for (int r = 0; r < R; ++r) {
+        const int k = r * 32 + lane;
+        id[r] = 0xFFFFFFFFu;
+        val[r] = 0ll;
+        rank[r] = 0;
+        if (k < n) group_record<S>(u, n_pts, n_steps, base + (uint32_t)k, id[r], val[r]);
+    }
+#pragma unroll
+    for (int rr = 0; rr < R; ++rr) {
+#pragma unroll 8
+        for (int src = 0; src < 32; ++src) {
+            const uint32_t other = __shfl_sync(0xffffffffu, id[rr], src);
+#pragma unroll
+            for (int r = 0; r < R; ++r) rank[r] += other < id[r] ? 1 : 0;
         }
+    }
+    long long fix = 0ll;
 #pragma unroll
-        for (int rr = 0; rr < kRankRegs; ++rr) {
-            if (rr >= rows) break;
-            const int m = min(32, n - rr * 32);
-            for (int src = 0; src < m; ++src) {
-                const uint32_t other = __shfl_sync(0xffffffffu, id[rr], src);
-#pragma unroll
-                for (int r = 0; r < kRankRegs; ++r)
-                    if (r < rows) rank[r] += other < id[r] ? 1 : 0;
-            }
-        }
-#pragma unroll
-        for (int r = 0; r < kRankRegs; ++r)
-            if (r < rows && r * 32 + lane < n && rank[r] < keep) fix += val[r];
+    for (int r = 0; r < R; ++r)
+        if (r * 32 + lane < n && rank[r] < keep) fix += val[r];
+    return fix;
+}
+
+// Sum of the accepted values of a voxel of the large list (e = voxel, group
+// base, records, accepted), by one warp, on every lane: register ranking
+// sized to the group up to 256 records; beyond, the group's records become
+// (id, value) arrays in place and a radix select finds the keep-th id.
+template <int S>
+__device__ long long large_group_sum(const UpdateScratch& u, uint32_t n_pts, uint32_t n_steps, const int4 e,
+                                     uint32_t* hist, int lane) {
+    const uint32_t base = (uint32_t)e.y;
+    const int n = e.z, keep = e.w;
+    long long fix;
+    if (n <= 32) {
+        fix = rank_group<S, 1>(u, n_pts, n_steps, base, n, keep, lane);
+    } else if (n <= 64) {
+        fix = rank_group<S, 2>(u, n_pts, n_steps, base, n, keep, lane);
+    } else if (n <= 128) {
+        fix = rank_group<S, 4>(u, n_pts, n_steps, base, n, keep, lane);
+    } else if (n <= 32 * kRankRegs) {
+        fix = rank_group<S, kRankRegs>(u, n_pts, n_steps, base, n, keep, lane);
     } else {
+        group_to_ids<S>(u, n_pts, n_steps, base, n, lane);
+        const uint32_t* ids = u.deferred + base;
+        const long long* vals = u.deferred_fix + base;
         const uint32_t last = radix_select(ids, n, keep, hist, lane);
+        fix = 0ll;
         for (int k = lane; k < n; k += 32)
             if (ids[k] <= last) fix += vals[k];
     }
@@ -593,9 +614,7 @@ deferred_kernel(DevVolume v, BatchArgs a, UpdateScratch u) {
     const int gw = blockIdx.x * kDeferWarps + warp, nw = gridDim.x * kDeferWarps;
     for (int d = gw; d < n_large; d += nw) {
         const int4 e = u.dvox[u.dvox_cap - 1 - d];  // (voxel, group base, records, accepted)
-        group_to_ids<S>(u, (uint32_t)a.n, n_steps, (uint32_t)e.y, e.z, lane);
-        const long long fix = warp_select(u.deferred + (uint32_t)e.y, u.deferred_fix + (uint32_t)e.y,
-                                          e.z, e.w, hist[warp], lane);
+        const long long fix = large_group_sum<S>(u, (uint32_t)a.n, n_steps, e, hist[warp], lane);
         if (lane == 0) {
             finish_voxel<S>(v, u, (uint32_t)e.x, e.w, fix);
             ++updated;
@@ -858,10 +877,8 @@ deferred_multi_kernel(StepWork w) {
         const int local = item - s_begin[sc];
         int done = 0;
         if (local < n_large) {
-                const int4 e = u.dvox[u.dvox_cap - 1 - local];
-            group_to_ids<S>(u, (uint32_t)sw.a.n, n_steps, (uint32_t)e.y, e.z, lane);
-            const long long fix = warp_select(u.deferred + (uint32_t)e.y, u.deferred_fix + (uint32_t)e.y,
-                                              e.z, e.w, hist[warp], lane);
+            const int4 e = u.dvox[u.dvox_cap - 1 - local];
+            const long long fix = large_group_sum<S>(u, (uint32_t)sw.a.n, n_steps, e, hist[warp], lane);
             if (lane == 0) finish_voxel<S>(v, u, (uint32_t)e.x, e.w, fix);
             done = 1;
         } else {
