@@ -3,13 +3,19 @@
 Workload (one step): reset the volume, then integrate every frame of the
 seeded 100-frame room trajectory (640x480, fx=fy=320, 2 cm voxels, trunc
 8 cm, 2^20 table slots, pool 2^19 blocks, weight cap 64), i.e. allocate +
-update per frame through the C ABI. frames/s = frames integrated / time.
+update of every frame through the C ABI. frames/s = frames integrated / time.
 
   value  device-resident points (uploaded once), CUDA events on the volume's
-         stream around exactly K steps, max over ranks;
-  e2e    the same steps from pinned HOST buffers: every frame's points are
+         stream around exactly K steps, max over ranks; the frames go through
+         osn_tsdf_cuda_integrate_frames, 3 consecutive frames per call
+         (--frames-per-call), with pipelined updates. value_per_frame: one
+         osn_tsdf_cuda_integrate call per frame, pipelined; value_serial:
+         one call per frame, serial;
+  e2e    the headline arm from pinned HOST buffers: every call's points are
          copied host->device inside the timed region (double-buffered on a
-         copy stream) and the block and drop counters are read back per step;
+         copy stream) and the block and drop counters are read back per step
+         (e2e_per_frame: the same with one integrate call per frame;
+         e2e_depth: per-frame depth images unprojected on the GPU);
   roofline  per-kernel CUDA-event times of one instrumented step; the
          dominant kernel's algorithmic bytes per launch / its mean duration
          against the measured HBM copy bandwidth;
@@ -44,6 +50,7 @@ VOXEL, TRUNC, CAP = 0.02, 0.08, 64.0
 SLOTS_PER_POINT = 2 * 4 + 1   # band samples per point: 2 * ceil(trunc / voxel) + 1
 HASH_SLOTS, POOL = 1 << 20, 1 << 19
 N_FRAMES, SEED = 100, 0
+FRAMES_PER_CALL = 3  # frames per osn_tsdf_cuda_integrate_frames call in the headline arm
 METRIC = "frames/s (640x480 integrate)"
 PROFILES = os.path.join(ROOT, "profiles")
 
@@ -340,24 +347,45 @@ def run_ours(args):
             vol.integrate(d_all[a:b], cams[k])
         vol.join()  # the last tails are part of the step
 
-    def timed_device(steps):
+    # Several frames per call: consecutive frames of the trajectory in groups.
+    fpc = max(1, min(args.frames_per_call, N_FRAMES))
+    groups = []
+    for lo in range(0, N_FRAMES, fpc):
+        hi = min(N_FRAMES, lo + fpc)
+        begin = np.asarray(offsets[lo:hi + 1] - offsets[lo], dtype=np.int32)
+        groups.append((lo, hi, int(offsets[lo]), int(offsets[hi]), begin,
+                       np.ascontiguousarray(np.asarray(cams[lo:hi], dtype=np.float32))))
+
+    def step_frames():
+        vol.reset()
+        for lo, hi, a, b, begin, gcams in groups:
+            vol.integrate_frames(d_all[a:b], begin, gcams)
+        vol.join()
+
+    def timed(step, steps):
+        """W warm-up steps, then K steps between CUDA events on the volume's
+        stream, barriers on both sides; the max over ranks (ms)."""
         for _ in range(args.warmup):
-            step_device()
+            step()
         barrier(dist, torch)
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ev0.record(vstream)
         for _ in range(steps):
-            step_device()
+            step()
         ev1.record(vstream)
         barrier(dist, torch)
         return max_over_ranks(ev0.elapsed_time(ev1), dist, torch)
 
-    # -- value_serial: one update after the other (the reference's stream order)
-    serial_ms = timed_device(args.steps)
-    # -- value: pipelined updates (each call's tail overlaps the next walk)
+    # -- value_serial: one call per frame, one update after the other (the
+    # reference's stream order)
+    serial_ms = timed(step_device, args.steps)
+    # -- value_per_frame: one call per frame, pipelined updates (each call's
+    # tail overlaps the next walk)
     vol.set_pipelined(True)
+    per_frame_ms = timed(step_device, args.steps)
+    # -- value: FRAMES_PER_CALL frames per integrate_frames call, pipelined
     with ClockSampler(local) as clocks:
-        ms = timed_device(args.steps)
+        ms = timed(step_frames, args.steps)
     blocks = vol.block_count()
     drops = vol.drop_count()
     status = vol.status()
@@ -365,7 +393,7 @@ def run_ours(args):
     value = frames_total / (ms / 1e3)
 
     # -- e2e: pinned host buffers, copies inside the timed region ------------
-    max_n = int(np.max(np.diff(offsets)))
+    max_n = max(int(np.max(np.diff(offsets))), max(b - a for _, _, a, b, _, _ in groups))
     stage = [torch.empty((max_n, 3), dtype=torch.float32, device="cuda") for _ in range(2)]
     cstream = torch.cuda.Stream()
     copied = [torch.cuda.Event() for _ in range(2)]
@@ -387,18 +415,27 @@ def run_ours(args):
         result[0] = vol.block_count()
         result[1] = vol.drop_count()
 
+    def step_e2e_frames():
+        vol.reset()
+        for g, (lo, hi, a, b, begin, gcams) in enumerate(groups):
+            s = g & 1
+            with torch.cuda.stream(cstream):
+                cstream.wait_event(free[s])
+                stage[s][: b - a].copy_(host_pinned[a:b], non_blocking=True)
+                copied[s].record(cstream)
+            vstream.wait_event(copied[s])
+            vol.integrate_frames(stage[s][: b - a], begin, gcams)
+            free[s].record(vstream)
+        result[0] = vol.block_count()
+        result[1] = vol.drop_count()
+
     for s in range(2):
         free[s].record(vstream)
-    for _ in range(args.warmup):
-        step_e2e()
-    barrier(dist, torch)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(vstream)
-    for _ in range(args.steps):
-        step_e2e()
-    e1.record(vstream)
-    barrier(dist, torch)
-    e2e_ms = max_over_ranks(e0.elapsed_time(e1), dist, torch)
+    # e2e_per_frame: one integrate call per frame
+    e2e_pf_ms = timed(step_e2e, args.steps)
+    e2e_per_frame = frames_total / (e2e_pf_ms / 1e3)
+    # e2e: the headline arm (FRAMES_PER_CALL frames per call)
+    e2e_ms = timed(step_e2e_frames, args.steps)
     e2e_value = frames_total / (e2e_ms / 1e3)
 
     # -- e2e from depth images: 4 B per pixel uploaded, unprojected on the GPU
@@ -423,16 +460,7 @@ def run_ours(args):
         result[0] = vol.block_count()
         result[1] = vol.drop_count()
 
-    for _ in range(args.warmup):
-        step_e2e_depth()
-    barrier(dist, torch)
-    d0, d1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    d0.record(vstream)
-    for _ in range(args.steps):
-        step_e2e_depth()
-    d1.record(vstream)
-    barrier(dist, torch)
-    e2e_depth_ms = max_over_ranks(d0.elapsed_time(d1), dist, torch)
+    e2e_depth_ms = timed(step_e2e_depth, args.steps)
     blocks_depth = vol.block_count()
 
     # -- one instrumented step: per-kernel CUDA-event times (every launch of
@@ -466,7 +494,9 @@ def run_ours(args):
         touched.append(st["touched_blocks"])
         crossing.append(st["crossing_voxels"])
     integrate_kernels = ("band", "finish", "group", "values", "deferred")
-    launches_per_step = sum(per_kernel[k][1] for k in integrate_kernels) + 2  # + reset's two
+    # Launches of the headline arm: per integrate_frames call the set-up
+    # kernel and the four passes; reset's two per step.
+    launches_per_step = 5 * len(groups) + 2
     dominant = max(integrate_kernels, key=lambda k: per_kernel[k][0])
 
     peak, peak_kind = measured_peak()
@@ -519,8 +549,12 @@ def run_ours(args):
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world,
+            "value_per_frame": frames_total / (per_frame_ms / 1e3),
             "value_serial": frames_total / (serial_ms / 1e3),
-            "mode": "pipelined updates (osn_tsdf_cuda_set_pipelined); value_serial: serial",
+            "mode": f"osn_tsdf_cuda_integrate_frames, {fpc} frames per call, pipelined updates; "
+                    "value_per_frame: one osn_tsdf_cuda_integrate per frame, pipelined; "
+                    "value_serial: one per frame, serial",
+            "frames_per_call": fpc,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic: seeded room trajectory (3 spheres, 2 boxes), depth noise "
@@ -530,7 +564,11 @@ def run_ours(args):
             "cpu_baseline": cpu,
             "reference_gpu_arm": a3,
             "e2e": {"value": e2e_value, "unit": "frames/s",
-                    "h2d_bytes_per_step": int(all_pts.nbytes), "d2h_bytes_per_step": 16},
+                    "h2d_bytes_per_step": int(all_pts.nbytes), "d2h_bytes_per_step": 16,
+                    "path": f"osn_tsdf_cuda_integrate_frames ({fpc} frames per call) from pinned host buffers"},
+            "e2e_per_frame": {"value": e2e_per_frame, "unit": "frames/s",
+                              "h2d_bytes_per_step": int(all_pts.nbytes), "d2h_bytes_per_step": 16,
+                              "path": "osn_tsdf_cuda_integrate per frame from pinned host buffers"},
             "e2e_depth": {"value": frames_total / (e2e_depth_ms / 1e3), "unit": "frames/s",
                           "h2d_bytes_per_step": dbytes, "d2h_bytes_per_step": 16,
                           "path": "osn_tsdf_cuda_integrate_depth (unprojection in the band walk)",
@@ -936,6 +974,8 @@ def main():
     ap.add_argument("--frames", type=int, default=N_FRAMES,
                     help="frames of the trajectory per step (fewer: a small profiling case)")
     ap.add_argument("--pool", type=int, default=POOL, help="pool capacity in blocks")
+    ap.add_argument("--frames-per-call", type=int, default=FRAMES_PER_CALL,
+                    help="frames per integrate_frames call in the headline arm")
     ap.add_argument("--workload", choices=["room", "batch32", "serve64", "sweep"], default="room",
                     help="room: the single-scene trajectory (default); batch32: the 32-scene "
                          "batched mix; serve64: the 64-session serving loop; sweep: voxel size x "
