@@ -5,7 +5,7 @@
  * cpp/include/osn_tsdf/c_api.h (lines 223-293), re-declared with identical
  * names, argument meanings and return codes, so a caller of the reference's
  * CUDA arm (A3) links against this library instead without a source change.
- * The CPU section of that header (c_api.h:181-213) is the reference's own CPU
+ * The CPU section of that header (c_api.h:14-46) is the reference's own CPU
  * arm and is not part of this library.
  *
  * Conventions (same as the reference):
@@ -30,7 +30,7 @@ extern "C" {
 typedef struct OsnTsdfCudaVolume OsnTsdfCudaVolume;
 
 /* Device pointers and parameters describing a volume's storage.
- * Same 104-byte layout as the reference (c_api.h:228-245, size asserted at
+ * Same 104-byte layout as the reference (c_api.h:61-78, size asserted at
  * cpp/src/c_api_cuda.cu:14): table slots are (int64 key, int32 block_idx,
  * int32 pad); tsdf/weight/r/g/b hold weighted SUMS, 512 floats per block at
  * block_idx * 512, voxel (lx,ly,lz) at (lz*8+ly)*8+lx. */
@@ -53,56 +53,56 @@ typedef struct {
     float weight_cap;
 } OsnTsdfDeviceView;
 
-/* ---- reference CUDA section (cpp/include/osn_tsdf/c_api.h:247-293) ---- */
+/* ---- reference CUDA section (cpp/include/osn_tsdf/c_api.h:80-126) ---- */
 
-/* c_api.h:247. NULL on invalid parameters or device allocation failure.
+/* c_api.h:80. NULL on invalid parameters or device allocation failure.
  * trunc_m <= 0 selects 4 * voxel_size_m; weight_cap <= 0 disables capping.
  * The table has next_pow2(2 * pool) slots, as in the reference. */
 OsnTsdfCudaVolume* osn_tsdf_cuda_create(float voxel_size_m, int32_t pool_capacity_blocks,
                                         float trunc_m, float weight_cap);
-/* c_api.h:249 */
+/* c_api.h:82 */
 void osn_tsdf_cuda_destroy(OsnTsdfCudaVolume* v);
-/* c_api.h:250. 1 when every device allocation succeeded. */
+/* c_api.h:83. 1 when every device allocation succeeded. */
 int32_t osn_tsdf_cuda_valid(const OsnTsdfCudaVolume* v);
-/* c_api.h:253. Returns 0 on success, 1 on a NULL or invalid volume. */
+/* c_api.h:86. Returns 0 on success, 1 on a NULL or invalid volume. */
 int32_t osn_tsdf_cuda_device_view(const OsnTsdfCudaVolume* v, OsnTsdfDeviceView* out);
 
-/* c_api.h:256-258. Allocate the blocks the batch's truncation bands touch.
+/* c_api.h:89-91. Allocate the blocks the batch's truncation bands touch.
  * Returns 0 (queued), 1 on bad arguments (NULL volume or positions, n <= 0),
  * 3 when the kernel launch failed. */
 int32_t osn_tsdf_cuda_allocate_blocks(OsnTsdfCudaVolume* v, const float* d_positions,
                                       int32_t n_points, float cam_x, float cam_y, float cam_z,
                                       float radius_m);
-/* c_api.h:259-261. Accumulate the batch into allocated blocks: unit weights,
+/* c_api.h:92-94. Accumulate the batch into allocated blocks: unit weights,
  * grey colour (128), contributions applied as if in (point, band step) order
  * with the weight cap "accept while weight before < cap". Return codes as
  * allocate_blocks. */
 int32_t osn_tsdf_cuda_update_voxels(OsnTsdfCudaVolume* v, const float* d_positions,
                                     int32_t n_points, float cam_x, float cam_y, float cam_z,
                                     float radius_m);
-/* c_api.h:264-265. Marching-tetrahedra triangle soup into HOST buffers:
+/* c_api.h:97-98. Marching-tetrahedra triangle soup into HOST buffers:
  * buffer_posnor holds vert_cap * 6 floats (position, face normal),
  * buffer_rgb vert_cap * 3 bytes or NULL. Returns the vertex count, or -1 if
  * vert_cap was too small or the arguments are invalid. */
 int32_t osn_tsdf_cuda_extract_mesh(OsnTsdfCudaVolume* v, float* buffer_posnor, uint8_t* buffer_rgb,
                                    int32_t vert_cap, float min_weight, float iso);
-/* c_api.h:273. Back to the just-created state without reallocating. Waits. */
+/* c_api.h:106. Back to the just-created state without reallocating. Waits. */
 int32_t osn_tsdf_cuda_reset(OsnTsdfCudaVolume* v);
-/* c_api.h:277-279. MEASUREMENT: allocate, adding every compare-exchange
+/* c_api.h:110-112. MEASUREMENT: allocate, adding every compare-exchange
  * ATTEMPT to drop_count. Only meaningful on a pool that drops nothing. */
 int32_t osn_tsdf_cuda_allocate_counting_cas(OsnTsdfCudaVolume* v, const float* d_positions,
                                             int32_t n_points, float cam_x, float cam_y,
                                             float cam_z, float radius_m);
-/* c_api.h:282-284. MEASUREMENT: probe and read, never insert. */
+/* c_api.h:115-117. MEASUREMENT: probe and read, never insert. */
 int32_t osn_tsdf_cuda_allocate_no_cas(OsnTsdfCudaVolume* v, const float* d_positions,
                                       int32_t n_points, float cam_x, float cam_y, float cam_z,
                                       float radius_m);
-/* c_api.h:287-289. MEASUREMENT: block index = hash slot, hash masked to the
+/* c_api.h:120-122. MEASUREMENT: block index = hash slot, hash masked to the
  * pool (which must be a power of two; 2 otherwise); no publication wait. */
 int32_t osn_tsdf_cuda_allocate_slot_index(OsnTsdfCudaVolume* v, const float* d_positions,
                                           int32_t n_points, float cam_x, float cam_y, float cam_z,
                                           float radius_m);
-/* c_api.h:291-293. Waiting reads of the counters; 0 for a NULL volume. */
+/* c_api.h:124-126. Waiting reads of the counters; 0 for a NULL volume. */
 int32_t osn_tsdf_cuda_block_count(const OsnTsdfCudaVolume* v);
 uint64_t osn_tsdf_cuda_drop_count(const OsnTsdfCudaVolume* v);
 void osn_tsdf_cuda_synchronize(const OsnTsdfCudaVolume* v);

@@ -10,7 +10,7 @@ from what_irregularity_costs_b200 import _lib
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
-# The reference's CUDA section, cpp/include/osn_tsdf/c_api.h:247-293.
+# The reference's CUDA section, cpp/include/osn_tsdf/c_api.h:80-126.
 REFERENCE_CUDA_ENTRY_POINTS = [
     "osn_tsdf_cuda_create", "osn_tsdf_cuda_destroy", "osn_tsdf_cuda_valid",
     "osn_tsdf_cuda_device_view", "osn_tsdf_cuda_allocate_blocks", "osn_tsdf_cuda_update_voxels",

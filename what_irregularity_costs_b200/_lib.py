@@ -16,7 +16,7 @@ HEADER = os.path.join(ROOT, "include", "osn_tsdf_b200.h")
 
 
 class OsnTsdfDeviceView(C.Structure):
-    """Mirror of OsnTsdfDeviceView (104 bytes, cpp/include/osn_tsdf/c_api.h:228-245)."""
+    """Mirror of OsnTsdfDeviceView (104 bytes, cpp/include/osn_tsdf/c_api.h:61-78)."""
 
     _fields_ = [
         ("table", C.c_void_p),

@@ -320,7 +320,7 @@ __device__ __forceinline__ int32_t find_block(const DevVolume& v, int32_t bx, in
 // ---- insertion (volume.cpp:94-145, volume_cuda.cu:59-107) -------------------
 
 // Allocation modes: the production insert and the reference's measurement
-// variants (cpp/include/osn_tsdf/c_api.h:275-289), plus a probe histogram.
+// variants (cpp/include/osn_tsdf/c_api.h:108-122), plus a probe histogram.
 enum AllocMode : int {
     kAllocInsert = 0,       // production
     kAllocCountingCas = 1,  // measurement: count CAS attempts into drop_count

@@ -2,7 +2,7 @@
 
 ``CudaVolume`` wraps one ``OsnTsdfCudaVolume`` of libosn_tsdf_b200.so. Its
 methods keep the reference's names and argument meanings
-(cpp/include/osn_tsdf/c_api.h:247-293, cpp/include/osn_tsdf/volume_cuda.hpp:24-86):
+(cpp/include/osn_tsdf/c_api.h:80-126, cpp/include/osn_tsdf/volume_cuda.hpp:24-86):
 positions are device-resident float32 ``(n, 3)`` world points (a CUDA torch
 tensor or a raw device address), ``cam`` is the camera origin, ``radius_m``
 the far cutoff (<= 0 disables). Bad arguments raise ``ValueError`` where the
