@@ -463,6 +463,34 @@ def run_ours(args):
     e2e_depth_ms = timed(step_e2e_depth, args.steps)
     blocks_depth = vol.block_count()
 
+    # -- the same with several depth images per call (integrate_depth_frames)
+    depth_all = torch.from_numpy(np.stack([d for d, _, _ in _DEPTH])).pin_memory()
+    dfpc = max(1, min(fpc, 16))
+    dgroups = []
+    for lo in range(0, N_FRAMES, dfpc):
+        hi = min(N_FRAMES, lo + dfpc)
+        dgroups.append((lo, hi, np.stack([_DEPTH[k][1] for k in range(lo, hi)]),
+                        np.stack([_DEPTH[k][2] for k in range(lo, hi)])))
+    dfstage = [torch.empty((dfpc,) + tuple(depth_all.shape[1:]), dtype=torch.float32, device="cuda")
+               for _ in range(2)]
+
+    def step_e2e_depth_frames():
+        vol.reset()
+        for g, (lo, hi, Rs_, ts_) in enumerate(dgroups):
+            s_ = g & 1
+            with torch.cuda.stream(cstream):
+                cstream.wait_event(free[s_])
+                dfstage[s_][: hi - lo].copy_(depth_all[lo:hi], non_blocking=True)
+                copied[s_].record(cstream)
+            vstream.wait_event(copied[s_])
+            vol.integrate_depth_frames(dfstage[s_][: hi - lo], K, Rs_, ts_)
+            free[s_].record(vstream)
+        result[0] = vol.block_count()
+        result[1] = vol.drop_count()
+
+    e2e_depth_frames_ms = timed(step_e2e_depth_frames, args.steps)
+    blocks_depth_frames = vol.block_count()
+
     # -- one instrumented step: per-kernel CUDA-event times (every launch of
     # the volume bracketed on its stream; no synchronisation between frames;
     # serial mode, so kernels do not overlap)
@@ -573,6 +601,10 @@ def run_ours(args):
                           "h2d_bytes_per_step": dbytes, "d2h_bytes_per_step": 16,
                           "path": "osn_tsdf_cuda_integrate_depth (unprojection in the band walk)",
                           "blocks": blocks_depth},
+            "e2e_depth_frames": {"value": frames_total / (e2e_depth_frames_ms / 1e3), "unit": "frames/s",
+                                 "h2d_bytes_per_step": dbytes, "d2h_bytes_per_step": 16,
+                                 "path": f"osn_tsdf_cuda_integrate_depth_frames ({dfpc} images per call)",
+                                 "blocks": blocks_depth_frames},
             "gpu_launches": int(launches_per_step * args.steps),
             "clocks": clocks.summary(),
             "alloc_mrays_per_s": n_points / t_alloc / 1e6 if t_alloc else None,

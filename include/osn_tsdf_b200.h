@@ -179,6 +179,22 @@ int32_t osn_tsdf_cuda_integrate_depth(OsnTsdfCudaVolume* v, const float* d_depth
                                       const double* cam_to_world_R, const double* cam_to_world_t,
                                       float max_range_m);
 
+/* integrate_depth of several depth images of the same size in one call (no
+ * counterpart in the reference): image k occupies d_depth[k * height * width
+ * .. (k + 1) * height * width) and is seen from the camera-to-world pose
+ * cam_to_world_R[9k .. 9k + 8] (row-major), cam_to_world_t[3k .. 3k + 2]
+ * (HOST arrays, read during the call); one set of intrinsics. Results as
+ * integrate_frames of the images' backprojected points: the same blocks,
+ * weights and colour sums as one integrate_depth call per image, each
+ * voxel's TSDF rounded once per call. At most OSN_TSDF_MAX_DEPTH_FRAMES
+ * images; FP32 and FP16 storage (2 for the FP64 oracle); other return codes
+ * as integrate. */
+#define OSN_TSDF_MAX_DEPTH_FRAMES 16
+int32_t osn_tsdf_cuda_integrate_depth_frames(OsnTsdfCudaVolume* v, const float* d_depth, int32_t width,
+                                             int32_t height, int32_t n_frames, double fx, double fy,
+                                             double cx, double cy, const double* cam_to_world_R,
+                                             const double* cam_to_world_t, float max_range_m);
+
 /* Extraction into DEVICE buffers (same layout as extract_mesh), skipping the
  * host copy. Returns the vertex count or -1 (overflow / bad arguments).
  * Waits for the count only. */

@@ -8,16 +8,17 @@ and to the CPU oracle fed frame by frame. A voxel's stored TSDF sum takes one
 rounding per call instead of one per frame, so mean TSDFs are held to the
 float parity bar (1e-5) against both. Covered: caps 64 / 6 (crossing inside
 a batch) / none, uneven and empty frames, one frame per call (bit-identical
-to integrate), pipelined calls, FP16 storage against the FP64 oracle, and the
-argument checks.
+to integrate), pipelined calls, FP16 storage against the FP64 oracle, depth
+images (osn_tsdf_cuda_integrate_depth_frames: bit-identical to integrate_frames
+of the host-backprojected points), and the argument checks.
 """
 import numpy as np
 import pytest
 
 import oracle
 from helpers import assert_same_blocks, assert_same_voxels, sorted_voxels
-from what_irregularity_costs_b200 import (MAX_FRAMES, STORAGE_FP16_U16, STORAGE_FP32, STORAGE_FP64,
-                                          CudaVolume, precision, scenes)
+from what_irregularity_costs_b200 import (MAX_DEPTH_FRAMES, MAX_FRAMES, STORAGE_FP16_U16, STORAGE_FP32,
+                                          STORAGE_FP64, CudaVolume, precision, scenes)
 
 pytestmark = pytest.mark.gpu
 
@@ -150,3 +151,50 @@ def test_frames_argument_checks(cuda):
         o.integrate_frames(d_all, begin, cams)
     assert v.block_count() == 0 and v.status() == 0
     assert v.storage == STORAGE_FP32
+
+
+@pytest.mark.parametrize("res,cap,max_range", [((640, 480), 64.0, 0.0), ((320, 240), 6.0, 3.0)])
+def test_depth_frames_equal_point_frames_and_per_image_calls(cuda, res, cap, max_range):
+    scene = scenes.RoomScene.make(2)
+    K = scenes.ROOM_K.scaled(*res)
+    frames = [scenes.room_frame(scene, k, K) for k in range(4)]
+    depth = cuda.from_numpy(np.stack([f.depth for f in frames])).cuda()
+    Rs = np.stack([f.R for f in frames])
+    ts = np.stack([f.t for f in frames])
+    pts = [scenes.frame_points(f, max_range) for f in frames]
+    begin = [0] + [int(x) for x in np.cumsum([p.shape[0] for p in pts])]
+    cams = np.array([f.cam for f in frames], dtype=np.float32)
+    dep = CudaVolume(0.02, 1 << 17, 0.08, cap, 1 << 18)
+    pts_vol = CudaVolume(0.02, 1 << 17, 0.08, cap, 1 << 18)
+    per_image = CudaVolume(0.02, 1 << 17, 0.08, cap, 1 << 18)
+    dep.integrate_depth_frames(depth, K, Rs, ts, max_range)
+    pts_vol.integrate_frames(cuda.from_numpy(np.concatenate(pts)).cuda(), begin, cams)
+    for k, f in enumerate(frames):
+        per_image.integrate_depth(depth[k], K, f.R, f.t, max_range)
+    assert dep.status() == 0 and dep.block_count() > 0
+    _bits_equal(dep, pts_vol)
+    assert dep.drop_count() == pts_vol.drop_count()
+    assert_same_voxels(dep, per_image)
+    if cap == 6.0:
+        assert dep.last_update_stats()["crossing_voxels"] > 0
+
+
+def test_depth_frames_argument_checks(cuda):
+    frames = _frames(2, (160, 120))
+    depth = cuda.from_numpy(np.stack([f.depth for f in frames])).cuda()
+    Rs = np.stack([f.R for f in frames])
+    ts = np.stack([f.t for f in frames])
+    K = scenes.ROOM_K.scaled(160, 120)
+    v = CudaVolume(0.02, 1 << 12, 0.08, 64.0)
+    with pytest.raises(ValueError):
+        v.integrate_depth_frames(depth, K, Rs[:1], ts[:1])       # one pose short
+    with pytest.raises(ValueError):
+        v.integrate_depth_frames(depth[0], K, Rs[:1], ts[:1])    # not (F, H, W)
+    n = MAX_DEPTH_FRAMES + 1
+    many = depth[:1].expand(n, -1, -1).contiguous()
+    with pytest.raises(ValueError):
+        v.integrate_depth_frames(many, K, np.repeat(Rs[:1], n, 0), np.repeat(ts[:1], n, 0))
+    o = CudaVolume(0.02, 1 << 12, 0.08, 64.0, storage=STORAGE_FP64)
+    with pytest.raises(ValueError):
+        o.integrate_depth_frames(depth, K, Rs, ts)
+    assert v.block_count() == 0 and v.status() == 0

@@ -53,6 +53,8 @@ _SIG = {
     "osn_tsdf_cuda_update_voxels": (_I, [_P, _P, _I, _F, _F, _F, _F]),
     "osn_tsdf_cuda_integrate": (_I, [_P, _P, _I, _F, _F, _F, _F]),
     "osn_tsdf_cuda_integrate_frames": (_I, [_P, _P, _P, _P, _I, _F]),
+    "osn_tsdf_cuda_integrate_depth_frames": (_I, [_P, _P, _I, _I, _I, C.c_double, C.c_double, C.c_double,
+                                                  C.c_double, _P, _P, _F]),
     "osn_tsdf_cuda_integrate_depth": (_I, [_P, _P, _I, _I, C.c_double, C.c_double, C.c_double,
                                            C.c_double, _P, _P, _F]),
     "osn_tsdf_cuda_extract_mesh": (_I, [_P, _P, _P, _I, _F, _F]),

@@ -349,11 +349,33 @@ struct FrameCursor {
     }
 };
 
+// Where a batch's points come from: xyz positions or one depth image.
+template <int SOURCE>
+struct BatchPoints {
+    const BatchArgs& a;
+    __device__ __forceinline__ bool load(int i, float& px, float& py, float& pz) const {
+        return load_point<SOURCE>(a, i, px, py, pz);
+    }
+};
+
+// Several depth images of npix pixels back to back: pixel i belongs to image
+// i / npix, unprojected with that image's pose (staged in shared memory).
+struct DepthFramesPoints {
+    const BatchArgs& a;
+    const FramePose* pose;
+    int32_t npix;
+    __device__ __forceinline__ bool load(int i, float& px, float& py, float& pz) const {
+        const int f = i / npix;
+        return unproject_pixel(a.depth, pose[f].R, pose[f].t, i, i - f * npix, px, py, pz);
+    }
+};
+
 // A persistent CTA's share of a batch: tiles of 128 points, strided by the
 // grid, then the CTA's drop and record counts.
-template <int MODE, bool RECORDS, int S, int SOURCE, bool FRAMES, typename Camera>
+template <int MODE, bool RECORDS, int S, bool FRAMES, typename Points, typename Camera>
 __device__ __forceinline__ void band_tiles(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
-                                           unsigned long long* hist, int n_bins, Camera cam) {
+                                           unsigned long long* hist, int n_bins, const Points pts,
+                                           Camera cam) {
     __shared__ BandSmem sm;
     const int t = threadIdx.x;
     const int lane = t & 31;
@@ -373,7 +395,7 @@ __device__ __forceinline__ void band_tiles(const DevVolume& v, const BatchArgs& 
     bool nhas = false;
     {
         const int i0 = blockIdx.x * kBandThreads + t;
-        if (blockIdx.x < n_tiles && i0 < a.n) nhas = load_point<SOURCE>(a, i0, nx, ny, nz);
+        if (blockIdx.x < n_tiles && i0 < a.n) nhas = pts.load(i0, nx, ny, nz);
     }
     for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
         const int i = tile * kBandThreads + t;
@@ -381,7 +403,7 @@ __device__ __forceinline__ void band_tiles(const DevVolume& v, const BatchArgs& 
         const bool has = nhas;
         const int inext = i + gridDim.x * kBandThreads;
         nhas = false;
-        if (inext < a.n) nhas = load_point<SOURCE>(a, inext, nx, ny, nz);
+        if (inext < a.n) nhas = pts.load(inext, nx, ny, nz);
         cam.at(i);
         band_point<MODE, RECORDS, S, kProbeWarp, FRAMES>(v, a, u, i, has, px, py, pz, sm, drops, counted,
                                                          hist, n_bins, cam.cx, cam.cy, cam.cz);
@@ -400,7 +422,7 @@ __device__ __forceinline__ void band_tiles(const DevVolume& v, const BatchArgs& 
 template <int MODE, bool RECORDS, int S, bool DEPTH = false>
 __global__ void __launch_bounds__(kBandThreads, kBandMinBlocks)
 band_kernel(DevVolume v, BatchArgs a, UpdateScratch u, unsigned long long* hist, int n_bins) {
-    band_tiles<MODE, RECORDS, S, DEPTH ? 1 : 0, false>(v, a, u, hist, n_bins, OneCamera{});
+    band_tiles<MODE, RECORDS, S, false>(v, a, u, hist, n_bins, BatchPoints<DEPTH ? 1 : 0>{a}, OneCamera{});
 }
 
 // Integrate (allocate + count-and-sum) of a batch of several frames: the
@@ -408,7 +430,22 @@ band_kernel(DevVolume v, BatchArgs a, UpdateScratch u, unsigned long long* hist,
 template <int S>
 __global__ void __launch_bounds__(kBandThreads, kBandMinBlocks)
 band_frames_kernel(DevVolume v, BatchArgs a, UpdateScratch u, const FrameCam* frames, int32_t n_frames) {
-    band_tiles<kAllocInsert, true, S, 0, true>(v, a, u, nullptr, 0, FrameCursor(frames, n_frames));
+    band_tiles<kAllocInsert, true, S, true>(v, a, u, nullptr, 0, BatchPoints<0>{a}, FrameCursor(frames, n_frames));
+}
+
+// The same for several depth images of equal size: each CTA stages the
+// images' poses in shared memory first.
+template <int S>
+__global__ void __launch_bounds__(kBandThreads, kBandMinBlocks)
+band_depth_frames_kernel(DevVolume v, BatchArgs a, UpdateScratch u, const FrameCam* frames,
+                         const FramePose* poses, int32_t n_frames) {
+    __shared__ FramePose s_pose[kMaxDepthFrames];
+    constexpr int kWords = (int)(sizeof(FramePose) / sizeof(double));
+    for (int k = threadIdx.x; k < n_frames * kWords; k += blockDim.x)
+        reinterpret_cast<double*>(s_pose)[k] = __ldg(reinterpret_cast<const double*>(poses) + k);
+    __syncthreads();
+    band_tiles<kAllocInsert, true, S, true>(v, a, u, nullptr, 0, DepthFramesPoints{a, s_pose, a.n / n_frames},
+                                            FrameCursor(frames, n_frames));
 }
 
 // Set-up of a several-frame integrate, in place of the control block's
@@ -421,6 +458,19 @@ __global__ void frames_setup_kernel(UpdateControl* ctl, FrameCam* dst, const Fra
 #pragma unroll
     for (int j = 0; j <= kMaxFrames; ++j)
         if (j == k && j <= t.n) dst[j] = t.f[j];
+}
+
+// The same for several depth images, with their poses.
+__global__ void frames_setup_depth_kernel(UpdateControl* ctl, FrameCam* dst, const FrameTable t,
+                                          FramePose* pdst, const PoseTable p) {
+    const int k = threadIdx.x;
+    if (k < (int)(sizeof(UpdateControl) / sizeof(uint32_t))) reinterpret_cast<uint32_t*>(ctl)[k] = 0u;
+#pragma unroll
+    for (int j = 0; j <= kMaxFrames; ++j)
+        if (j == k && j <= t.n) dst[j] = t.f[j];
+#pragma unroll
+    for (int j = 0; j < kMaxDepthFrames; ++j)
+        if (j == k && j < p.n) pdst[j] = p.p[j];
 }
 
 // ---- batched steps -----------------------------------------------------
@@ -599,11 +649,47 @@ cudaError_t launch_band_frames_t(const DevVolume& v, const BatchArgs& a, const U
     band_frames_kernel<S><<<grid, kBandThreads, 0, s>>>(v, a, u, frames, n_frames);
     return cudaGetLastError();
 }
+template <int S>
+cudaError_t launch_band_depth_frames_t(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
+                                       const FrameCam* frames, const FramePose* poses, int32_t n_frames,
+                                       int sm_count, cudaStream_t s) {
+    static int per_sm = 0;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, band_depth_frames_kernel<S>, kBandThreads,
+                                                          0) != cudaSuccess ||
+            per_sm < 1)
+            per_sm = 1;
+    });
+    const int tiles = (a.n + kBandThreads - 1) / kBandThreads;
+    const int grid = std::min(tiles, per_sm * sm_count);
+    band_depth_frames_kernel<S><<<grid, kBandThreads, 0, s>>>(v, a, u, frames, poses, n_frames);
+    return cudaGetLastError();
+}
 }  // namespace
 
 cudaError_t launch_frames_setup(UpdateControl* ctl, FrameCam* d_frames, const FrameTable& t, cudaStream_t s) {
     frames_setup_kernel<<<1, 64, 0, s>>>(ctl, d_frames, t);
     return cudaGetLastError();
+}
+
+cudaError_t launch_frames_setup_depth(UpdateControl* ctl, FrameCam* d_frames, const FrameTable& t,
+                                      FramePose* d_poses, const PoseTable& p, cudaStream_t s) {
+    frames_setup_depth_kernel<<<1, 64, 0, s>>>(ctl, d_frames, t, d_poses, p);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_band_depth_frames(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
+                                     const FrameCam* d_frames, const FramePose* d_poses, int32_t n_frames,
+                                     int sm_count, cudaStream_t s) {
+    if (a.n <= 0 || n_frames < 1 || n_frames > kMaxDepthFrames || a.n % n_frames != 0)
+        return cudaErrorInvalidValue;
+    switch (v.storage) {
+        case kStoreF32: return launch_band_depth_frames_t<kStoreF32>(v, a, u, d_frames, d_poses, n_frames, sm_count, s);
+        case kStoreF16U16:
+            return launch_band_depth_frames_t<kStoreF16U16>(v, a, u, d_frames, d_poses, n_frames, sm_count, s);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 cudaError_t launch_band_frames(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,

@@ -190,6 +190,48 @@ int32_t osn_tsdf_cuda_integrate_depth(OsnTsdfCudaVolume* v, const float* d_depth
     return v->vol.integrate(a) == cudaSuccess ? 0 : 3;
 }
 
+static_assert(OSN_TSDF_MAX_DEPTH_FRAMES == osn_b200::kMaxDepthFrames, "one depth frame limit");
+
+int32_t osn_tsdf_cuda_integrate_depth_frames(OsnTsdfCudaVolume* v, const float* d_depth, int32_t width,
+                                             int32_t height, int32_t n_frames, double fx, double fy,
+                                             double cx, double cy, const double* cam_to_world_R,
+                                             const double* cam_to_world_t, float max_range_m) {
+    if (!usable(v) || !d_depth || width <= 0 || height <= 0 || n_frames < 1 ||
+        n_frames > osn_b200::kMaxDepthFrames || !cam_to_world_R || !cam_to_world_t || !(fx != 0.0) ||
+        !(fy != 0.0))
+        return 1;
+    const int64_t npix = (int64_t)width * height;
+    const int64_t n = npix * n_frames;
+    if (n > INT32_MAX || !batch_fits(v, (int32_t)n)) return 1;
+    if (v->vol.storage() == osn_b200::kStoreF64) return 2;
+    osn_b200::FrameTable t{};
+    osn_b200::PoseTable p{};
+    t.n = n_frames;
+    p.n = n_frames;
+    for (int32_t k = 0; k <= n_frames; ++k) {
+        t.f[k].begin = (int32_t)(npix * k);
+        if (k == n_frames) break;
+        // The camera origin of the walk is the pose translation as float, as
+        // for a single depth image.
+        t.f[k].x = (float)cam_to_world_t[3 * k];
+        t.f[k].y = (float)cam_to_world_t[3 * k + 1];
+        t.f[k].z = (float)cam_to_world_t[3 * k + 2];
+        for (int j = 0; j < 9; ++j) p.p[k].R[j] = cam_to_world_R[9 * k + j];
+        for (int j = 0; j < 3; ++j) p.p[k].t[j] = cam_to_world_t[3 * k + j];
+    }
+    BatchArgs a = batch(nullptr, (int32_t)n, t.f[0].x, t.f[0].y, t.f[0].z, 0.0f);
+    a.depth.depth = d_depth;
+    a.depth.width = width;
+    a.depth.max_range = max_range_m;
+    a.depth.fx = fx;
+    a.depth.fy = fy;
+    a.depth.cx = cx;
+    a.depth.cy = cy;
+    for (int j = 0; j < 9; ++j) a.depth.R[j] = cam_to_world_R[j];
+    for (int j = 0; j < 3; ++j) a.depth.t[j] = cam_to_world_t[j];
+    return v->vol.integrate_frames(a, t, &p) == cudaSuccess ? 0 : 3;
+}
+
 int32_t osn_tsdf_cuda_extract_mesh(OsnTsdfCudaVolume* v, float* buffer_posnor, uint8_t* buffer_rgb,
                                    int32_t vert_cap, float min_weight, float iso) {
     if (!usable(v) || !buffer_posnor || vert_cap <= 0) return -1;

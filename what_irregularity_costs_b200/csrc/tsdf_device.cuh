@@ -145,6 +145,30 @@ struct BatchArgs {
     DepthSource depth;
 };
 
+// Pixel p of a depth image (depth value at index i of the batch's depth
+// array) unprojected with the camera-to-world pose (R, t) in FP64, rounded to
+// float; false for an invalid pixel (non-finite, <= 0 or beyond max_range).
+__device__ __forceinline__ bool unproject_pixel(const DepthSource& d, const double* R, const double* t,
+                                                int i, int p, float& px, float& py, float& pz) {
+    const float z = d.depth[i];
+    px = py = pz = 0.0f;
+    if (!isfinite(z) || !(z > 0.0f) || (d.max_range > 0.0f && z > d.max_range)) return false;
+    const int v = p / d.width, u = p - v * d.width;
+    const double zd = (double)z;
+    const double x = __ddiv_rn(__dmul_rn(__dsub_rn((double)u, d.cx), zd), d.fx);
+    const double y = __ddiv_rn(__dmul_rn(__dsub_rn((double)v, d.cy), zd), d.fy);
+    float w[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+        w[k] = __double2float_rn(__dadd_rn(
+            __dadd_rn(__dadd_rn(__dmul_rn(R[3 * k], x), __dmul_rn(R[3 * k + 1], y)), __dmul_rn(R[3 * k + 2], zd)),
+            t[k]));
+    px = w[0];
+    py = w[1];
+    pz = w[2];
+    return true;
+}
+
 // Point i of a batch; false when it has none (an invalid depth pixel).
 // SOURCE: 0 = xyz positions, 1 = depth image, -1 = whichever the batch has.
 template <int SOURCE = -1>
@@ -155,25 +179,7 @@ __device__ __forceinline__ bool load_point(const BatchArgs& a, int i, float& px,
         pz = a.pos[(size_t)i * 3 + 2];
         return true;
     }
-    const DepthSource& d = a.depth;
-    const float z = d.depth[i];
-    px = py = pz = 0.0f;
-    if (!isfinite(z) || !(z > 0.0f) || (d.max_range > 0.0f && z > d.max_range)) return false;
-    const int v = i / d.width, u = i - v * d.width;
-    const double zd = (double)z;
-    const double x = __ddiv_rn(__dmul_rn(__dsub_rn((double)u, d.cx), zd), d.fx);
-    const double y = __ddiv_rn(__dmul_rn(__dsub_rn((double)v, d.cy), zd), d.fy);
-    float w[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k)
-        w[k] = __double2float_rn(__dadd_rn(
-            __dadd_rn(__dadd_rn(__dmul_rn(d.R[3 * k], x), __dmul_rn(d.R[3 * k + 1], y)),
-                      __dmul_rn(d.R[3 * k + 2], zd)),
-            d.t[k]));
-    px = w[0];
-    py = w[1];
-    pz = w[2];
-    return true;
+    return unproject_pixel(a.depth, a.depth.R, a.depth.t, i, i, px, py, pz);
 }
 
 __device__ __forceinline__ long long pack_key(int32_t x, int32_t y, int32_t z) {

@@ -142,6 +142,7 @@ Volume::~Volume() {
     cudaFree(mesh_rgb_);
     cudaFree(mesh_ctl_);
     cudaFree(d_frames_);
+    cudaFree(d_poses_);
     if (host_small_) cudaFreeHost(host_small_);
     for (auto& p : pending_) {
         cudaEventDestroy(p.start);
@@ -317,7 +318,7 @@ void Volume::join() {
 }
 
 cudaError_t Volume::run_update(const BatchArgs& a, const UpdateScratch& scratch, bool insert,
-                               const FrameTable* frames) {
+                               const FrameTable* frames, const PoseTable* poses) {
     // Pipelined: this update's scratch set alternates; its walk waits only for
     // the tail two updates back (the last user of that set), its tail for its
     // walk. The walk's saturation filter may read weights the previous tail is
@@ -347,12 +348,14 @@ cudaError_t Volume::run_update(const BatchArgs& a, const UpdateScratch& scratch,
     cudaError_t e = cudaSuccess;
     if (pipe) e = cudaStreamWaitEvent(stream_, tail_done_[p], 0);
     if (e == cudaSuccess)
-        e = frames ? launch_frames_setup(u.ctl, d_frames_, *frames, stream_)
-                   : cudaMemsetAsync(u.ctl, 0, sizeof(UpdateControl), stream_);
+        e = poses    ? launch_frames_setup_depth(u.ctl, d_frames_, *frames, d_poses_, *poses, stream_)
+            : frames ? launch_frames_setup(u.ctl, d_frames_, *frames, stream_)
+                     : cudaMemsetAsync(u.ctl, 0, sizeof(UpdateControl), stream_);
     if (e != cudaSuccess) return e;
     mark_start(kKBand);
-    e = frames ? launch_band_frames(dv_, a, u, d_frames_, frames->n, sm_count_, stream_)
-               : launch_band_records(dv_, a, u, insert, sm_count_, stream_);
+    e = poses    ? launch_band_depth_frames(dv_, a, u, d_frames_, d_poses_, frames->n, sm_count_, stream_)
+        : frames ? launch_band_frames(dv_, a, u, d_frames_, frames->n, sm_count_, stream_)
+                 : launch_band_records(dv_, a, u, insert, sm_count_, stream_);
     mark_end(kKBand);
     if (e != cudaSuccess) return e;
     if (pipe) {
@@ -398,14 +401,19 @@ cudaError_t Volume::integrate(const BatchArgs& a) {
     return run_update(a, us_, true);
 }
 
-cudaError_t Volume::integrate_frames(const BatchArgs& a, const FrameTable& t) {
+cudaError_t Volume::integrate_frames(const BatchArgs& a, const FrameTable& t, const PoseTable* poses) {
     if (dv_.storage == kStoreF64) return cudaErrorInvalidValue;  // one frame per oracle batch
+    if ((poses != nullptr) != (a.depth.depth != nullptr)) return cudaErrorInvalidValue;
     if (!d_frames_ && cudaMalloc(&d_frames_, sizeof(FrameCam) * (kMaxFrames + 1)) != cudaSuccess) {
         d_frames_ = nullptr;
         return cudaErrorMemoryAllocation;
     }
+    if (poses && !d_poses_ && cudaMalloc(&d_poses_, sizeof(FramePose) * kMaxDepthFrames) != cudaSuccess) {
+        d_poses_ = nullptr;
+        return cudaErrorMemoryAllocation;
+    }
     if (!ensure_records(batch_records(a.n, dv_.steps))) return cudaErrorMemoryAllocation;
-    return run_update(a, us_, true, &t);
+    return run_update(a, us_, true, &t, poses);
 }
 
 bool Volume::ensure_mesh(int32_t cap, bool rgb) {

@@ -68,6 +68,17 @@ struct FrameTable {
     int32_t n;
     FrameCam f[kMaxFrames + 1];
 };
+// Several depth images as one batch: image k's camera-to-world pose (the
+// unprojection of its pixels; the walk's camera is (float)t).
+constexpr int kMaxDepthFrames = 16;
+struct FramePose {
+    double R[9];  // row-major
+    double t[3];
+};
+struct PoseTable {
+    int32_t n;
+    FramePose p[kMaxDepthFrames];
+};
 
 struct UpdateScratch {
     UpdateControl* ctl = nullptr;
@@ -116,7 +127,7 @@ public:
     // integrate() of several consecutive frames as one batch (a.n = all
     // their points; t gives each frame's first point and camera). FP32 and
     // FP16 storage.
-    cudaError_t integrate_frames(const BatchArgs& a, const FrameTable& t);
+    cudaError_t integrate_frames(const BatchArgs& a, const FrameTable& t, const PoseTable* poses = nullptr);
     // update() with its control counters and records in caller-provided
     // device memory instead of the volume's own (grown) buffer.
     cudaError_t update_static_scratch(const BatchArgs& a, void* scratch);
@@ -165,7 +176,7 @@ public:
 private:
     bool alloc_device(uint32_t hash_slots);
     cudaError_t run_update(const BatchArgs& a, const UpdateScratch& u, bool insert,
-                           const FrameTable* frames = nullptr);
+                           const FrameTable* frames = nullptr, const PoseTable* poses = nullptr);
     bool ensure_records(int64_t n_records);
     bool ensure_mesh(int32_t cap, bool rgb);
 
@@ -195,6 +206,7 @@ private:
     int32_t mesh_cap_ = 0;
     int32_t* mesh_ctl_ = nullptr;  // [0] vertex count, [1] overflow flag
     FrameCam* d_frames_ = nullptr;  // frame table of the last several-frame integrate
+    FramePose* d_poses_ = nullptr;  // poses of the last several-image depth integrate
 
     // Pinned host staging for small reads.
     int64_t* host_small_ = nullptr;
@@ -248,6 +260,13 @@ cudaError_t launch_band_records(const DevVolume& v, const BatchArgs& a, const Up
 cudaError_t launch_frames_setup(UpdateControl* ctl, FrameCam* d_frames, const FrameTable& t, cudaStream_t s);
 cudaError_t launch_band_frames(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
                                const FrameCam* d_frames, int32_t n_frames, int sm_count, cudaStream_t s);
+// The same for depth images (a.depth set): poses stored by the set-up, the
+// walk unprojecting image i / (width * height) with its pose.
+cudaError_t launch_frames_setup_depth(UpdateControl* ctl, FrameCam* d_frames, const FrameTable& t,
+                                      FramePose* d_poses, const PoseTable& p, cudaStream_t s);
+cudaError_t launch_band_depth_frames(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
+                                     const FrameCam* d_frames, const FramePose* d_poses, int32_t n_frames,
+                                     int sm_count, cudaStream_t s);
 cudaError_t launch_finish(const DevVolume& v, const UpdateScratch& u, int sm_count, cudaStream_t s);
 cudaError_t launch_group(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
                          cudaStream_t s);

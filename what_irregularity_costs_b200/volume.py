@@ -18,6 +18,7 @@ import numpy as np
 from . import _lib
 
 MAX_FRAMES = 32  # OSN_TSDF_MAX_FRAMES: frames per integrate_frames call
+MAX_DEPTH_FRAMES = 16  # OSN_TSDF_MAX_DEPTH_FRAMES: images per integrate_depth_frames call
 KERNEL_NAMES = ["allocate", "band", "finish", "group", "deferred", "extract", "reset", "values"]
 
 # Voxel storage modes (OSN_TSDF_STORAGE_* in include/osn_tsdf_b200.h).
@@ -162,6 +163,30 @@ class CudaVolume:
         if rc == 2:
             raise ValueError("integrate_frames: the FP64 oracle integrates one frame per call")
         self._check(rc, "integrate_frames")
+
+    def integrate_depth_frames(self, depth, K, Rs, ts, max_range_m: float = 0.0):
+        """integrate_depth() of several images in one call: depth is a
+        contiguous (F, H, W) float32 CUDA tensor, Rs (F, 3, 3) and ts (F, 3)
+        the images' camera-to-world poses. Same blocks and weights as one
+        integrate_depth() per image; each voxel's TSDF is rounded once per
+        call. FP32 and FP16 storage; at most MAX_DEPTH_FRAMES images."""
+        if not (hasattr(depth, "is_cuda") and depth.is_cuda and depth.dim() == 3 and depth.is_contiguous()):
+            raise ValueError("depth must be a contiguous (F, H, W) CUDA tensor")
+        import torch
+        if depth.dtype != torch.float32:
+            raise ValueError("depth must be float32")
+        f = int(depth.shape[0])
+        Rh = np.ascontiguousarray(np.asarray(Rs, dtype=np.float64).reshape(-1))
+        th = np.ascontiguousarray(np.asarray(ts, dtype=np.float64).reshape(-1))
+        if Rh.size != 9 * f or th.size != 3 * f:
+            raise ValueError("integrate_depth_frames: one pose per image")
+        self._keep.append(depth)
+        rc = self.lib.osn_tsdf_cuda_integrate_depth_frames(
+            self.h, _addr(depth), int(depth.shape[2]), int(depth.shape[1]), f, float(K.fx), float(K.fy),
+            float(K.cx), float(K.cy), Rh.ctypes.data, th.ctypes.data, float(max_range_m))
+        if rc == 2:
+            raise ValueError("integrate_depth_frames: the FP64 oracle integrates one image per call")
+        self._check(rc, "integrate_depth_frames")
 
     def integrate_depth(self, depth, K, R, t, max_range_m: float = 0.0):
         """integrate() from a device depth image (H, W) float32, unprojected on
