@@ -542,8 +542,10 @@ def run_ours(args):
     t_update = sum(per_kernel[k][0] for k in integrate_kernels) / 1e3
     n_slots = n_points * SLOTS_PER_POINT
     n_rec, n_touch = int(np.sum(records)), int(np.sum(touched))
-    # Bytes each kernel must move, every structure touched once (the
-    # definitions are in DESIGN.md, roofline section).
+    # Bytes each kernel must move, every structure touched once. Band walk:
+    # 12 B per point read, a 4-byte record per band slot written, and per
+    # counted sample a 4-byte count and an 8-byte fixed-point sum reduced
+    # (16 B with the read of the voxel's weight).
     alg_total = {
         "band": 12 * n_points + 4 * n_slots + 16 * n_rec,
         "finish": n_touch * 512 * (16 + 36),   # read cnt,w,t,sum; write t,w,r,g,b,cnt,sum
