@@ -512,6 +512,13 @@ def run_ours(args):
     for k in range(N_FRAMES):
         a, b = int(offsets[k]), int(offsets[k + 1])
         vol.integrate(d_all[a:b], cams[k])
+    # Extraction of the trajectory's volume into a device buffer (the
+    # marching-tetrahedra kernel alone is timed).
+    ext_cap = 1 << 24
+    ext_buf = torch.empty((ext_cap, 6), dtype=torch.float32, device="cuda")
+    ext_blocks = vol.block_count()
+    ext_verts = vol.extract_mesh_device(ext_buf, None, ext_cap, 0.5, 0.0)
+    del ext_buf
     # Allocation alone (allocate_blocks), for the allocate Mrays/s figure.
     vol.reset()
     for k in range(N_FRAMES):
@@ -554,8 +561,14 @@ def run_ours(args):
         "deferred": 0,
     }
     # Update as the reference scopes it: positions + tsdf/weight tiles of the
-    # touched blocks, read and written.
+    # touched blocks, read and written; the stricter figure counts only the
+    # voxels that were updated.
     update_alg_bytes = 12 * n_points + n_touch * 512 * 2 * 8
+    update_alg_bytes_voxels = 12 * n_points + int(np.sum(updated)) * 2 * 8
+    # Extraction: each allocated block's 512 voxels and 217 halo voxels read
+    # (tsdf and weight, 8 bytes), 24 bytes written per vertex.
+    t_extract = per_kernel["extract"][0] / 1e3
+    extract_alg_bytes = ext_blocks * (512 + 217) * 8 + 24 * max(ext_verts, 0)
     dom_ms, dom_n = per_kernel[dominant]
     dom_alg = alg_total.get(dominant, 0) / N_FRAMES
     achieved = dom_alg / (dom_ms / 1e3 / dom_n) / 1e9 if dom_n else 0.0
@@ -621,6 +634,12 @@ def run_ours(args):
             "clocks": clocks.summary(),
             "alloc_mrays_per_s": n_points / t_alloc / 1e6 if t_alloc else None,
             "update_gbps": update_alg_bytes / t_update / 1e9 if t_update else None,
+            "update_gbps_updated_voxels": update_alg_bytes_voxels / t_update / 1e9 if t_update else None,
+            "extract": {"blocks": ext_blocks, "vertices": ext_verts,
+                        "ms": round(1e3 * t_extract, 4) if t_extract else None,
+                        "gbps": extract_alg_bytes / t_extract / 1e9 if t_extract else None,
+                        "frac": extract_alg_bytes / t_extract / 1e9 / peak if t_extract else None,
+                        "alg_bytes": extract_alg_bytes},
             "kernel_ms_per_step": {k: round(v[0], 4) for k, v in per_kernel.items()},
             "kernel_launches_per_step": {k: v[1] for k, v in per_kernel.items()},
             "blocks": blocks, "drops": int(drops), "status": status,

@@ -201,6 +201,16 @@ int32_t osn_tsdf_cuda_integrate_depth_frames(OsnTsdfCudaVolume* v, const float* 
 int32_t osn_tsdf_cuda_extract_mesh_device(OsnTsdfCudaVolume* v, float* d_posnor, uint8_t* d_rgb,
                                           int32_t vert_cap, float min_weight, float iso);
 
+/* Extract the mesh and write it as a raw "OSN1" file (the reference's geometry
+ * dump, cpp/bench/bench_arms.cu:506-523; no counterpart in its C ABI):
+ * uint32 magic 0x314e534f (the bytes "OSN1"), uint32 vertex count, then the
+ * vertices' interleaved position and normal floats (6 per vertex) exactly as
+ * extraction produced them, little-endian. Returns the vertex count, -1 on bad
+ * arguments or when vert_cap is too small (nothing written), -2 on a file
+ * error. Waits. */
+int32_t osn_tsdf_cuda_write_mesh_osn1(OsnTsdfCudaVolume* v, const char* path, int32_t vert_cap,
+                                      float min_weight, float iso);
+
 /* Snapshot and restore through host memory (checkpoint a volume, or move an
  * idle session out of HBM and back). A snapshot holds the allocated blocks'
  * coordinates and voxel arrays (pool order) and the drop counter; the table

@@ -58,6 +58,7 @@ _SIG = {
     "osn_tsdf_cuda_integrate_depth": (_I, [_P, _P, _I, _I, C.c_double, C.c_double, C.c_double,
                                            C.c_double, _P, _P, _F]),
     "osn_tsdf_cuda_extract_mesh": (_I, [_P, _P, _P, _I, _F, _F]),
+    "osn_tsdf_cuda_write_mesh_osn1": (_I, [_P, C.c_char_p, _I, _F, _F]),
     "osn_tsdf_cuda_extract_mesh_device": (_I, [_P, _P, _P, _I, _F, _F]),
     "osn_tsdf_cuda_reset": (_I, [_P]),
     "osn_tsdf_cuda_allocate_counting_cas": (_I, [_P, _P, _I, _F, _F, _F, _F]),

@@ -2,7 +2,9 @@
 // (implemented there by cpp/src/c_api_cuda.cu) plus this library's
 // extensions, declared in include/osn_tsdf_b200.h.
 #include <climits>
+#include <cstdio>
 #include <cstring>
+#include <memory>
 
 #include "../../include/osn_tsdf_b200.h"
 #include "volume.h"
@@ -236,6 +238,23 @@ int32_t osn_tsdf_cuda_extract_mesh(OsnTsdfCudaVolume* v, float* buffer_posnor, u
                                    int32_t vert_cap, float min_weight, float iso) {
     if (!usable(v) || !buffer_posnor || vert_cap <= 0) return -1;
     return v->vol.extract(buffer_posnor, buffer_rgb, vert_cap, min_weight, iso, true);
+}
+
+int32_t osn_tsdf_cuda_write_mesh_osn1(OsnTsdfCudaVolume* v, const char* path, int32_t vert_cap,
+                                      float min_weight, float iso) {
+    if (!usable(v) || !path || vert_cap <= 0) return -1;
+    std::unique_ptr<float[]> posnor(new (std::nothrow) float[(size_t)vert_cap * 6]);
+    if (!posnor) return -1;
+    const int32_t n = v->vol.extract(posnor.get(), nullptr, vert_cap, min_weight, iso, true);
+    if (n < 0) return -1;
+    std::FILE* f = std::fopen(path, "wb");
+    if (!f) return -2;
+    const uint32_t magic = 0x314e534fu;  // the bytes "OSN1" in little-endian order
+    const uint32_t nv = (uint32_t)n;
+    bool ok = std::fwrite(&magic, 4, 1, f) == 1 && std::fwrite(&nv, 4, 1, f) == 1;
+    if (ok && n > 0) ok = std::fwrite(posnor.get(), sizeof(float), (size_t)n * 6, f) == (size_t)n * 6;
+    ok = std::fclose(f) == 0 && ok;
+    return ok ? n : -2;
 }
 
 int32_t osn_tsdf_cuda_extract_mesh_device(OsnTsdfCudaVolume* v, float* d_posnor, uint8_t* d_rgb,

@@ -11,6 +11,7 @@ C ABI returns 1; a failed launch raises ``RuntimeError`` (return code 3).
 from __future__ import annotations
 
 import ctypes as C
+import os
 from typing import Sequence
 
 import numpy as np
@@ -205,6 +206,18 @@ class CudaVolume:
             self.h, _addr(depth), int(depth.shape[1]), int(depth.shape[0]), float(K.fx), float(K.fy),
             float(K.cx), float(K.cy), Rh.ctypes.data, th.ctypes.data, float(max_range_m))
         self._check(rc, "integrate_depth")
+
+    def write_mesh_osn1(self, path: str, vert_cap: int = 1 << 22, min_weight: float = 0.5,
+                        iso: float = 0.0) -> int:
+        """Extract the mesh and write it as an OSN1 file (meshio); returns the
+        vertex count."""
+        n = self.lib.osn_tsdf_cuda_write_mesh_osn1(self.h, os.fsencode(path), int(vert_cap),
+                                                   float(min_weight), float(iso))
+        if n == -1:
+            raise ValueError("write_mesh_osn1: bad arguments or vert_cap too small")
+        if n < 0:
+            raise OSError(f"write_mesh_osn1: cannot write {path}")
+        return int(n)
 
     def snapshot(self) -> np.ndarray:
         """The volume's allocated blocks and voxels as a host byte array."""
