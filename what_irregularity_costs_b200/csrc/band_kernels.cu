@@ -35,6 +35,12 @@
 // Samples whose voxel already holds the cap's weight are left out: under
 // "accept while weight before < cap" they cannot be accepted in any order,
 // so leaving them out changes no result.
+//
+// Several frames per call (band_frames_kernel, band_depth_frames_kernel): the
+// same walk, each point seen from the camera of its frame (a per-call table
+// the set-up kernel stores; depth images also carry their poses). The points
+// of frame k precede those of frame k+1, so the canonical (point, step) order
+// is (frame, point, step) order and the cap keeps what per-frame calls keep.
 #include <algorithm>
 #include <climits>
 #include <mutex>
