@@ -188,6 +188,22 @@ def max_over_ranks(x, dist, torch):
     return float(t.item())
 
 
+def frame_groups(offsets, cams, frames_per_call):
+    """Consecutive frames in groups of frames_per_call (the last may be
+    shorter): (first frame, end frame, first point, end point, frame_begin
+    relative to the group's first point (int32, one entry per frame plus
+    one), cameras (float32, one row per frame)) per integrate_frames call."""
+    offsets = np.asarray(offsets, dtype=np.int64)
+    n = len(offsets) - 1
+    out = []
+    for lo in range(0, n, frames_per_call):
+        hi = min(n, lo + frames_per_call)
+        begin = np.asarray(offsets[lo:hi + 1] - offsets[lo], dtype=np.int32)
+        out.append((lo, hi, int(offsets[lo]), int(offsets[hi]), begin,
+                    np.ascontiguousarray(np.asarray(cams[lo:hi], dtype=np.float32))))
+    return out
+
+
 def replica_work(frames_per_rank, world):
     """Frames the whole job integrates: every rank runs its own replica."""
     return frames_per_rank * world
@@ -353,12 +369,7 @@ def run_ours(args):
 
     # Several frames per call: consecutive frames of the trajectory in groups.
     fpc = max(1, min(args.frames_per_call, N_FRAMES))
-    groups = []
-    for lo in range(0, N_FRAMES, fpc):
-        hi = min(N_FRAMES, lo + fpc)
-        begin = np.asarray(offsets[lo:hi + 1] - offsets[lo], dtype=np.int32)
-        groups.append((lo, hi, int(offsets[lo]), int(offsets[hi]), begin,
-                       np.ascontiguousarray(np.asarray(cams[lo:hi], dtype=np.float32))))
+    groups = frame_groups(offsets, cams, fpc)
 
     def step_frames():
         vol.reset()
