@@ -212,29 +212,82 @@ def replica_work(frames_per_rank, world):
 # ---------------------------------------------------------------------------
 
 
-def cpu_reference_rate(pts, cams, budget_s=15.0, threads=None):
+def sorted_fp32_voxels(coords, tsdf, weight, r, g, b):
+    """The five FP32 voxel arrays with blocks in coordinate order."""
+    order = np.lexsort(coords.T[::-1]) if coords.shape[0] else np.zeros(0, dtype=np.int64)
+    return coords[order], tsdf[order], weight[order], r[order], g[order], b[order]
+
+
+def parity_vs_oracle(gpu_arrays, pts, cams, path):
+    """The headline run's volume against the CPU oracle fed the same frames one
+    at a time (outside every timed region): block set, weights and colour sums
+    exact, mean TSDF within the float parity bar of 1e-5."""
+    import oracle
+    t0 = time.perf_counter()
+    ref = oracle.OracleVolume(VOXEL, POOL, TRUNC, CAP, HASH_SLOTS)
+    for p, c in zip(pts, cams):
+        ref.integrate(p, c)
+    rc, rt, rw, rr, rg, rb = sorted_fp32_voxels(*ref.voxels())
+    gc, gt, gw, gr, gg, gb = gpu_arrays
+    out = {"path": path, "frames": len(pts), "oracle": "oracle/tsdf_oracle.c (single-threaded)",
+           "tol_mean_tsdf": 1e-5, "oracle_s": None}
+    out["blocks"] = "exact" if gc.shape == rc.shape and np.array_equal(gc, rc) else "differ"
+    if out["blocks"] != "exact":
+        out.update(weights=None, colour=None, max_mean_tsdf_err=None, ok=False)
+        return out
+    out["weights"] = "exact" if np.array_equal(gw, rw) else f"{int(np.sum(gw != rw))} differ"
+    out["colour"] = "exact" if all(np.array_equal(x, y) for x, y in ((gr, rr), (gg, rg), (gb, rb))) \
+        else "differ"
+    seen = rw > 0
+    err = float(np.max(np.abs(gt[seen] / gw[seen] - rt[seen] / rw[seen]))) if seen.any() else 0.0
+    out["max_mean_tsdf_err"] = err
+    out["blocks_n"] = int(gc.shape[0])
+    out["ok"] = out["weights"] == "exact" and out["colour"] == "exact" and err <= 1e-5
+    out["oracle_s"] = round(time.perf_counter() - t0, 1)
+    return out
+
+
+def l2_ceilings(lib, bytes_=32 << 20):
+    """Measured L2 ceilings of this GPU (osn_tsdf_cuda_l2_probe on a 32 MiB,
+    L2-resident buffer): reductions and atomics in G ops/s, streamed loads in
+    GB/s, random 4-byte loads in G loads/s."""
+    import ctypes as C
+    out = {"buffer_bytes": bytes_}
+    for kind, name, iters in ((0, "red_u64_gops", 256), (1, "red_u32_gops", 256), (2, "atom_u32_gops", 128),
+                              (3, "load16_gbps", 512), (4, "load4_random_gloads", 256)):
+        r = C.c_double(0.0)
+        rc = lib.osn_tsdf_cuda_l2_probe(kind, bytes_, iters, C.addressof(r))
+        out[name] = r.value if rc == 0 else None
+    return out
+
+
+def cpu_reference_rate(pts, cams, budget_s=15.0, threads=None, max_frames=None):
     """Reference CPU arm (osn_tsdf_create/_integrate, all host threads) on the
-    first frames of the trajectory, from an empty volume, bounded by budget_s."""
+    first max_frames frames of the trajectory, each pass from an empty volume,
+    passes repeated until budget_s is spent (at least one). Returns (frames/s,
+    frames integrated, threads, seconds)."""
     import ctypes as C
     import oracle
     lib = oracle.ref_lib()
     threads = threads or (os.cpu_count() or 1)
-    v = lib.osn_tsdf_create(VOXEL, POOL, TRUNC, CAP)
-    lib.osn_tsdf_set_thread_count(v, threads)
+    sample = list(zip(pts, cams))[: max_frames or len(pts)]
     done, t_total = 0, 0.0
-    try:
-        for p, cam in zip(pts, cams):
-            ptr = p.ctypes.data_as(C.POINTER(C.c_float))
-            t0 = time.perf_counter()
-            rc = lib.osn_tsdf_integrate(v, ptr, None, None, p.shape[0], 0, *cam, 0.0)
-            t_total += time.perf_counter() - t0
-            if rc != 0:
-                raise RuntimeError(f"reference integrate returned {rc}")
-            done += 1
-            if t_total > budget_s:
-                break
-    finally:
-        lib.osn_tsdf_destroy(v)
+    while True:
+        v = lib.osn_tsdf_create(VOXEL, POOL, TRUNC, CAP)
+        lib.osn_tsdf_set_thread_count(v, threads)
+        try:
+            for p, cam in sample:
+                ptr = p.ctypes.data_as(C.POINTER(C.c_float))
+                t0 = time.perf_counter()
+                rc = lib.osn_tsdf_integrate(v, ptr, None, None, p.shape[0], 0, *cam, 0.0)
+                t_total += time.perf_counter() - t0
+                if rc != 0:
+                    raise RuntimeError(f"reference integrate returned {rc}")
+                done += 1
+        finally:
+            lib.osn_tsdf_destroy(v)
+        if t_total > budget_s:
+            break
     return done / t_total, done, threads, t_total
 
 
@@ -304,7 +357,7 @@ def run_reference(args):
     threads = os.cpu_count() or 1
     rates = []
     for i in range(args.warmup + args.steps):
-        rate, done, _, t = cpu_reference_rate(pts, cams, budget_s=1e9, threads=threads)
+        rate, done, _, t = cpu_reference_rate(pts, cams, budget_s=0.0, threads=threads)
         if i >= args.warmup:
             rates.append((done, t))
     total_frames = sum(d for d, _ in rates)
@@ -409,6 +462,8 @@ def run_ours(args):
     blocks = vol.block_count()
     drops = vol.drop_count()
     status = vol.status()
+    # The headline run's volume, kept for the parity check against the oracle.
+    headline_voxels = sorted_fp32_voxels(*vol.voxels()) if rank == 0 else None
     frames_total = replica_work(N_FRAMES * args.steps, world)
     value = frames_total / (ms / 1e3)
 
@@ -512,17 +567,16 @@ def run_ours(args):
     blocks_depth_frames = vol.block_count()
     clocks.__exit__(None, None, None)
 
-    # -- one instrumented step: per-kernel CUDA-event times (every launch of
-    # the volume bracketed on its stream; no synchronisation between frames;
-    # serial mode, so kernels do not overlap)
+    # -- one instrumented step of the headline arm: per-kernel CUDA-event
+    # times (every launch of the volume bracketed on its stream; no
+    # synchronisation between calls; serial mode, so kernels do not overlap)
     vol.set_pipelined(False)
     vol.set_timing(True)
     vol.kernel_times()  # flush
     base = vol.kernel_times()
     vol.reset()
-    for k in range(N_FRAMES):
-        a, b = int(offsets[k]), int(offsets[k + 1])
-        vol.integrate(d_all[a:b], cams[k])
+    for lo, hi, a, b, begin, gcams in groups:
+        vol.integrate_frames(d_all[a:b], begin, gcams)
     # Extraction of the trajectory's volume into a device buffer (the
     # marching-tetrahedra kernel alone is timed).
     ext_cap = 1 << 24
@@ -538,21 +592,38 @@ def run_ours(args):
     times = vol.kernel_times()
     vol.set_timing(False)
     per_kernel = {k: (times[k][0] - base[k][0], times[k][1] - base[k][1]) for k in KERNEL_NAMES}
-    # -- stage statistics of every frame (read back per frame; untimed)
+    # -- stage statistics of every call of the headline arm (read back per
+    # call; untimed)
     vol.reset()
     updated, records, touched, crossing = [], [], [], []
-    for k in range(N_FRAMES):
-        a, b = int(offsets[k]), int(offsets[k + 1])
-        vol.integrate(d_all[a:b], cams[k])
+    for lo, hi, a, b, begin, gcams in groups:
+        vol.integrate_frames(d_all[a:b], begin, gcams)
         st = vol.last_update_stats()
         updated.append(st["updated_voxels"])
         records.append(st["records"])
         touched.append(st["touched_blocks"])
         crossing.append(st["crossing_voxels"])
-    integrate_kernels = ("band", "finish", "group", "values", "deferred")
+    # -- allocation's L2 atomics (CAS attempts counted by the measurement
+    # mode; each new block adds its pool-counter add and its publishing
+    # exchange) and the probe-depth histogram of every resolved block run
+    vol.reset()
+    cas = 0
+    for k in range(N_FRAMES):
+        a, b = int(offsets[k]), int(offsets[k + 1])
+        before = vol.drop_count()
+        vol.allocate_counting_cas(d_all[a:b], cams[k])
+        cas += vol.drop_count() - before
+    alloc_atomics = int(cas) + 2 * vol.block_count()
+    vol.reset()
+    hist = np.zeros(32, dtype=np.uint64)
+    for k in range(N_FRAMES):
+        a, b = int(offsets[k]), int(offsets[k + 1])
+        hist += vol.allocate_probe_histogram(d_all[a:b], cams[k], n_bins=32)
+    probes_mean = float(np.sum(hist * np.arange(32)) / max(1, int(hist.sum())))
+    integrate_kernels = ("band", "finish", "group")
     # Launches of the headline arm: per integrate_frames call the set-up
-    # kernel and the four passes; reset's two per step.
-    launches_per_step = 5 * len(groups) + 2
+    # kernel and the three passes; reset's two per step.
+    launches_per_step = 4 * len(groups) + 2
     dominant = max(integrate_kernels, key=lambda k: per_kernel[k][0])
 
     peak, peak_kind = measured_peak()
@@ -567,9 +638,7 @@ def run_ours(args):
     alg_total = {
         "band": 12 * n_points + 4 * n_slots + 16 * n_rec,
         "finish": n_touch * 512 * (16 + 36),   # read cnt,w,t,sum; write t,w,r,g,b,cnt,sum
-        "group": 4 * n_slots,
-        "values": 0,
-        "deferred": 0,
+        "group": 8 * n_slots,   # record and normalised SDF of every band slot
     }
     # Update as the reference scopes it: positions + tsdf/weight tiles of the
     # touched blocks, read and written; the stricter figure counts only the
@@ -581,13 +650,34 @@ def run_ours(args):
     t_extract = per_kernel["extract"][0] / 1e3
     extract_alg_bytes = ext_blocks * (512 + 217) * 8 + 24 * max(ext_verts, 0)
     dom_ms, dom_n = per_kernel[dominant]
-    dom_alg = alg_total.get(dominant, 0) / N_FRAMES
+    dom_alg = alg_total.get(dominant, 0) / dom_n if dom_n else 0.0
     achieved = dom_alg / (dom_ms / 1e3 / dom_n) / 1e9 if dom_n else 0.0
     roofline = {
         "bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
         "frac": achieved / peak, "peak_source": peak_kind,
         "traffic": profile_traffic(dominant),
         "alg_bytes_per_launch": dom_alg, "mean_launch_us": 1e3 * dom_ms / dom_n if dom_n else None,
+    }
+    # The roofs the L2-resident kernels are judged against: the band walk's
+    # per-sample reductions (a 4-byte count and an 8-byte sum per counted
+    # sample) against the measured L2 reduction rate at that 1:1 mix; finish's
+    # tile bytes against the measured L2 streaming rate.
+    from what_irregularity_costs_b200 import _lib as _l
+    l2 = l2_ceilings(_l.load())
+    t_band = per_kernel["band"][0] / 1e3
+    t_fin = per_kernel["finish"][0] / 1e3
+    r32, r64 = l2.get("red_u32_gops"), l2.get("red_u64_gops")
+    red_mix = 2.0 / (1.0 / r32 + 1.0 / r64) if r32 and r64 else None
+    band_red = 2.0 * n_rec / t_band / 1e9 if t_band else None
+    fin_gbps = alg_total["finish"] / t_fin / 1e9 if t_fin else None
+    roofline["l2"] = {
+        "ceilings": l2,
+        "band": {"achieved_red_gops": band_red, "peak_red_gops": red_mix,
+                 "frac": band_red / red_mix if band_red and red_mix else None,
+                 "unit": "G reductions/s (count u32 + sum u64 per counted sample)"},
+        "finish": {"achieved_gbps": fin_gbps, "peak_gbps": l2.get("load16_gbps"),
+                   "frac": fin_gbps / l2["load16_gbps"] if fin_gbps and l2.get("load16_gbps") else None,
+                   "unit": "GB/s of tile bytes (read + written) against L2 streaming loads"},
     }
 
     a3 = None
@@ -597,15 +687,57 @@ def run_ours(args):
         except Exception as e:  # reported beside the line, never required
             a3 = {"impl": "reference CUDA arm (A3)", "value": None, "error": str(e)}
 
+    # -- the batched form against the plain arm on the 32-scene mix: a bounded
+    # run (batch_warmup + batch_steps steps) reported beside the headline
+    batch32 = None
+    if rank == 0 and world == 1 and args.batch_steps > 0:
+        try:
+            from what_irregularity_costs_b200 import workloads
+            specs = workloads.scene_mix(32)
+            mix = workloads.mix_frames(specs, args.batch_warmup + args.batch_steps)
+            fig = batch32_figures(specs, mix, args.batch_steps, args.batch_warmup, torch)
+            errs = [e for e in fig["precision_vs_fp64"]["fp16_u16"] if "max_m" in e]
+            batch32 = {
+                "metric": "frames/s (32-scene batched integrate)",
+                "batched_fp16": fig["value"], "plain_fp32": fig["plain_fp32"]["value"],
+                "batched_fp32": fig["batched_fp32"]["value"],
+                "ratio_fp16_vs_plain": fig["speedup_vs_plain"],
+                "ratio_fp32_vs_plain": fig["batched_fp32"]["value"] / fig["plain_fp32"]["value"],
+                "blocks_identical": fig["blocks_identical"],
+                "fp16_tsdf_err_max_m": max((e["max_m"] for e in errs), default=None),
+                "fp16_tsdf_err_rms_m": max((e["rms_m"] for e in errs), default=None),
+                "precision_scenes": len(errs),
+                "e2e": fig["e2e"], "steps": args.batch_steps, "warmup": args.batch_warmup,
+                "shape": fig["shape"], "status": fig["status"],
+                "note": "every scene of the mix advances one frame per step; batched arms are the "
+                        "work-queued passes replayed from a CUDA graph; plain = each scene through "
+                        "osn_tsdf_cuda_integrate on its own stream",
+            }
+            del mix
+            torch.cuda.synchronize()
+        except Exception as e:  # reported beside the line, never required
+            batch32 = {"error": str(e)}
+
+    parity = None
+    if rank == 0 and not args.no_parity:
+        try:
+            parity = parity_vs_oracle(headline_voxels, pts, cams,
+                                      f"osn_tsdf_cuda_integrate_frames, {fpc} frames per call, pipelined")
+        except Exception as e:  # reported, never fatal to the line
+            parity = {"ok": False, "error": str(e)}
+
     cpu = None
     if rank == 0 and not args.no_cpu:
         try:
             import oracle
             if oracle.ref_available():
-                rate, done, threads, t = cpu_reference_rate(pts, cams, budget_s=args.cpu_budget)
+                nf = min(args.ref_frames, N_FRAMES)
+                rate, done, threads, t = cpu_reference_rate(pts, cams, budget_s=args.cpu_budget,
+                                                            max_frames=nf)
                 cpu = {"value": rate, "unit": "frames/s", "cores": threads, "kind": "reference",
-                       "sample": f"first {done} frames of the trajectory from an empty volume "
-                                 f"({t:.1f} s)"}
+                       "sample": f"the first {nf} frames of the trajectory from an empty volume, "
+                                 f"repeated: {done} frames in {t:.1f} s (the sample bench.py "
+                                 f"--impl reference times)"}
         except Exception as e:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "frames/s", "cores": None, "kind": "reference",
                    "sample": f"failed: {e}"}
@@ -644,6 +776,18 @@ def run_ours(args):
             "gpu_launches": int(launches_per_step * args.steps),
             "clocks": clocks.summary(),
             "alloc_mrays_per_s": n_points / t_alloc / 1e6 if t_alloc else None,
+            "alloc_l2_atomics": {
+                "ops": alloc_atomics, "gops_per_s": alloc_atomics / t_alloc / 1e9 if t_alloc else None,
+                "peak_atom_gops": l2.get("atom_u32_gops"),
+                "frac": (alloc_atomics / t_alloc / 1e9 / l2["atom_u32_gops"])
+                if t_alloc and l2.get("atom_u32_gops") else None,
+                "note": "CAS attempts + pool-counter add + publishing exchange per new block, over "
+                        "the allocate-only walk of the trajectory; warp key grouping keeps CAS "
+                        "attempts near one per new block"},
+            "probe_hist": {"bins": [int(x) for x in hist[:12]], "mean_probes": probes_mean,
+                           "unit": "block resolutions by slots probed (bin k = k slots)"},
+            "parity": parity,
+            "batch32": batch32,
             "update_gbps": update_alg_bytes / t_update / 1e9 if t_update else None,
             "update_gbps_updated_voxels": update_alg_bytes_voxels / t_update / 1e9 if t_update else None,
             "extract": {"blocks": ext_blocks, "vertices": ext_verts,
@@ -654,10 +798,11 @@ def run_ours(args):
             "kernel_ms_per_step": {k: round(v[0], 4) for k, v in per_kernel.items()},
             "kernel_launches_per_step": {k: v[1] for k, v in per_kernel.items()},
             "blocks": blocks, "drops": int(drops), "status": status,
-            "updated_voxels_per_frame": float(np.mean(updated)),
-            "touched_blocks_per_frame": float(np.mean(touched)),
-            "crossing_voxels_per_frame": float(np.mean(crossing)),
-            "records_per_frame": float(np.mean(records)),
+            # Per frame of the headline arm (its calls' counts over the frames).
+            "updated_voxels_per_frame": float(np.sum(updated)) / N_FRAMES,
+            "touched_blocks_per_frame": float(np.sum(touched)) / N_FRAMES,
+            "crossing_voxels_per_frame": float(np.sum(crossing)) / N_FRAMES,
+            "records_per_frame": float(np.sum(records)) / N_FRAMES,
         }
         print(json.dumps(line))
     if dist is not None:
@@ -682,13 +827,39 @@ def run_batch32(args):
     """
     from what_irregularity_costs_b200 import workloads
     specs = workloads.scene_mix(32)
-    n_steps = args.warmup + args.steps
-    frames = workloads.mix_frames(specs, n_steps)  # before any CUDA use
+    frames = workloads.mix_frames(specs, args.warmup + args.steps)  # before any CUDA use
     import torch
-    from what_irregularity_costs_b200 import (STORAGE_FP16_U16, STORAGE_FP32, STORAGE_FP64, Batch,
-                                              device_tensor, precision)
     rank, local, world, dist = dist_setup(args.gpus)
     torch.cuda.set_device(local)
+    fig = batch32_figures(specs, frames, args.steps, args.warmup, torch)
+    if rank == 0:
+        line = {
+            "metric": "frames/s (32-scene batched integrate)", "value": fig["value"],
+            "unit": "frames/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f16 tsdf / u16 weight storage, f32 running average",
+            "data": "synthetic: 32 seeded room scenes (scene_mix seed 4)",
+        }
+        line.update(fig)
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def batch32_figures(specs, frames, steps, warmup, torch):
+    """The arms of the 32-scene batched mix over the same steps (see
+    run_batch32), as a dict: value (batched FP16), plain_fp32, batched_fp32,
+    speedup_vs_plain, blocks_identical, precision_vs_fp64, e2e, autotune."""
+    from what_irregularity_costs_b200 import (STORAGE_FP16_U16, STORAGE_FP32, STORAGE_FP64, Batch,
+                                              device_tensor, precision, workloads)
+
+    class _A:  # the step counts the arms below read
+        pass
+    args = _A()
+    args.steps, args.warmup = steps, warmup
+    n_steps = args.warmup + args.steps
     dev = workloads.upload(frames, torch)
     active = [[s.index for s in specs if k < len(frames[s.index])] for k in range(n_steps)]
     timed_frames = sum(len(active[k]) for k in range(args.warmup, n_steps))
@@ -831,35 +1002,26 @@ def run_batch32(args):
                          "rms_m": float(np.sqrt(np.mean(e * e))) if e.size else 0.0})
         del o
 
-    if rank == 0:
-        line = {
-            "metric": "frames/s (32-scene batched integrate)", "value": res16["value"],
-            "unit": "frames/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": res16["ms_per_step"], "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f16 tsdf / u16 weight storage, f32 running average",
-            "data": "synthetic: 32 seeded room scenes (scene_mix seed 4)",
-            "config": {"workload": "32-scene mix: tables 2^14-2^20 (log-uniform), voxels 1-4 cm "
-                                   "(log-uniform), 160x120..1280x720, 8-256 frames, cap 64; step = "
-                                   "every active scene integrates its next frame",
-                       "scenes": [s.__dict__ for s in specs], "frames_in_window": timed_frames,
-                       "l2": "inputs larger than L2: %.0f MB of points in the timed steps"
-                             % (sum(dev[si][k].numel() * 4 for k in range(args.warmup, n_steps)
-                                    for si in active[k]) / 1e6)},
-            "shape": shape, "graph": True, "status": res16["status"],
-            "plain_fp32": plain, "batched_fp32": res32b,
-            "speedup_vs_plain": res16["value"] / plain["value"],
-            "blocks_identical": blocks16 == blocks32b == blocks_plain,
-            "precision_vs_fp64": {"fp16_u16": errs16, "fp32": errs32},
-            "e2e": {"value": res_e2e["value"], "unit": "frames/s",
-                    "h2d_bytes_per_step": res_e2e["h2d_bytes_per_step"],
-                    "d2h_bytes_per_step": res_e2e["d2h_bytes_per_step"]},
-            "autotune": res16.get("tune"),
-        }
-        print(json.dumps(line))
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
-    return 0
+    line = {
+        "value": res16["value"], "unit": "frames/s", "ms_per_step": res16["ms_per_step"],
+        "config": {"workload": "32-scene mix: tables 2^14-2^20 (log-uniform), voxels 1-4 cm "
+                               "(log-uniform), 160x120..1280x720, 8-256 frames, cap 64; step = "
+                               "every active scene integrates its next frame",
+                   "scenes": [s.__dict__ for s in specs], "frames_in_window": timed_frames,
+                   "l2": "inputs larger than L2: %.0f MB of points in the timed steps"
+                         % (sum(dev[si][k].numel() * 4 for k in range(args.warmup, n_steps)
+                                for si in active[k]) / 1e6)},
+        "shape": shape, "graph": True, "status": res16["status"],
+        "plain_fp32": plain, "batched_fp32": res32b,
+        "speedup_vs_plain": res16["value"] / plain["value"],
+        "blocks_identical": blocks16 == blocks32b == blocks_plain,
+        "precision_vs_fp64": {"fp16_u16": errs16, "fp32": errs32},
+        "e2e": {"value": res_e2e["value"], "unit": "frames/s",
+                "h2d_bytes_per_step": res_e2e["h2d_bytes_per_step"],
+                "d2h_bytes_per_step": res_e2e["d2h_bytes_per_step"]},
+        "autotune": res16.get("tune"),
+    }
+    return line
 
 
 def run_serve64(args):
@@ -1042,6 +1204,11 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-a3", action="store_true", help="skip timing the reference's CUDA arm")
+    ap.add_argument("--batch-steps", type=int, default=5,
+                    help="timed steps of the 32-scene batched comparison in the room line (0: skip)")
+    ap.add_argument("--batch-warmup", type=int, default=3)
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the check of the headline run's volume against the oracle")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--ref-frames", type=int, default=20,
                     help="frames per step of the reference arm")

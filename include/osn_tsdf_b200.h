@@ -2,7 +2,7 @@
  * reference's CUDA C ABI.
  *
  * The first block below is the reference's CUDA section of
- * cpp/include/osn_tsdf/c_api.h (lines 223-293), re-declared with identical
+ * cpp/include/osn_tsdf/c_api.h (lines 56-126), re-declared with identical
  * names, argument meanings and return codes, so a caller of the reference's
  * CUDA arm (A3) links against this library instead without a source change.
  * The CPU section of that header (c_api.h:14-46) is the reference's own CPU
@@ -137,6 +137,35 @@ OsnTsdfCudaVolume* osn_tsdf_cuda_create_ex(float voxel_size_m, int32_t pool_capa
                                            float trunc_m, float weight_cap, uint32_t hash_slots,
                                            int32_t storage);
 
+/* Table layouts for create_layout.
+ *   POOL        the reference's: a block's pool index comes from a counter
+ *               after its key is claimed, published into the slot once its
+ *               coordinate is written; a thread that meets a claimed key
+ *               waits for the index (bounded).
+ *   SLOT_INDEX  the pool is the table: a block's pool index is its table
+ *               slot, so a claim publishes everything at once and a thread
+ *               that meets the key returns the slot without waiting (the
+ *               layout of the reference's slot-index measurement variant,
+ *               cpp/src/volume_cuda.cu:194-257, as a production layout). The
+ *               pool capacity becomes the table size (hash_slots, or
+ *               next_pow2(2 * pool)): about twice the voxel memory. In the
+ *               device view block_coord, tsdf, weight, ... are indexed by
+ *               slot (only occupied slots -- key >= 0 -- are blocks), not
+ *               dense 0..block_count-1; snapshot/restore and chunk eviction
+ *               need the POOL layout (they return -1 / 1 here). Results
+ *               (blocks, voxels, meshes) are those of the POOL layout. */
+#define OSN_TSDF_LAYOUT_POOL 0
+#define OSN_TSDF_LAYOUT_SLOT_INDEX 1
+
+/* create_ex with a table layout (OSN_TSDF_LAYOUT_*). No counterpart in the
+ * reference. NULL for an unknown layout. */
+OsnTsdfCudaVolume* osn_tsdf_cuda_create_layout(float voxel_size_m, int32_t pool_capacity_blocks,
+                                               float trunc_m, float weight_cap, uint32_t hash_slots,
+                                               int32_t storage, int32_t layout);
+
+/* The volume's table layout, or -1 for a bad handle. */
+int32_t osn_tsdf_cuda_layout(const OsnTsdfCudaVolume* v);
+
 /* allocate_blocks then update_voxels on the same points, as the reference's
  * CPU integrate (cpp/src/volume.cpp:301-304), in one pass: blocks are
  * allocated and contributions counted by the same walk. Results are those of
@@ -227,10 +256,54 @@ int64_t osn_tsdf_cuda_snapshot_bytes(OsnTsdfCudaVolume* v);
 int64_t osn_tsdf_cuda_snapshot(OsnTsdfCudaVolume* v, void* host_buffer, int64_t capacity);
 int32_t osn_tsdf_cuda_restore(OsnTsdfCudaVolume* v, const void* host_buffer, int64_t size);
 
+/* Streaming by chunk id. No counterpart in the reference, which declares a
+ * chunk id on every point batch (cpp/include/osn_tsdf/types.hpp:127) but
+ * never reads it. Every block carries the chunk id of the last call that
+ * allocated or updated it; set_chunk sets the id later calls give (0 at
+ * creation; the C++ class takes PointBatch::chunk_id).
+ * evict_chunks moves every block whose chunk id lies in [lo, hi] into a host
+ * pack (header, coordinates, chunk ids, voxel arrays; evict_chunks_bytes
+ * gives its size) and removes it from the volume: the remaining blocks move
+ * to the front of the pool in their old order (new pool indices, same
+ * contents), the freed pool entries are zeroed and the table is rebuilt, so
+ * a scene larger than the pool keeps integrating. Returns the pack's bytes,
+ * or -1 (bad range, buffer too small, CUDA error).
+ * stream_in inserts a pack's blocks again with their voxels and chunk ids;
+ * blocks present again in the volume are left as they are and counted in
+ * *skipped. Returns 0, 1 on a bad pack (another volume's voxel size,
+ * truncation, cap or storage), 2 when the pool filled (some blocks not
+ * restored), 3 on a CUDA error. All wait for the volume's stream. */
+int32_t osn_tsdf_cuda_set_chunk(OsnTsdfCudaVolume* v, int32_t chunk_id);
+int64_t osn_tsdf_cuda_evict_chunks_bytes(OsnTsdfCudaVolume* v, int32_t lo, int32_t hi);
+int64_t osn_tsdf_cuda_evict_chunks(OsnTsdfCudaVolume* v, int32_t lo, int32_t hi, void* host_buffer,
+                                   int64_t capacity);
+int32_t osn_tsdf_cuda_stream_in(OsnTsdfCudaVolume* v, const void* host_buffer, int64_t size,
+                                int32_t* skipped);
+
 /* Device error word, after waiting for the stream: 0 when every bounded
  * wait in the kernels finished in time; bit 0 = a publication wait gave up,
  * bit 1 = an update batch exceeded its scratch. */
 uint32_t osn_tsdf_cuda_status(const OsnTsdfCudaVolume* v);
+
+/* Bound on each device-side wait of this volume's later calls (a thread
+ * waiting for another to publish the pool index of a block it inserted), in
+ * iterations of ~100 ns, 1 .. 2^20 (the default, ~0.1 s). A wait that runs
+ * out drops its samples and sets bit 0 of the status word. No counterpart in
+ * the reference, whose waits are unbounded (cpp/src/volume_cuda.cu:71-72).
+ * Returns 0, or 1 on a bad volume or an out-of-range bound. */
+int32_t osn_tsdf_cuda_set_spin_limit(OsnTsdfCudaVolume* v, int32_t iterations);
+
+/* Measured L2 ceiling of the current GPU, for roofline fractions of kernels
+ * whose working set stays in L2. No counterpart in the reference. One probe
+ * kernel over a fresh device buffer of `bytes` (1 MiB .. 2 GiB; L2-resident
+ * well below 126 MB), `iters` operations per thread on a persistent grid of
+ * 8 x 256-thread CTAs per SM, timed after a warm-up launch. kind 0:
+ * red.add.u64 to pseudo-random words (G ops/s); 1: red.add.u32 (G ops/s);
+ * 2: atomic add with return (G ops/s); 3: streamed 16-byte loads through L2
+ * (GB/s); 4: pseudo-random 4-byte loads through L2 (G loads/s). Allocates and
+ * frees its buffer and synchronises. Returns 0, 1 on bad arguments, 3 on a
+ * CUDA error. */
+int32_t osn_tsdf_cuda_l2_probe(int32_t kind, int64_t bytes, int32_t iters, double* result);
 
 /* The volume's cudaStream_t, for callers that order their own work after it.
  * In pipelined mode (below) the last calls' update tails may still run on an
@@ -238,8 +311,8 @@ uint32_t osn_tsdf_cuda_status(const OsnTsdfCudaVolume* v);
 void* osn_tsdf_cuda_stream(const OsnTsdfCudaVolume* v);
 
 /* Pipelined updates. When enabled, an integrate/update call's band walk is
- * queued on the volume's stream as usual but its update tail (finish, group,
- * deferred) runs on an internal stream, so the next call's walk
+ * queued on the volume's stream as usual but its update tail (finish,
+ * group) runs on an internal stream, so the next call's walk
  * overlaps this call's tail; the per-call scratch alternates between two sets
  * (twice the per-voxel batch state: +12 bytes per voxel). Results are
  * identical. The positions (or depth image) of a call may be reused once the
@@ -279,17 +352,20 @@ int32_t osn_tsdf_cuda_last_update_stats(const OsnTsdfCudaVolume* v, int64_t* out
 /* update_voxels that allocates no device memory. No counterpart in the
  * reference. update_voxels may grow its scratch with cudaMalloc (after
  * waiting for the stream) when a batch is larger than any before it; callers
- * that cannot allow that -- code recording the integrate into a CUDA graph
- * (no allocation during stream capture), serving loops that budget device
- * memory up front, latency-critical threads that cannot absorb the implied
- * synchronisation -- call this instead. Same results as update_voxels.
- * Its scratch is one fixed 56 MiB array inside the library, held on every
+ * that cannot allow that -- serving loops that admit work against a fixed
+ * device-memory budget, latency-critical threads that cannot absorb the
+ * device-wide synchronisation cudaMalloc/cudaFree imply -- call this
+ * instead. Same results as update_voxels.
+ * Its scratch is one fixed 32 MiB array inside the library, held on every
  * GPU where the library's code is loaded until the process exits, and shared
  * by all calls: calls whose work overlaps on the GPU race and must be
- * serialised. The first call on a device resolves the array's address and
- * must come before any stream capture. Returns 0 (queued), 1 on bad
- * arguments, 3 on a set-up or launch failure, 4 when n_points * (2*steps+1)
- * exceeds OSN_TSDF_NOALLOC_MAX_RECORDS (nothing is queued; split the batch). */
+ * serialised. The calling thread's current device must be the volume's. The
+ * first call on a device resolves the array's address (a set-up step) and
+ * should come before any stream capture. last_update_stats afterwards reports
+ * this call's counters. Returns 0 (queued), 1 on bad arguments (including a
+ * current device other than the volume's), 3 on a set-up or launch failure,
+ * 4 when n_points * (2*steps+1) exceeds OSN_TSDF_NOALLOC_MAX_RECORDS
+ * (nothing is queued; split the batch). */
 int32_t osn_tsdf_cuda_update_voxels_noalloc(OsnTsdfCudaVolume* v, const float* d_positions,
                                             int32_t n_points, float cam_x, float cam_y,
                                             float cam_z, float radius_m);
@@ -300,7 +376,7 @@ int32_t osn_tsdf_cuda_update_voxels_noalloc(OsnTsdfCudaVolume* v, const float* d
  * size and truncation, one storage mode for all) integrate one frame each
  * per step in one chain of work-queued passes on the batch's stream: a
  * table of the step's scenes is uploaded, then one pass of each kernel
- * (band walk, finish, group, values, deferred) covers every scene, its CTAs
+ * (band walk, finish, group) covers every scene, its CTAs
  * taking (scene, tile range) work items from atomic queues. Results are
  * bit-identical to integrating each scene alone with osn_tsdf_cuda_integrate.
  *
@@ -359,8 +435,9 @@ int32_t osn_tsdf_batch_size(OsnTsdfBatch* b);
  * waits for) the accumulated per-kernel milliseconds and launch counts.
  * Kernel ids: 0 allocate, 1 band (count-and-sum walk; allocates too in
  * integrate), 2 finish (per touched block), 3 group (records of voxels that
- * cross the cap), 4 deferred (ordered cap selection), 5 extract, 6 reset,
- * 7 values (ids and signed distances of the grouped records).
+ * cross the cap, grouped per voxel, with the ordered cap selection and the
+ * voxels' update), 5 extract, 6 reset; ids 4 and 7 are kept for the
+ * numbering and record no launches.
  * Returns the number of ids written. */
 int32_t osn_tsdf_cuda_set_timing(OsnTsdfCudaVolume* v, int32_t enabled);
 int32_t osn_tsdf_cuda_kernel_times(OsnTsdfCudaVolume* v, double* ms, int64_t* launches,

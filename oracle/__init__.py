@@ -29,10 +29,12 @@ _i32p = C.POINTER(C.c_int32)
 _i64p = C.POINTER(C.c_int64)
 
 
-def build(ref_root: str | None = None) -> None:
-    """Compile the restatement and, when the reference tree is present, the reference."""
+def build(ref_root: str | None = None, gate: bool = False) -> None:
+    """Compile the restatement and, when the reference tree is present, the
+    reference's CPU and CUDA arms; with gate=True (the library must be built)
+    also the reference's own C++ GPU test linked against this library."""
     env = dict(os.environ)
-    cmd = ["make", "-s", "-C", HERE, "all"]
+    cmd = ["make", "-s", "-C", HERE, "all"] + (["gate"] if gate else [])
     if ref_root:
         cmd.append(f"REF_ROOT={ref_root}")
     subprocess.run(cmd, check=True, env=env)

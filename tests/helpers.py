@@ -52,6 +52,26 @@ def assert_same_voxels(gpu, ref, tol=TSDF_TOL, exact_tsdf=False):
     return err
 
 
+# Mean normalised TSDF of FP16 storage against the oracle: four half ulps of
+# [-1, 1] (FP16 rounding of the running mean) plus the FP32 parity bar.
+FP16_ORACLE_TOL = 4 * 2.0 ** -11 + TSDF_TOL
+
+
+def assert_matches_oracle(vol, ref, tol=TSDF_TOL):
+    """Any storage mode against the CPU oracle: block set and weights exact,
+    mean normalised TSDF within tol. Returns the largest mean difference."""
+    from what_irregularity_costs_b200 import precision
+    gc, gm, gw = precision._aligned(vol)
+    rc, rt, rw, *_ = sorted_voxels(ref)
+    assert gc.shape == rc.shape and np.array_equal(gc, rc), "block sets differ from the oracle"
+    bad = int(np.sum(gw != rw))
+    assert bad == 0, f"{bad} weights differ from the oracle"
+    seen = rw > 0
+    err = float(np.max(np.abs(gm[seen] - rt[seen] / rw[seen]))) if seen.any() else 0.0
+    assert err <= tol, f"mean TSDF differs from the oracle by {err:.3e} > {tol:.1e}"
+    return err
+
+
 def sphere_errors(mesh, center, radius):
     p = mesh[:, :3].astype(np.float64) - np.asarray(center, dtype=np.float64)
     e = np.abs(np.linalg.norm(p, axis=1) - radius)

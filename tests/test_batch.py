@@ -11,6 +11,8 @@ and caps; scenes that sit steps out; CUDA-graph replay; the autotuner
 import numpy as np
 import pytest
 
+import oracle
+from helpers import FP16_ORACLE_TOL, assert_matches_oracle
 from what_irregularity_costs_b200 import (STORAGE_FP16_U16, STORAGE_FP32, Batch, CudaVolume,
                                           precision, scenes)
 
@@ -83,6 +85,17 @@ def _run(torch, storage=STORAGE_FP32, n_frames=3, idle=None, graph=False, tune=0
     return batch, bvols, avols
 
 
+def _oracles(n_frames=3):
+    """Every MIX scene fed to the CPU oracle, frame by frame."""
+    out = []
+    for seed, voxel, slots, res, cap in MIX:
+        ref = oracle.OracleVolume(voxel, min(slots // 2, 1 << 15), 4 * voxel, cap, slots)
+        for f in _frames(seed, res, n_frames):
+            ref.integrate(scenes.frame_points(f), f.cam)
+        out.append(ref)
+    return out
+
+
 def test_batch_equals_each_scene_alone(cuda):
     batch, bvols, avols = _run(cuda)
     for b, a in zip(bvols, avols):
@@ -91,6 +104,11 @@ def test_batch_equals_each_scene_alone(cuda):
         _same(b, a)
     # A capped scene crossed its cap inside a frame (ordered selection ran).
     assert any(a.last_update_stats()["crossing_voxels"] > 0 for a in avols)
+    # And every scene of the mix -- 1280x720 frames, a 2^14-slot table, caps
+    # 64 / 32 / 6 / none, voxels 1-4 cm -- equals the CPU oracle.
+    for b, ref in zip(bvols, _oracles()):
+        assert b.drop_count() == ref.drop_count()
+        assert_matches_oracle(b, ref)
 
 
 def test_batch_with_idle_scenes(cuda):
@@ -130,6 +148,8 @@ def test_batch_fp16_storage(cuda):
     _, bvols, avols = _run(cuda, storage=STORAGE_FP16_U16)
     for b, a in zip(bvols, avols):
         _same(b, a)
+    for b, ref in zip(bvols, _oracles()):
+        assert_matches_oracle(b, ref, tol=FP16_ORACLE_TOL)
 
 
 def test_batch_argument_checks(cuda):

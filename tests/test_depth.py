@@ -10,7 +10,8 @@ drops -- with invalid pixels, a range cutoff, and voxels crossing the cap.
 import numpy as np
 import pytest
 
-from helpers import sorted_voxels
+import oracle
+from helpers import assert_matches_oracle, sorted_voxels
 from what_irregularity_costs_b200 import CudaVolume, scenes
 
 pytestmark = pytest.mark.gpu
@@ -30,16 +31,20 @@ def test_depth_frames_equal_backprojected_points(cuda, res, cap, max_range):
     K = scenes.ROOM_K.scaled(*res)
     pts_vol = CudaVolume(0.02, 1 << 17, 0.08, cap, 1 << 18)
     dep_vol = CudaVolume(0.02, 1 << 17, 0.08, cap, 1 << 18)
+    ref = oracle.OracleVolume(0.02, 1 << 17, 0.08, cap, 1 << 18)
     for k in range(3):
         f = scenes.room_frame(scene, k, K)
         pts = scenes.frame_points(f, max_range)
         pts_vol.integrate(cuda.from_numpy(pts).cuda(), f.cam)
         dep_vol.integrate_depth(cuda.from_numpy(f.depth).cuda(), f.K, f.R, f.t, max_range)
+        ref.integrate(pts, f.cam)  # the host's FP64 backprojection, fed to the oracle
     pts_vol.synchronize()
     dep_vol.synchronize()
     assert dep_vol.status() == 0
-    assert dep_vol.block_count() == pts_vol.block_count() > 0
+    assert dep_vol.block_count() == pts_vol.block_count() == ref.block_count() > 0
     _same(pts_vol, dep_vol)
+    assert dep_vol.drop_count() == ref.drop_count()
+    assert_matches_oracle(dep_vol, ref)
     if cap == 6.0:
         assert dep_vol.last_update_stats()["crossing_voxels"] > 0
 
@@ -53,6 +58,10 @@ def test_depth_sphere_frame_and_mesh(cuda):
     _same(a, b)
     ma, mb = a.extract_mesh(1 << 20), b.extract_mesh(1 << 20)
     assert ma.shape == mb.shape and ma.shape[0] > 0
+    ref = oracle.OracleVolume(0.01, 1 << 15, 0.04, 64.0)
+    ref.integrate(scenes.frame_points(f), f.cam)
+    assert_matches_oracle(b, ref)
+    assert ref.extract(0.5, 0.0, 1 << 20).shape == mb.shape
 
 
 def test_depth_argument_checks(cuda):

@@ -11,6 +11,8 @@ memory budget must hold sessions back until earlier ones finish.
 import numpy as np
 import pytest
 
+import oracle
+from helpers import FP16_ORACLE_TOL, assert_matches_oracle
 from what_irregularity_costs_b200 import STORAGE_FP16_U16, CudaVolume, precision, scenes
 from what_irregularity_costs_b200.serving import Request, Server, footprint_bytes, poisson_schedule
 from what_irregularity_costs_b200.workloads import SceneSpec
@@ -65,6 +67,13 @@ def _check(torch, specs, frames, reqs, server):
         for r in reqs:
             if r.kind == "extract" and r.session == sp.index:
                 assert r.vertices == counts[r.frame] and r.vertices > 0
+        # The served session against the CPU oracle fed the same frames: block
+        # set and weights exact, mean TSDF within FP16 storage's bound.
+        ref = oracle.OracleVolume(sp.voxel, sp.pool, sp.trunc, sp.cap, sp.hash_slots)
+        for k in range(sp.frames):
+            p, cam = frames[sp.index][k % len(frames[sp.index])]
+            ref.integrate(p, cam)
+        assert_matches_oracle(served, ref, tol=FP16_ORACLE_TOL)
 
 
 def test_served_sessions_equal_alone(cuda):

@@ -71,6 +71,14 @@ _SIG = {
     "osn_tsdf_cuda_status": (C.c_uint32, [_P]),
     "osn_tsdf_cuda_stream": (_P, [_P]),
     "osn_tsdf_cuda_set_pipelined": (_I, [_P, _I]),
+    "osn_tsdf_cuda_set_spin_limit": (_I, [_P, _I]),
+    "osn_tsdf_cuda_set_chunk": (_I, [_P, _I]),
+    "osn_tsdf_cuda_create_layout": (_P, [_F, _I, _F, _F, C.c_uint32, _I, _I]),
+    "osn_tsdf_cuda_layout": (_I, [_P]),
+    "osn_tsdf_cuda_evict_chunks_bytes": (C.c_int64, [_P, _I, _I]),
+    "osn_tsdf_cuda_evict_chunks": (C.c_int64, [_P, _I, _I, _P, C.c_int64]),
+    "osn_tsdf_cuda_stream_in": (_I, [_P, _P, C.c_int64, _P]),
+    "osn_tsdf_cuda_l2_probe": (_I, [_I, C.c_int64, _I, _P]),
     "osn_tsdf_cuda_join": (_I, [_P]),
     "osn_tsdf_cuda_storage": (_I, [_P]),
     "osn_tsdf_cuda_snapshot_bytes": (C.c_int64, [_P]),

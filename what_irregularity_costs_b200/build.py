@@ -51,7 +51,7 @@ def _stale(out: str, deps: list[str]) -> bool:
 def build(verbose: bool = False, ptxas_info: bool = False) -> str:
     os.makedirs(OBJ, exist_ok=True)
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
-    headers.append(os.path.join(ROOT, "include", "osn_tsdf_b200.h"))
+    headers += [os.path.join(ROOT, "include", f) for f in os.listdir(os.path.join(ROOT, "include"))]
     exe = nvcc()
     jobs = []
     for src in sources():

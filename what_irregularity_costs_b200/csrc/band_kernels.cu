@@ -114,7 +114,8 @@ template <int MODE>
 __device__ __noinline__ int32_t resolve_slow(HashEntry* table, uint32_t hash_mask, int32_t pool,
                                              int32_t* block_count, unsigned long long* drop_count,
                                              BlockCoord* block_coord, uint32_t* status,
-                                             long long key) {
+                                             int32_t spin_limit, int32_t* block_chunk, int32_t chunk,
+                                             int32_t slot_index, long long key) {
     DevVolume v{};
     v.table = table;
     v.hash_mask = hash_mask;
@@ -123,6 +124,10 @@ __device__ __noinline__ int32_t resolve_slow(HashEntry* table, uint32_t hash_mas
     v.drop_count = drop_count;
     v.block_coord = block_coord;
     v.status = status;
+    v.spin_limit = spin_limit;
+    v.block_chunk = block_chunk;
+    v.chunk = chunk;
+    v.slot_index = slot_index;
     return resolve<MODE>(v, key, nullptr, 0);
 }
 
@@ -133,7 +138,8 @@ __device__ __forceinline__ int32_t resolve_from(const DevVolume& v, int4 raw, lo
     const int32_t bi = settle_home<MODE>(v, raw, key);
     if (bi != -2) return bi;
     return resolve_slow<MODE>(v.table, v.hash_mask, v.pool_capacity, v.block_count, v.drop_count,
-                              v.block_coord, v.status, key);
+                              v.block_coord, v.status, v.spin_limit, v.block_chunk, v.chunk, v.slot_index,
+                              key);
 }
 
 // Tag a block as touched by this update; the first tagger appends it to the

@@ -17,8 +17,9 @@ static_assert(sizeof(OsnTsdfDeviceView) == 104,
 
 struct OsnTsdfCudaVolume {
     Volume vol;
-    OsnTsdfCudaVolume(float voxel, int32_t pool, float trunc, float cap, uint32_t slots, int storage)
-        : vol(voxel, pool, trunc, cap, slots, storage) {}
+    OsnTsdfCudaVolume(float voxel, int32_t pool, float trunc, float cap, uint32_t slots, int storage,
+                      int layout)
+        : vol(voxel, pool, trunc, cap, slots, storage, layout) {}
 };
 
 namespace {
@@ -68,12 +69,20 @@ OsnTsdfCudaVolume* osn_tsdf_cuda_create(float voxel_size_m, int32_t pool_capacit
 OsnTsdfCudaVolume* osn_tsdf_cuda_create_ex(float voxel_size_m, int32_t pool_capacity_blocks,
                                            float trunc_m, float weight_cap, uint32_t hash_slots,
                                            int32_t storage) {
+    return osn_tsdf_cuda_create_layout(voxel_size_m, pool_capacity_blocks, trunc_m, weight_cap, hash_slots,
+                                       storage, OSN_TSDF_LAYOUT_POOL);
+}
+
+OsnTsdfCudaVolume* osn_tsdf_cuda_create_layout(float voxel_size_m, int32_t pool_capacity_blocks,
+                                               float trunc_m, float weight_cap, uint32_t hash_slots,
+                                               int32_t storage, int32_t layout) {
     if (storage != OSN_TSDF_STORAGE_FP32 && storage != OSN_TSDF_STORAGE_FP16_U16 &&
         storage != OSN_TSDF_STORAGE_FP64)
         return nullptr;
+    if (layout != OSN_TSDF_LAYOUT_POOL && layout != OSN_TSDF_LAYOUT_SLOT_INDEX) return nullptr;
     if (!(voxel_size_m > 0.0f) || pool_capacity_blocks <= 0) return nullptr;
     auto* v = new (std::nothrow) OsnTsdfCudaVolume(voxel_size_m, pool_capacity_blocks, trunc_m,
-                                                   weight_cap, hash_slots, storage);
+                                                   weight_cap, hash_slots, storage, layout);
     if (!v) return nullptr;
     if (!v->vol.ok()) {
         delete v;
@@ -110,6 +119,10 @@ int32_t osn_tsdf_cuda_device_view(const OsnTsdfCudaVolume* v, OsnTsdfDeviceView*
 
 int32_t osn_tsdf_cuda_storage(const OsnTsdfCudaVolume* v) {
     return usable(v) ? v->vol.storage() : -1;
+}
+
+int32_t osn_tsdf_cuda_layout(const OsnTsdfCudaVolume* v) {
+    return usable(v) ? v->vol.layout() : -1;
 }
 
 int32_t osn_tsdf_cuda_allocate_blocks(OsnTsdfCudaVolume* v, const float* d_positions,
@@ -322,6 +335,11 @@ void osn_tsdf_cuda_synchronize(const OsnTsdfCudaVolume* v) {
 
 uint32_t osn_tsdf_cuda_status(const OsnTsdfCudaVolume* v) {
     return usable(v) ? const_cast<OsnTsdfCudaVolume*>(v)->vol.status() : 0u;
+}
+
+int32_t osn_tsdf_cuda_set_spin_limit(OsnTsdfCudaVolume* v, int32_t iterations) {
+    if (!usable(v)) return 1;
+    return v->vol.set_spin_limit(iterations) ? 0 : 1;
 }
 
 int32_t osn_tsdf_cuda_set_pipelined(OsnTsdfCudaVolume* v, int32_t enabled) {

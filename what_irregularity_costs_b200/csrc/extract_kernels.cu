@@ -107,9 +107,28 @@ __device__ __forceinline__ Vert interp(const Halo<COL>& h, const Cube& q, float 
     return o;
 }
 
+// Where a CTA's vertices go: the block's output range is contiguous, so its
+// first kStageVerts vertices are staged in shared memory (with the range's
+// offset inside its 16-byte group, so the copy-out is aligned) and written
+// out by the whole CTA with 16-byte streaming stores; any further vertices
+// of an unusually dense block go straight to global memory. The instance
+// with colours stages fewer (its halo holds the colours too).
+template <bool COL>
+__host__ __device__ constexpr int stage_verts() { return COL ? 1024 : 1536; }
+template <bool COL>
+struct VertexSink {
+    float* stage;     // shared: [pad + stage_verts * 6]
+    int pad;          // floats of the 16-byte group before the block's first vertex
+    float* posnor;    // global output
+    int64_t base;     // the block's first vertex in the output
+    __device__ __forceinline__ float* slot(int local) const {
+        return local < stage_verts<COL>() ? stage + pad + local * 6 : posnor + (base + local) * 6;
+    }
+};
+
 template <bool COL>
 __device__ __forceinline__ void emit_triangle(const Vert& a, const Vert& b, const Vert& c,
-                                              float* posnor, uint8_t* rgb, int64_t at) {
+                                              const VertexSink<COL>& out, uint8_t* rgb, int local) {
     // marching_tets.cpp:206-218: face normal of the emitted triangle.
     const float e1[3] = {__fsub_rn(b.p[0], a.p[0]), __fsub_rn(b.p[1], a.p[1]), __fsub_rn(b.p[2], a.p[2])};
     const float e2[3] = {__fsub_rn(c.p[0], a.p[0]), __fsub_rn(c.p[1], a.p[1]), __fsub_rn(c.p[2], a.p[2])};
@@ -125,7 +144,7 @@ __device__ __forceinline__ void emit_triangle(const Vert& a, const Vert& b, cons
     }
     const Vert* vs[3] = {&a, &b, &c};
     for (int k = 0; k < 3; ++k) {
-        float* dst = posnor + (at + k) * 6;
+        float* dst = out.slot(local + k);
         dst[0] = vs[k]->p[0];
         dst[1] = vs[k]->p[1];
         dst[2] = vs[k]->p[2];
@@ -133,7 +152,7 @@ __device__ __forceinline__ void emit_triangle(const Vert& a, const Vert& b, cons
         dst[4] = ny;
         dst[5] = nz;
         if constexpr (COL) {
-            uint8_t* cc = rgb + (at + k) * 3;
+            uint8_t* cc = rgb + (out.base + local + k) * 3;
             cc[0] = (uint8_t)fminf(fmaxf(vs[k]->c[0], 0.0f), 255.0f);
             cc[1] = (uint8_t)fminf(fmaxf(vs[k]->c[1], 0.0f), 255.0f);
             cc[2] = (uint8_t)fminf(fmaxf(vs[k]->c[2], 0.0f), 255.0f);
@@ -149,15 +168,16 @@ __device__ __forceinline__ void emit_triangle(const Vert& a, const Vert& b, cons
 #endif
 template <int S, bool COL>
 __global__ void __launch_bounds__(kExtractThreads, COL ? 1 : OSN_EXTRACT_MIN_BLOCKS)
-extract_kernel(DevVolume v, int32_t n_blocks, float min_w, float iso, float* out_posnor,
+extract_kernel(DevVolume v, int32_t n_blocks, const int32_t* list, float min_w, float iso, float* out_posnor,
                uint8_t* out_rgb, int32_t cap, int32_t* ctl) {
     __shared__ Halo<COL> h;
+    __shared__ __align__(16) float s_stage[4 + stage_verts<COL>() * 6];
     __shared__ int s_nb[8];
     __shared__ int s_warp[kExtractThreads / 32];
-    __shared__ int s_base;
+    __shared__ int s_base, s_total;
 
-    const int b = blockIdx.x;
-    if (b >= n_blocks) return;
+    if ((int)blockIdx.x >= n_blocks) return;
+    const int b = list ? list[blockIdx.x] : (int)blockIdx.x;  // the block's pool index
     const int t = threadIdx.x;
     const BlockCoord bc = v.block_coord[b];
     if (t < 8) {
@@ -176,10 +196,12 @@ extract_kernel(DevVolume v, int32_t n_blocks, float min_w, float iso, float* out
         h.val[k] = 0.0f;
         if (nb >= 0) {
             const size_t idx = (size_t)nb * kBlockVoxels + (size_t)((((hz & 7) * kBlockDim) + (hy & 7)) * kBlockDim + (hx & 7));
+            // Weight and stored TSDF loaded together (one round trip).
             const float w = weight_at<S>(v, idx);
+            const float m = mean_from<S>(v, idx, w);
             if (!(w < min_w || w <= 0.0f)) {
                 ok = 1;
-                h.val[k] = mean_at<S>(v, idx, w);
+                h.val[k] = m;
                 if constexpr (COL) {
                     if constexpr (S == kStoreF32) {
                         const float inv = __fdiv_rn(1.0f, w);
@@ -253,11 +275,20 @@ extract_kernel(DevVolume v, int32_t n_blocks, float min_w, float iso, float* out
                 }
             }
             s_base = base;
+            s_total = total;
         }
     }
     __syncthreads();
-    if (s_base < 0 || n_vert == 0) return;
-    int64_t at = (int64_t)s_base + (warp ? s_warp[warp - 1] : 0) + x - n_vert;
+    const int total = s_total;
+    if (s_base < 0 || total == 0) return;  // uniform across the CTA
+    VertexSink<COL> sink;
+    sink.stage = s_stage;
+    // The caller's buffer is float-aligned, not necessarily 16-byte aligned:
+    // the pad is taken from the address of the block's first float.
+    sink.pad = (int)((reinterpret_cast<uintptr_t>(out_posnor + (int64_t)s_base * 6) >> 2) & 3);
+    sink.posnor = out_posnor;
+    sink.base = s_base;
+    int at = (warp ? s_warp[warp - 1] : 0) + x - n_vert;  // block-relative
 
     for (int k = 0; k < 6; ++k) {
         const int* tq = c_tets[k];
@@ -269,16 +300,34 @@ extract_kernel(DevVolume v, int32_t n_blocks, float min_w, float iso, float* out
             const Vert v0 = interp(h, q, iso, a, bb);
             const Vert v1 = interp(h, q, iso, a, c);
             const Vert v2 = interp(h, q, iso, a, d);
-            emit_triangle<COL>(v0, v1, v2, out_posnor, out_rgb, at);
+            emit_triangle<COL>(v0, v1, v2, sink, out_rgb, at);
             at += 3;
         } else if (kind == 2) {
             const Vert ac = interp(h, q, iso, a, c);
             const Vert ad = interp(h, q, iso, a, d);
             const Vert bd = interp(h, q, iso, bb, d);
             const Vert bcv = interp(h, q, iso, bb, c);
-            emit_triangle<COL>(ac, ad, bd, out_posnor, out_rgb, at);
-            emit_triangle<COL>(ac, bd, bcv, out_posnor, out_rgb, at + 3);
+            emit_triangle<COL>(ac, ad, bd, sink, out_rgb, at);
+            emit_triangle<COL>(ac, bd, bcv, sink, out_rgb, at + 3);
             at += 6;
+        }
+    }
+    __syncthreads();
+    // Copy-out of the staged vertices: 16-byte groups of the output, each
+    // wholly inside the block's range stored as one vector, the partial
+    // first and last groups float by float.
+    const int n_floats = min(total, stage_verts<COL>()) * 6;
+    // The 16-byte group holding the block's first float; only floats of the
+    // block's range [pad, pad + n_floats) are written.
+    float* gbase = reinterpret_cast<float*>(reinterpret_cast<uintptr_t>(out_posnor + (int64_t)s_base * 6) -
+                                            4 * (uintptr_t)sink.pad);
+    const int groups = (sink.pad + n_floats + 3) >> 2;
+    for (int g = t; g < groups; g += kExtractThreads) {
+        const int lo = 4 * g;
+        if (lo >= sink.pad && lo + 4 <= sink.pad + n_floats) {
+            __stcs(reinterpret_cast<float4*>(gbase) + g, reinterpret_cast<const float4*>(s_stage)[g]);
+        } else {
+            for (int j = max(lo, sink.pad); j < min(lo + 4, sink.pad + n_floats); ++j) gbase[j] = s_stage[j];
         }
     }
 }
@@ -288,6 +337,44 @@ __global__ void reset_table_kernel(HashEntry* table, uint32_t count, long long k
         table[k].key = key;
         table[k].block_idx = -1;
         table[k].pad = 0;
+    }
+}
+
+// Every occupied slot of the table (slot-index layout: the slot is the
+// block's pool index), appended warp by warp.
+__global__ void list_blocks_kernel(const HashEntry* table, uint32_t size, int32_t* out, int32_t* count) {
+    for (uint32_t base = blockIdx.x * blockDim.x; base < size; base += gridDim.x * blockDim.x) {
+        const uint32_t k = base + threadIdx.x;
+        bool occ = false;
+        if (k < size) {
+            const int4 raw = reinterpret_cast<const int4*>(table)[k];
+            const long long key = ((long long)(unsigned)raw.y << 32) | (unsigned)raw.x;
+            occ = key >= 0 && raw.z == (int)k;
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, occ);
+        int at = 0;
+        if ((threadIdx.x & 31) == 0 && m) at = atomicAdd(count, __popc(m));
+        at = __shfl_sync(0xffffffffu, at, 0);
+        if (occ) out[at + __popc(m & lanemask_lt())] = (int32_t)k;
+    }
+}
+
+// Zero the voxels of the blocks of a list, one CTA per block.
+__global__ void reset_listed_kernel(DevVolume v, const int32_t* list, int32_t n) {
+    const int32_t i = blockIdx.x;
+    if (i >= n) return;
+    const size_t b = (size_t)list[i];
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+    const int n_t = kBlockVoxels * tsdf_bytes(v.storage) / 16;
+    const int n_w = kBlockVoxels * weight_bytes(v.storage) / 16;
+    for (int k = threadIdx.x; k < n_t; k += blockDim.x) {
+        reinterpret_cast<float4*>(v.tsdf)[b * n_t + k] = z;
+        if (k < n_w) reinterpret_cast<float4*>(v.weight)[b * n_w + k] = z;
+        if (v.storage == kStoreF32) {
+            reinterpret_cast<float4*>(v.r)[b * n_t + k] = z;
+            reinterpret_cast<float4*>(v.g)[b * n_t + k] = z;
+            reinterpret_cast<float4*>(v.b)[b * n_t + k] = z;
+        }
     }
 }
 
@@ -312,7 +399,7 @@ __global__ void reset_voxels_kernel(DevVolume v, size_t n_voxels) {
 
 }  // namespace
 
-cudaError_t launch_extract(const DevVolume& v, int32_t n_blocks, float min_w, float iso,
+cudaError_t launch_extract(const DevVolume& v, int32_t n_blocks, const int32_t* list, float min_w, float iso,
                            float* posnor, uint8_t* rgb, int32_t cap, int32_t* ctl, cudaStream_t s) {
     if (n_blocks <= 0) return cudaSuccess;
     // Colours in a separate instance: without them the halo holds a quarter
@@ -320,16 +407,16 @@ cudaError_t launch_extract(const DevVolume& v, int32_t n_blocks, float min_w, fl
     const bool col = rgb != nullptr;
     switch (v.storage) {
         case kStoreF16U16:
-            if (col) extract_kernel<kStoreF16U16, true><<<n_blocks, kExtractThreads, 0, s>>>(v, n_blocks, min_w, iso, posnor, rgb, cap, ctl);
-            else extract_kernel<kStoreF16U16, false><<<n_blocks, kExtractThreads, 0, s>>>(v, n_blocks, min_w, iso, posnor, nullptr, cap, ctl);
+            if (col) extract_kernel<kStoreF16U16, true><<<n_blocks, kExtractThreads, 0, s>>>(v, n_blocks, list, min_w, iso, posnor, rgb, cap, ctl);
+            else extract_kernel<kStoreF16U16, false><<<n_blocks, kExtractThreads, 0, s>>>(v, n_blocks, list, min_w, iso, posnor, nullptr, cap, ctl);
             break;
         case kStoreF64:
-            if (col) extract_kernel<kStoreF64, true><<<n_blocks, kExtractThreads, 0, s>>>(v, n_blocks, min_w, iso, posnor, rgb, cap, ctl);
-            else extract_kernel<kStoreF64, false><<<n_blocks, kExtractThreads, 0, s>>>(v, n_blocks, min_w, iso, posnor, nullptr, cap, ctl);
+            if (col) extract_kernel<kStoreF64, true><<<n_blocks, kExtractThreads, 0, s>>>(v, n_blocks, list, min_w, iso, posnor, rgb, cap, ctl);
+            else extract_kernel<kStoreF64, false><<<n_blocks, kExtractThreads, 0, s>>>(v, n_blocks, list, min_w, iso, posnor, nullptr, cap, ctl);
             break;
         default:
-            if (col) extract_kernel<kStoreF32, true><<<n_blocks, kExtractThreads, 0, s>>>(v, n_blocks, min_w, iso, posnor, rgb, cap, ctl);
-            else extract_kernel<kStoreF32, false><<<n_blocks, kExtractThreads, 0, s>>>(v, n_blocks, min_w, iso, posnor, nullptr, cap, ctl);
+            if (col) extract_kernel<kStoreF32, true><<<n_blocks, kExtractThreads, 0, s>>>(v, n_blocks, list, min_w, iso, posnor, rgb, cap, ctl);
+            else extract_kernel<kStoreF32, false><<<n_blocks, kExtractThreads, 0, s>>>(v, n_blocks, list, min_w, iso, posnor, nullptr, cap, ctl);
             break;
     }
     return cudaGetLastError();
@@ -342,8 +429,19 @@ cudaError_t launch_reset_table(HashEntry* first, uint32_t count, long long key, 
     return cudaGetLastError();
 }
 
-cudaError_t launch_reset_voxels(const DevVolume& v, int32_t n_blocks, cudaStream_t s) {
+cudaError_t launch_list_blocks(const DevVolume& v, int32_t* out, int32_t* count, cudaStream_t s) {
+    const uint32_t size = v.hash_mask + 1;
+    const int grid = (int)std::min<uint32_t>((size + 255) / 256, 148u * 8u);
+    list_blocks_kernel<<<grid, 256, 0, s>>>(v.table, size, out, count);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_reset_voxels(const DevVolume& v, int32_t n_blocks, const int32_t* list, cudaStream_t s) {
     if (n_blocks <= 0) return cudaSuccess;
+    if (list) {
+        reset_listed_kernel<<<n_blocks, 128, 0, s>>>(v, list, n_blocks);
+        return cudaGetLastError();
+    }
     const size_t n_voxels = (size_t)n_blocks * kBlockVoxels;
     const size_t n_vec = n_voxels * (size_t)tsdf_bytes(v.storage) / 16;
     const int grid = (int)std::min<size_t>((n_vec + 255) / 256, (size_t)148 * 16);

@@ -18,29 +18,33 @@
 //
 // The band walk (band_kernels.cu) has left, per voxel, the batch count n and
 // the fixed-point sum of the records' normalised SDFs, the list of touched
-// blocks, and one record per band slot.
+// blocks, and per band slot a record (the voxel) and the normalised SDF.
 //
-//   finish     one 128-thread CTA per touched block, 4 voxels per thread,
-//              every array read and written as 128-bit vectors: a voxel that
-//              accepts all of its records (keep == n, the common case) gets
-//              tsdf + sum, w0 + n, 128 * (w0 + n) and its count and sum back
-//              to zero. A voxel that crosses the cap inside the batch
-//              reserves a group of n deferred records instead and its block
-//              is tagged.
-//              Crossing voxels go to one of two lists: small groups (at most
-//              kLaneRecords records, most of them) and large ones.
-//   group      one pass over the records of the batch, eight per thread: a
-//              record of a tagged block whose voxel reserved a group takes
-//              the next place of the group (a few percent of the records).
-//   values     (FP64 oracle only) one thread per grouped record: its
-//              canonical id and its normalised SDF recomputed in double from
-//              its point. FP32 / FP16 records carry their band slot, from
-//              which deferred reads the id and the value the walk kept.
-//   deferred   selects the keep records with the smallest ids of every
-//              crossing voxel and finishes it: one half-warp per small group
-//              (one record per lane, shuffle ranking), one warp per large group
-//              (register ranking up to 256 records, a radix select of the
-//              keep-th id beyond that).
+//   finish   one 128-thread CTA per touched block (two per CTA pass), 4
+//            voxels per thread, every array read and written as 128-bit
+//            vectors: a voxel that accepts all of its records (keep == n,
+//            the common case) gets tsdf + sum, w0 + n, 128 * (w0 + n) and
+//            its count and sum back to zero. A voxel that crosses the cap
+//            inside the batch instead reserves a group of n places (one
+//            warp-aggregated atomic), keeps the group's base in its sum word
+//            and n in its count word, and sets its bit in the block's
+//            crossing bitmap (16 words per block, rewritten for every block
+//            finish visits).
+//   group    one pass over the band slots of the batch, eight per thread
+//            (records and normalised SDFs loaded as 128-bit vectors): a
+//            record whose voxel's bit is set takes the next place of the
+//            voxel's group (atomic add on the sum word) and stores its
+//            canonical id and value there, then counts the voxel's pending
+//            records down with an acquire-release atomic. The record that
+//            brings the count to zero is the last of its group: its warp
+//            loads the whole group, keeps the keep records with the smallest
+//            ids (shuffle ranking in registers up to 256 records, a radix
+//            select beyond) and finishes the voxel. No pass runs between the
+//            grouping and the selection.
+//
+// The FP64 oracle storage keeps no per-slot values: its group entries hold
+// the band slot, and the selection recomputes each record's normalised SDF
+// in double from its point.
 //
 // Sums are 64-bit fixed point added to the stored sum with one rounding, so
 // results do not depend on the order in which threads meet the records:
@@ -55,12 +59,11 @@ namespace {
 
 constexpr int kFinishThreads = 128;  // 4 voxels per thread, one block per CTA pass
 constexpr int kGroupThreads = 256;
-constexpr int kDeferThreads = 128;
-constexpr int kDeferWarps = kDeferThreads / 32;
-constexpr int kRankRegs = 8;
-static_assert(kFinishThreads >= kMaxBatchScenes && kGroupThreads >= kMaxBatchScenes &&
-                  kDeferThreads >= kMaxBatchScenes,
-              "one thread per scene builds the item prefix");  // crossing voxels of up to 256 records are ranked in registers
+constexpr int kGroupWarps = kGroupThreads / 32;
+constexpr int kGroupPerThread = 8;  // band slots per thread (two 128-bit loads)
+constexpr int kRankRegs = 8;        // groups of up to 32 * 8 records are ranked in registers
+static_assert(kFinishThreads >= kMaxBatchScenes && kGroupThreads >= kMaxBatchScenes,
+              "one thread per scene builds the item prefix");
 
 // Contributions a voxel accepts given its weight w0 before the batch and n
 // unit-weight records: the j-th record (0-based, canonical order) is accepted
@@ -71,6 +74,15 @@ __device__ __forceinline__ int accept_count(float w0, float cap, int n) {
     if (w0 >= cap) return 0;
     const double room = ceil((double)cap - (double)w0);
     return room >= (double)n ? n : (int)room;
+}
+
+// Atomic add with acquire-release semantics at GPU scope: the caller's
+// earlier stores are visible to whoever reads the result of a later add to
+// the same word, and the caller sees what earlier adders stored.
+__device__ __forceinline__ uint32_t atom_add_acq_rel(uint32_t* p, uint32_t x) {
+    uint32_t old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(x) : "memory");
+    return old;
 }
 
 // ---- finish ----------------------------------------------------------------
@@ -167,69 +179,52 @@ __device__ __forceinline__ void cta_add(int* smem_acc, int mine, int* global) {
 }
 
 // One touched block's quad of voxels, its arrays already loaded: finish
-// the voxels that accept all their records, reserve groups for those that
+// the voxels that accept all their records, open groups for those that
 // cross the cap. Warp-synchronous (all lanes of the warp call it).
 template <int S>
 __device__ __forceinline__ void finish_quad(const DevVolume& v, const UpdateScratch& u, int32_t bi,
                                             size_t q4, int t, int lane, const uint4 c4, Quad<S>& x,
                                             const ulonglong2 a01, const ulonglong2 a23, int& updated) {
     const bool any = (c4.x | c4.y | c4.z | c4.w) != 0u;
-    if (!__any_sync(0xffffffffu, any)) return;  // warp-uniform skip
+    // Warp-uniform skip: no record of this update names these 128 voxels, so
+    // the group pass never reads their crossing bits either.
+    if (!__any_sync(0xffffffffu, any)) return;
     const uint32_t n[4] = {c4.x, c4.y, c4.z, c4.w};
     unsigned long long acc[4] = {a01.x, a01.y, a23.x, a23.y};
     uint32_t cnt[4] = {0u, 0u, 0u, 0u};
     int keepv[4] = {0, 0, 0, 0};
-    // Voxels crossing the cap reserve a group of their n records and an
-    // entry in the small (n <= kLaneRecords) or large list; the warp's
-    // reservations are summed and made with one atomic per counter.
-    uint32_t my_records = 0u;
-    uint32_t my_small = 0u, my_large = 0u;
+    // Voxels crossing the cap reserve n places each; the warp's reservations
+    // are summed and made with one atomic.
+    uint32_t my_records = 0u, my_cross = 0u;
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         if (n[q] == 0u) continue;
         keepv[q] = accept_count(x.w[q], v.weight_cap, (int)n[q]);
         if (keepv[q] != 0 && (uint32_t)keepv[q] != n[q]) {
             my_records += n[q];
-            if (n[q] <= (uint32_t)kLaneRecords) ++my_small;
-            else ++my_large;
+            ++my_cross;
         }
     }
-    const unsigned crossers = __ballot_sync(0xffffffffu, my_records > 0u);
-    uint32_t rec_base = 0u, small_at = 0u, large_at = 0u;
-    bool lists_ok = true;
-    if (crossers) {
-        uint32_t rec_incl = my_records, s_incl = my_small, l_incl = my_large;
+    uint32_t rec_base = 0u;
+    if (__ballot_sync(0xffffffffu, my_records > 0u)) {
+        uint32_t rec_incl = my_records, x_incl = my_cross;
         for (int o = 1; o < 32; o <<= 1) {
             const uint32_t ry = __shfl_up_sync(0xffffffffu, rec_incl, o);
-            const uint32_t sy = __shfl_up_sync(0xffffffffu, s_incl, o);
-            const uint32_t ly = __shfl_up_sync(0xffffffffu, l_incl, o);
+            const uint32_t xy = __shfl_up_sync(0xffffffffu, x_incl, o);
             if (lane >= o) {
                 rec_incl += ry;
-                s_incl += sy;
-                l_incl += ly;
+                x_incl += xy;
             }
         }
         uint32_t rb = 0u;
-        unsigned long long lb = 0ull;
         if (lane == 31) {
             rb = atomicAdd(&u.ctl->x_used, rec_incl);
-            lb = atomicAdd(&u.ctl->def_lists, (unsigned long long)s_incl |
-                                                  ((unsigned long long)l_incl << 32));
+            atomicAdd(&u.ctl->n_crossing, (unsigned long long)x_incl);
         }
         rb = __shfl_sync(0xffffffffu, rb, 31);
-        lb = __shfl_sync(0xffffffffu, lb, 31);
-        const uint32_t s_tot = __shfl_sync(0xffffffffu, s_incl, 31);
-        const uint32_t l_tot = __shfl_sync(0xffffffffu, l_incl, 31);
         rec_base = rb + rec_incl - my_records;
-        const uint64_t s0 = lb & 0xFFFFFFFFull, l0 = lb >> 32;
-        small_at = (uint32_t)s0 + s_incl - my_small;
-        large_at = (uint32_t)l0 + l_incl - my_large;
-        // The lists grow towards each other: entries written under a
-        // reservation that fits never overlap later ones.
-        lists_ok = s0 + s_tot + l0 + l_tot <= (uint64_t)u.dvox_cap;
     }
-    if (!any) return;  // no warp-synchronous step follows
-    bool crossing = false;
+    uint32_t xmask = 0u;  // bit q: voxel 4t + q crosses the cap
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         if (n[q] == 0u) continue;
@@ -241,33 +236,43 @@ __device__ __forceinline__ void finish_quad(const DevVolume& v, const UpdateScra
             }
             acc[q] = 0ull;
         } else {
-            // Crosses the cap: its group is filled by the group pass and
-            // the voxel finished by the deferred kernel.
-            const uint32_t vi = (uint32_t)bi * kBlockVoxels + 4u * t + q;
-            const bool small = n[q] <= (uint32_t)kLaneRecords;
-            const int entry = small ? (int)small_at : u.dvox_cap - 1 - (int)large_at;
-            if ((uint64_t)rec_base + n[q] <= (uint64_t)u.record_cap && lists_ok) {
-                u.dvox[entry] = make_int4((int)vi, (int)rec_base, (int)n[q], keepv[q]);
-                acc[q] = (unsigned long long)(rec_base + 1u) << 32;  // low half: fill ticket
+            // Crosses the cap: the group pass places its records and the
+            // last of them finishes it. The sum word holds the group's base
+            // + 1 (high half) and the next free place (low half); the count
+            // word the records still to be placed.
+            if ((uint64_t)rec_base + n[q] <= (uint64_t)u.record_cap) {
+                acc[q] = (unsigned long long)(rec_base + 1u) << 32;
                 cnt[q] = n[q];
+                xmask |= 1u << q;
             } else {
-                // Out of scratch (the status word says so): a reserved
-                // list entry still gets an empty group, never a stale one.
-                if (lists_ok) u.dvox[entry] = make_int4((int)vi, 0, 0, 0);
+                // Out of scratch (only after a failed update left stale
+                // counters): the voxel's records are dropped, the status
+                // word says so.
                 atomicOr(v.status, kStatusScratchOverflow);
                 acc[q] = 0ull;
             }
             rec_base += n[q];
-            if (small) ++small_at;
-            else ++large_at;
-            crossing = true;
         }
     }
-    if (crossing) u.blk_cross[bi] = u.tag;
+    // The block's crossing bitmap: voxel 32w + j is bit j of word w, and the
+    // four voxels of thread t are bits 4(t % 8) .. 4(t % 8) + 3 of word t / 8.
+    uint32_t bits = xmask << (4 * (t & 7));
+    bits |= __shfl_xor_sync(0xffffffffu, bits, 1);
+    bits |= __shfl_xor_sync(0xffffffffu, bits, 2);
+    bits |= __shfl_xor_sync(0xffffffffu, bits, 4);
+    if ((t & 7) == 0) u.xbits[(size_t)bi * kXWords + (t >> 3)] = bits;
+    if (!any) return;
     store_quad<S>(v, q4, x);
     reinterpret_cast<uint4*>(u.vcnt)[q4] = make_uint4(cnt[0], cnt[1], cnt[2], cnt[3]);
     reinterpret_cast<ulonglong2*>(u.vacc)[2 * q4] = make_ulonglong2(acc[0], acc[1]);
     reinterpret_cast<ulonglong2*>(u.vacc)[2 * q4 + 1] = make_ulonglong2(acc[2], acc[3]);
+}
+
+// A touched block now belongs to the current call's chunk.
+__device__ __forceinline__ void tag_chunk(const DevVolume& v, int32_t ba, int32_t bb, bool has_b) {
+    if (!v.block_chunk) return;
+    v.block_chunk[ba] = v.chunk;
+    if (has_b) v.block_chunk[bb] = v.chunk;
 }
 
 template <int S>
@@ -305,118 +310,62 @@ finish_kernel(DevVolume v, UpdateScratch u) {
         ulonglong2 a01, a23, b01, b23;
         load_item<S>(v, u, qa, ca, xa, a01, a23);
         if (has_b) load_item<S>(v, u, qb, cb, xb, b01, b23);
+        if (t == 0) tag_chunk(v, ba, bb, has_b);
         finish_quad<S>(v, u, ba, qa, t, lane, ca, xa, a01, a23, updated);
         if (has_b) finish_quad<S>(v, u, bb, qb, t, lane, cb, xb, b01, b23, updated);
     }
     cta_add(&s_updated, updated, &u.ctl->n_updated);
 }
 
-// ---- group ---------------------------------------------------------------
+// ---- group and select ------------------------------------------------------
 
-// Canonical id and normalised SDF (2^-40 fixed point) of the record in band
-// slot `slot`: the value the band walk kept for the slot (the FP64 oracle
-// recomputes it from the point in double, with the walk's arithmetic).
-template <int S>
-__device__ __forceinline__ uint32_t slot_record(const DevVolume& v, const BatchArgs& a,
-                                                const UpdateScratch& u, uint32_t slot, long long& fix) {
+// Canonical id of band slot `slot` (point i at step s sits at s * n + i):
+// i * (2 * steps + 1) + s, the position of the sample in (point, step) order.
+__device__ __forceinline__ uint32_t slot_id(uint32_t slot, uint32_t n_pts, uint32_t n_steps) {
+    const uint32_t s = slot / n_pts, i = slot - s * n_pts;
+    return i * n_steps + s;
+}
+
+// The FP64 oracle's canonical id and normalised SDF (2^-40 fixed point) of
+// the record in band slot `slot`, recomputed in double from its point with
+// the walk's sample (the same voxel, so the same accepted set).
+__device__ __forceinline__ uint32_t slot_record_f64(const DevVolume& v, const BatchArgs& a, uint32_t slot,
+                                                    long long& fix) {
     const uint32_t n_steps = 2u * (uint32_t)v.steps + 1u;
     if (a.n <= 0) {  // no batch: nothing to recompute (never a valid record)
         fix = 0;
         return 0xFFFFFFFFu;
     }
     const uint32_t s = slot / (uint32_t)a.n, i = slot - s * (uint32_t)a.n;
-    if constexpr (S != kStoreF64) {
-        // The band walk kept the slot's normalised SDF: no point is read again.
-        fix = to_fix(u.slot_val[slot]);
-        return i * n_steps + s;
-    }
     Ray r;
     int vx = 0, vy = 0, vz = 0;
     float sdf = 0.0f;
     const bool ok = ray_setup(a, (int)i, r);
     if (ok) band_sample(v, a, r, (int)s - v.steps, vx, vy, vz, sdf);
-    if constexpr (S == kStoreF64) {
-        fix = ok ? to_fix(clamp_sdf_n_f64(sdf_f64(v, a, r.px, r.py, r.pz, vx, vy, vz), v.trunc)) : 0ll;
-    } else {
-        fix = to_fix(fminf(fmaxf(__fmul_rn(sdf, v.inv_trunc), -1.0f), 1.0f));
-    }
+    fix = ok ? to_fix(clamp_sdf_n_f64(sdf_f64(v, a, r.px, r.py, r.pz, vx, vy, vz), v.trunc)) : 0ll;
     return i * n_steps + s;
 }
 
-constexpr int kGroupPerThread = 8;  // records per thread (two 128-bit loads)
-
-// Eight band slots from `first` of one batch: records of voxels that
-// reserved a group take the next place of the group.
-__device__ __forceinline__ void group_slots(const UpdateScratch& u, uint32_t first, uint32_t n_slots) {
-    // Eight consecutive band slots per thread (same step, neighbouring points,
-    // so mostly the same block): the block-tag gathers of distinct blocks in
-    // flight together, then the (rare) records of crossing voxels take the
-    // next place of their voxel's group with their band slot.
-    if (first >= n_slots) return;
-    uint32_t vi[kGroupPerThread];
-    if (first + kGroupPerThread <= n_slots) {
-        const uint4 r0 = __ldcs(reinterpret_cast<const uint4*>(u.records + first));
-        const uint4 r1 = __ldcs(reinterpret_cast<const uint4*>(u.records + first) + 1);
-        vi[0] = r0.x; vi[1] = r0.y; vi[2] = r0.z; vi[3] = r0.w;
-        vi[4] = r1.x; vi[5] = r1.y; vi[6] = r1.z; vi[7] = r1.w;
-    } else {
-#pragma unroll
-        for (int m = 0; m < kGroupPerThread; ++m)
-            vi[m] = first + m < n_slots ? u.records[first + m] : kNoVoxel;
-    }
-    uint32_t tag[kGroupPerThread];
-    bool same[kGroupPerThread];  // same block as the previous slot: reuse its tag
-#pragma unroll
-    for (int m = 0; m < kGroupPerThread; ++m) {
-        const uint32_t blk = vi[m] / kBlockVoxels;
-        same[m] = m > 0 && vi[m] != kNoVoxel && vi[m - 1] != kNoVoxel && vi[m - 1] / kBlockVoxels == blk;
-        tag[m] = (vi[m] == kNoVoxel || same[m]) ? 0u : u.blk_cross[blk];
-    }
-#pragma unroll
-    for (int m = 1; m < kGroupPerThread; ++m)
-        if (same[m]) tag[m] = tag[m - 1];
-    uint32_t hi[kGroupPerThread];
-#pragma unroll
-    for (int m = 0; m < kGroupPerThread; ++m)
-        hi[m] = (vi[m] != kNoVoxel && tag[m] == u.tag) ? (uint32_t)(u.vacc[vi[m]] >> 32) : 0u;
-#pragma unroll
-    for (int m = 0; m < kGroupPerThread; ++m) {
-        if (hi[m] == 0u) continue;  // not a voxel that reserved a group
-        const uint32_t tk = (uint32_t)atomicAdd(&u.vacc[vi[m]], 1ull);
-        if (tk < u.vcnt[vi[m]]) u.deferred[(size_t)(hi[m] - 1u) + tk] = first + m;
-        else atomicOr(u.status, kStatusScratchOverflow);  // state left by a failed update
-    }
-}
-
-__global__ void __launch_bounds__(kGroupThreads)
-group_kernel(UpdateScratch u, uint32_t n_slots) {
-    launch_dependents();
-    grid_dependency_wait();
-    if (u.ctl->def_lists == 0ull) return;  // no voxel crossed the cap in this batch
-    group_slots(u, (blockIdx.x * kGroupThreads + threadIdx.x) * kGroupPerThread, n_slots);
-}
-
-// ---- values --------------------------------------------------------------
-
-// One thread per grouped record: its band slot becomes its canonical id and
-// its normalised SDF (recomputed from the point, the walk's arithmetic with
-// the same rounding; the FP64 oracle's value in double).
+// Id and value of a group entry: (id | normalised SDF bits << 32) as the
+// group pass stored it, or, for the FP64 oracle, its band slot.
 template <int S>
-__global__ void __launch_bounds__(kGroupThreads)
-values_kernel(DevVolume v, BatchArgs a, UpdateScratch u) {
-    launch_dependents();
-    grid_dependency_wait();
-    if (u.ctl->def_lists == 0ull) return;
-    const uint32_t n = (uint32_t)min((long long)u.ctl->x_used, (long long)u.record_cap);
-    for (uint32_t k = blockIdx.x * kGroupThreads + threadIdx.x; k < n; k += gridDim.x * kGroupThreads) {
-        long long fix;
-        const uint32_t id = slot_record<S>(v, a, u, u.deferred[k], fix);
-        u.deferred[k] = id;
-        u.deferred_fix[k] = fix;
+__device__ __forceinline__ void entry_record(const DevVolume& v, const BatchArgs& a, unsigned long long e,
+                                             uint32_t& id, long long& fix) {
+    if constexpr (S == kStoreF64) {
+        id = slot_record_f64(v, a, (uint32_t)e, fix);
+    } else {
+        id = (uint32_t)e;
+        fix = to_fix(__uint_as_float((uint32_t)(e >> 32)));
     }
 }
 
-// ---- deferred ------------------------------------------------------------
+template <int S>
+__device__ __forceinline__ uint32_t entry_id(const DevVolume& v, const BatchArgs& a, unsigned long long e) {
+    if constexpr (S == kStoreF64)
+        return slot_id((uint32_t)e, (uint32_t)a.n, 2u * (uint32_t)v.steps + 1u);
+    else
+        return (uint32_t)e;
+}
 
 // Finish a cap-crossing voxel: keep contributions accepted, their values
 // summing to fix * 2^-40.
@@ -446,16 +395,54 @@ __device__ __forceinline__ void finish_voxel(const DevVolume& v, const UpdateScr
     u.vcnt[vi] = 0u;
 }
 
+// Sum of the accepted values of a group of at most 32 * R records, by one
+// warp: record r * 32 + lane in registers, ranked by id against every other
+// record with shuffles; a record is accepted when fewer than keep ids are
+// below its own. Ids are distinct and below 0xFFFFFFFF, so the padding
+// entries never rank below a record. Entries are read through L2: they were
+// stored by other threads of this grid.
+template <int S, int R>
+__device__ __forceinline__ long long rank_group(const DevVolume& v, const BatchArgs& a,
+                                                const unsigned long long* grp, int n, int keep, int lane) {
+    uint32_t id[R];
+    long long val[R];
+    int rank[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int k = r * 32 + lane;
+        id[r] = 0xFFFFFFFFu;
+        val[r] = 0ll;
+        rank[r] = 0;
+        if (k < n) entry_record<S>(v, a, __ldcg(grp + k), id[r], val[r]);
+    }
+#pragma unroll
+    for (int rr = 0; rr < R; ++rr) {
+        const int srcs = min(32, n - rr * 32);  // warp-uniform
+        for (int src = 0; src < srcs; ++src) {
+            const uint32_t other = __shfl_sync(0xffffffffu, id[rr], src);
+#pragma unroll
+            for (int r = 0; r < R; ++r) rank[r] += other < id[r] ? 1 : 0;
+        }
+    }
+    long long fix = 0ll;
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+        if (r * 32 + lane < n && rank[r] < keep) fix += val[r];
+    return fix;
+}
+
 // The keep-th smallest id (1-based) of a group, by four 8-bit radix passes
 // with a per-warp histogram. Ids are distinct, so exactly keep ids are <= it.
-__device__ uint32_t radix_select(const uint32_t* ids, int n, int keep, uint32_t* hist, int lane) {
+template <int S>
+__device__ uint32_t radix_select(const DevVolume& v, const BatchArgs& a, const unsigned long long* grp,
+                                 int n, int keep, uint32_t* hist, int lane) {
     uint32_t prefix = 0u, pmask = 0u;
     int need = keep;
     for (int shift = 24; shift >= 0; shift -= 8) {
         for (int b = lane; b < 256; b += 32) hist[b] = 0u;
         __syncwarp();
         for (int k = lane; k < n; k += 32) {
-            const uint32_t id = ids[k];
+            const uint32_t id = entry_id<S>(v, a, __ldcg(grp + k));
             if ((id & pmask) == prefix) atomicAdd(&hist[(id >> shift) & 255u], 1u);
         }
         __syncwarp();
@@ -495,156 +482,156 @@ __device__ uint32_t radix_select(const uint32_t* ids, int n, int keep, uint32_t*
     return prefix;
 }
 
-// Id and fixed-point value of the record at group position pos: as the values
-// pass left them (the FP64 oracle), or from the record's band slot (FP32 /
-// FP16 storage: id from the slot's point and step, value kept by the walk).
+// Sum of the accepted values of a group of more than 32 records, by one
+// warp.
 template <int S>
-__device__ __forceinline__ void group_record(const UpdateScratch& u, uint32_t n_pts, uint32_t n_steps,
-                                             uint32_t pos, uint32_t& id, long long& fix) {
-    if constexpr (S == kStoreF64) {
-        id = u.deferred[pos];
-        fix = u.deferred_fix[pos];
-    } else {
-        const uint32_t slot = u.deferred[pos];
-        const uint32_t st = slot / n_pts;
-        id = (slot - st * n_pts) * n_steps + st;
-        fix = to_fix(u.slot_val[slot]);
-    }
-}
-
-// A large group's records as (id, value) arrays in place, by the whole warp.
-template <int S>
-__device__ __forceinline__ void group_to_ids(const UpdateScratch& u, uint32_t n_pts, uint32_t n_steps,
-                                             uint32_t base, int n, int lane) {
-    if constexpr (S != kStoreF64) {
-        for (int k = lane; k < n; k += 32) {
-            uint32_t id;
-            long long fix;
-            group_record<S>(u, n_pts, n_steps, base + (uint32_t)k, id, fix);
-            u.deferred[base + k] = id;
-            u.deferred_fix[base + k] = fix;
-        }
-        __syncwarp();
-    }
-}
-
-// Sum of the accepted values of a group of at most 32 * R records, by one
-// warp: record r * 32 + lane in registers (id and value straight from its
-// band slot), ranked by id against every other record with shuffles; a record
-// is accepted when fewer than keep ids are below its own. Ids are distinct
-// and below 0xFFFFFFFF, so the padding entries never rank below a record.
-template <int S, int R>
-__device__ __forceinline__ long long rank_group(const UpdateScratch& u, uint32_t n_pts, uint32_t n_steps,
-                                                uint32_t base, int n, int keep, int lane) {
-    uint32_t id[R];
-    long long val[R];
-    int rank[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-        const int k = r * 32 + lane;
-        id[r] = 0xFFFFFFFFu;
-        val[r] = 0ll;
-        rank[r] = 0;
-        if (k < n) group_record<S>(u, n_pts, n_steps, base + (uint32_t)k, id[r], val[r]);
-    }
-#pragma unroll
-    for (int rr = 0; rr < R; ++rr) {
-#pragma unroll 8
-        for (int src = 0; src < 32; ++src) {
-            const uint32_t other = __shfl_sync(0xffffffffu, id[rr], src);
-#pragma unroll
-            for (int r = 0; r < R; ++r) rank[r] += other < id[r] ? 1 : 0;
-        }
-    }
+__device__ __forceinline__ long long large_group_sum(const DevVolume& v, const BatchArgs& a,
+                                                     const unsigned long long* grp, int n, int keep,
+                                                     uint32_t* hist, int lane) {
+    if (n <= 64) return rank_group<S, 2>(v, a, grp, n, keep, lane);
+    if (n <= 128) return rank_group<S, 4>(v, a, grp, n, keep, lane);
+    if (n <= 32 * kRankRegs) return rank_group<S, kRankRegs>(v, a, grp, n, keep, lane);
+    const uint32_t last = radix_select<S>(v, a, grp, n, keep, hist, lane);
     long long fix = 0ll;
-#pragma unroll
-    for (int r = 0; r < R; ++r)
-        if (r * 32 + lane < n && rank[r] < keep) fix += val[r];
+    for (int k = lane; k < n; k += 32) {
+        uint32_t id;
+        long long val;
+        entry_record<S>(v, a, __ldcg(grp + k), id, val);
+        if (id <= last) fix += val;
+    }
     return fix;
 }
 
-// Sum of the accepted values of a voxel of the large list (e = voxel, group
-// base, records, accepted), by one warp, on every lane: register ranking
-// sized to the group up to 256 records; beyond, the group's records become
-// (id, value) arrays in place and a radix select finds the keep-th id.
+// The same out of line for the storages whose entries carry their values
+// (no volume or batch needed), so the common small groups keep the pass's
+// registers.
 template <int S>
-__device__ long long large_group_sum(const UpdateScratch& u, uint32_t n_pts, uint32_t n_steps, const int4 e,
-                                     uint32_t* hist, int lane) {
-    const uint32_t base = (uint32_t)e.y;
-    const int n = e.z, keep = e.w;
-    long long fix;
-    if (n <= 32) {
-        fix = rank_group<S, 1>(u, n_pts, n_steps, base, n, keep, lane);
-    } else if (n <= 64) {
-        fix = rank_group<S, 2>(u, n_pts, n_steps, base, n, keep, lane);
-    } else if (n <= 128) {
-        fix = rank_group<S, 4>(u, n_pts, n_steps, base, n, keep, lane);
-    } else if (n <= 32 * kRankRegs) {
-        fix = rank_group<S, kRankRegs>(u, n_pts, n_steps, base, n, keep, lane);
+__device__ __noinline__ long long large_group_sum_out(const unsigned long long* grp, int n, int keep,
+                                                      uint32_t* hist, int lane) {
+    static_assert(S != kStoreF64, "the FP64 oracle recomputes values from its batch");
+    return large_group_sum<S>(DevVolume{}, BatchArgs{}, grp, n, keep, hist, lane);
+}
+
+// Select and finish the cap-crossing voxel vi whose group is complete, by
+// the whole warp (vi is warp-uniform). The sum word now holds the group's
+// base + 1 and its size; the weight is the one before the batch (finish
+// left crossing voxels untouched).
+template <int S>
+__device__ __forceinline__ void finish_group(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
+                                             uint32_t vi, uint32_t* hist, int lane, int& updated) {
+    const unsigned long long h = __ldcg(&u.vacc[vi]);
+    const uint32_t base = (uint32_t)(h >> 32) - 1u;
+    const int n = (int)(uint32_t)h;
+    const int keep = accept_count(weight_at<S>(v, vi), v.weight_cap, n);
+    long long fix = 0ll;
+    if ((uint64_t)base + (uint64_t)n > (uint64_t)u.record_cap) {
+        // Counters left by a failed update: nothing to rank.
+        if (lane == 0) atomicOr(u.status, kStatusScratchOverflow);
     } else {
-        group_to_ids<S>(u, n_pts, n_steps, base, n, lane);
-        const uint32_t* ids = u.deferred + base;
-        const long long* vals = u.deferred_fix + base;
-        const uint32_t last = radix_select(ids, n, keep, hist, lane);
-        fix = 0ll;
-        for (int k = lane; k < n; k += 32)
-            if (ids[k] <= last) fix += vals[k];
+        const unsigned long long* grp = u.grp + base;
+        if (n <= 32)
+            fix = rank_group<S, 1>(v, a, grp, n, keep, lane);
+        else if constexpr (S == kStoreF64)
+            fix = large_group_sum<S>(v, a, grp, n, keep, hist, lane);
+        else
+            fix = large_group_sum_out<S>(grp, n, keep, hist, lane);
     }
     for (int o = 16; o > 0; o >>= 1) fix += __shfl_xor_sync(0xffffffffu, fix, o);
-    return fix;
+    if (lane == 0) {
+        finish_voxel<S>(v, u, vi, keep, fix);
+        ++updated;
+    }
+}
+
+// Eight band slots from `first` of one batch, by every thread of the warp
+// (warp-synchronous): records of voxels whose crossing bit is set take their
+// place in the voxel's group; the warp then selects and finishes every group
+// one of its records completed.
+template <int S>
+__device__ __forceinline__ void group_slots(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
+                                            uint32_t first, uint32_t n_slots, uint32_t* hist, int& updated) {
+    const int lane = threadIdx.x & 31;
+    uint32_t vi[kGroupPerThread];
+    float val[kGroupPerThread] = {};
+    if (first + kGroupPerThread <= n_slots) {
+        // Eight consecutive band slots: one step, neighbouring points.
+        const uint4 r0 = __ldcs(reinterpret_cast<const uint4*>(u.records + first));
+        const uint4 r1 = __ldcs(reinterpret_cast<const uint4*>(u.records + first) + 1);
+        vi[0] = r0.x; vi[1] = r0.y; vi[2] = r0.z; vi[3] = r0.w;
+        vi[4] = r1.x; vi[5] = r1.y; vi[6] = r1.z; vi[7] = r1.w;
+        if constexpr (S != kStoreF64) {
+            const float4 s0 = __ldcs(reinterpret_cast<const float4*>(u.slot_val + first));
+            const float4 s1 = __ldcs(reinterpret_cast<const float4*>(u.slot_val + first) + 1);
+            val[0] = s0.x; val[1] = s0.y; val[2] = s0.z; val[3] = s0.w;
+            val[4] = s1.x; val[5] = s1.y; val[6] = s1.z; val[7] = s1.w;
+        }
+    } else {
+#pragma unroll
+        for (int m = 0; m < kGroupPerThread; ++m) {
+            const bool in = first + m < n_slots;
+            vi[m] = in ? u.records[first + m] : kNoVoxel;
+            if constexpr (S != kStoreF64) val[m] = in ? u.slot_val[first + m] : 0.0f;
+        }
+    }
+    // Crossing bits: one gather per distinct bitmap word among the eight.
+    uint32_t word[kGroupPerThread];
+    bool same[kGroupPerThread];
+#pragma unroll
+    for (int m = 0; m < kGroupPerThread; ++m) {
+        same[m] = m > 0 && vi[m] != kNoVoxel && vi[m - 1] != kNoVoxel && (vi[m - 1] >> 5) == (vi[m] >> 5);
+        word[m] = (vi[m] == kNoVoxel || same[m]) ? 0u : __ldg(&u.xbits[vi[m] >> 5]);
+    }
+#pragma unroll
+    for (int m = 1; m < kGroupPerThread; ++m)
+        if (same[m]) word[m] = word[m - 1];
+    const uint32_t n_steps = 2u * (uint32_t)v.steps + 1u;
+    uint32_t last = 0u;  // bit m: slot m's record completed its voxel's group
+#pragma unroll
+    for (int m = 0; m < kGroupPerThread; ++m) {
+        if (vi[m] == kNoVoxel || !((word[m] >> (vi[m] & 31u)) & 1u)) continue;
+        const unsigned long long tk = atomicAdd(&u.vacc[vi[m]], 1ull);
+        const uint64_t pos = (uint64_t)((uint32_t)(tk >> 32) - 1u) + (uint32_t)tk;
+        const uint32_t slot = first + m;
+        unsigned long long e;
+        if constexpr (S == kStoreF64)
+            e = slot;
+        else
+            e = (unsigned long long)slot_id(slot, (uint32_t)a.n, n_steps) |
+                ((unsigned long long)__float_as_uint(val[m]) << 32);
+        if (pos < (uint64_t)u.record_cap) u.grp[pos] = e;
+        else atomicOr(u.status, kStatusScratchOverflow);  // state left by a failed update
+        if (atom_add_acq_rel(&u.vcnt[vi[m]], 0xFFFFFFFFu) == 1u) last |= 1u << m;
+    }
+    // Every group completed here is selected by the whole warp, one at a
+    // time, lowest lane first.
+    while (__any_sync(0xffffffffu, last != 0u)) {
+        const int src = __ffs(__ballot_sync(0xffffffffu, last != 0u)) - 1;
+        uint32_t pick = kNoVoxel;
+        bool got = false;
+#pragma unroll
+        for (int m = 0; m < kGroupPerThread; ++m)
+            if (!got && ((last >> m) & 1u)) {
+                pick = vi[m];
+                got = true;
+            }
+        if (lane == src) last &= last - 1u;  // its lowest pending group
+        finish_group<S>(v, a, u, __shfl_sync(0xffffffffu, pick, src), hist, lane, updated);
+    }
 }
 
 template <int S>
-__global__ void __launch_bounds__(kDeferThreads)
-deferred_kernel(DevVolume v, BatchArgs a, UpdateScratch u) {
-    __shared__ uint32_t hist[kDeferWarps][256];
+__global__ void __launch_bounds__(kGroupThreads, 4)
+group_kernel(DevVolume v, BatchArgs a, UpdateScratch u, uint32_t n_slots) {
+    __shared__ uint32_t hist[kGroupWarps][256];
     __shared__ int s_updated;
     if (threadIdx.x == 0) s_updated = 0;
     __syncthreads();
     launch_dependents();
     grid_dependency_wait();
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t n_steps = 2u * (uint32_t)v.steps + 1u;
-    const unsigned long long lists = u.ctl->def_lists;
-    int n_small = (int)(lists & 0xFFFFFFFFull), n_large = (int)(lists >> 32);
-    if ((long long)n_small + n_large > (long long)u.dvox_cap) n_small = n_large = 0;  // overflowed
+    if (u.ctl->n_crossing == 0ull) return;  // no voxel crossed the cap in this batch
     int updated = 0;
-
-    // Large groups: one warp each.
-    const int gw = blockIdx.x * kDeferWarps + warp, nw = gridDim.x * kDeferWarps;
-    for (int d = gw; d < n_large; d += nw) {
-        const int4 e = u.dvox[u.dvox_cap - 1 - d];  // (voxel, group base, records, accepted)
-        const long long fix = large_group_sum<S>(u, (uint32_t)a.n, n_steps, e, hist[warp], lane);
-        if (lane == 0) {
-            finish_voxel<S>(v, u, (uint32_t)e.x, e.w, fix);
-            ++updated;
-        }
-    }
-
-    // Small groups (at most kLaneRecords = 16 records): one half-warp each,
-    // one record per lane, ranked by id with shuffles inside the half.
-    static_assert(kLaneRecords == 16, "small groups are ranked by half-warps");
-    const int half = lane >> 4, hl = lane & 15;
-    for (int d0 = 2 * gw; d0 < n_small; d0 += 2 * nw) {  // uniform across the warp
-        const int d = d0 + half;
-        const bool live = d < n_small;
-        const int4 e = live ? u.dvox[d] : make_int4(0, 0, 0, 0);
-        const int n = e.z, keep = e.w;
-        const bool mine = live && hl < n;
-        uint32_t id = 0xFFFFFFFFu;
-        long long val = 0ll;
-        if (mine) group_record<S>(u, (uint32_t)a.n, n_steps, (uint32_t)e.y + hl, id, val);
-        int rank = 0;
-#pragma unroll
-        for (int src = 0; src < 16; ++src) rank += __shfl_sync(0xffffffffu, id, src, 16) < id ? 1 : 0;
-        long long fix = (mine && rank < keep) ? val : 0ll;
-#pragma unroll
-        for (int o = 8; o > 0; o >>= 1) fix += __shfl_xor_sync(0xffffffffu, fix, o, 16);
-        if (live && hl == 0) {
-            finish_voxel<S>(v, u, (uint32_t)e.x, keep, fix);
-            ++updated;
-        }
-    }
+    group_slots<S>(v, a, u, (blockIdx.x * kGroupThreads + threadIdx.x) * kGroupPerThread, n_slots,
+                   hist[threadIdx.x >> 5], updated);
     cta_add(&s_updated, updated, &u.ctl->n_updated);
 }
 
@@ -687,7 +674,7 @@ __global__ void batch_prepare_kernel(StepWork w) {
 
 // Work items a pass has in one scene (read by thread 0 after the previous
 // pass completed).
-enum MultiPass : int { kPassFinishPairs, kPassFinishSingle, kPassGroup, kPassValues, kPassDeferred };
+enum MultiPass : int { kPassFinishPairs, kPassFinishSingle, kPassGroup };
 
 template <int PASS>
 __device__ __forceinline__ int scene_items(const SceneWork& sw) {
@@ -699,18 +686,9 @@ __device__ __forceinline__ int scene_items(const SceneWork& sw) {
         const int nt = min(c->n_touched, sw.v.pool_capacity);
         return PASS == kPassFinishPairs ? (nt + 1) / 2 : nt;
     }
-    if (c->def_lists == 0ull) return 0;  // no voxel crossed the cap in this scene
-    if (PASS == kPassGroup)
-        return (int)(((uint32_t)sw.n_slots + kGroupThreads * kGroupPerThread - 1) /
-                     (kGroupThreads * kGroupPerThread));
-    if (PASS == kPassValues) {
-        const long long x = min((long long)c->x_used, (long long)sw.u.record_cap);
-        return (int)((x + kGroupThreads - 1) / kGroupThreads);
-    }
-    // Deferred: one warp item per large group and per pair of small groups.
-    const int n_small = (int)(c->def_lists & 0xFFFFFFFFull), n_large = (int)(c->def_lists >> 32);
-    if ((long long)n_small + n_large > (long long)sw.u.dvox_cap) return 0;  // overflowed
-    return n_large + (n_small + 1) / 2;
+    if (c->n_crossing == 0ull) return 0;  // no voxel crossed the cap in this scene
+    return (int)(((uint32_t)sw.n_slots + kGroupThreads * kGroupPerThread - 1) /
+                 (kGroupThreads * kGroupPerThread));
 }
 
 // Exclusive item prefix of the scenes into begin[0..n]: one thread per scene
@@ -777,131 +755,51 @@ finish_multi_kernel(StepWork w) {
         ulonglong2 a01, a23, b01, b23;
         load_item<S>(sw.v, sw.u, qa, ca, xa, a01, a23);
         if (has_b) load_item<S>(sw.v, sw.u, qb, cb, xb, b01, b23);
+        if (t == 0) tag_chunk(sw.v, ba, bb, has_b);
         finish_quad<S>(sw.v, sw.u, ba, qa, t, lane, ca, xa, a01, a23, updated);
         if (has_b) finish_quad<S>(sw.v, sw.u, bb, qb, t, lane, cb, xb, b01, b23, updated);
         __syncthreads();  // s_item and the descriptor are rewritten next
     }
 }
 
-// Group the records of every scene that has cap-crossing voxels.
-__global__ void __launch_bounds__(kGroupThreads)
+// Group, select and finish the cap-crossing voxels of every scene that has
+// any: work items of 2048 band slots of one scene.
+template <int S>
+__global__ void __launch_bounds__(kGroupThreads, 4)
 group_multi_kernel(StepWork w) {
-    __shared__ UpdateScratch su;
+    __shared__ SceneWork sw;
+    __shared__ uint32_t hist[kGroupWarps][256];
     __shared__ int s_begin[kMaxBatchScenes + 1];
-    __shared__ int s_item;
-    __shared__ uint32_t s_slots;
-    const int t = threadIdx.x;
+    __shared__ int s_item, s_updated;
+    const int t = threadIdx.x, lane = t & 31;
     launch_dependents();
     grid_dependency_wait();
+    if (t == 0) s_updated = 0;
     scene_prefix<kPassGroup>(w, s_begin);
     const int total = s_begin[w.n_scenes];
-    int cur = -1;
+    int cur = -1, updated = 0;
     for (;;) {
         if (t == 0) s_item = (int)atomicAdd(&w.queues[kQGroup], 1u);
         __syncthreads();
         const int item = s_item;
-        if (item >= total) break;
-        const int sc = scene_of(s_begin, w.n_scenes, item);
-        if (sc != cur) {
-            cta_copy(&su, &w.scenes[sc].u);
-            if (t == 0) s_slots = (uint32_t)w.scenes[sc].n_slots;
+        const bool done = item >= total;
+        const int sc = done ? -1 : scene_of(s_begin, w.n_scenes, item);
+        if (sc != cur || done) {
+            const int wsum = __reduce_add_sync(0xffffffffu, updated);
+            if (lane == 0 && wsum) atomicAdd(&s_updated, wsum);
             __syncthreads();
-            cur = sc;
-        }
-        const uint32_t first = ((uint32_t)(item - s_begin[sc]) * kGroupThreads + t) * kGroupPerThread;
-        group_slots(su, first, s_slots);
-        __syncthreads();
-    }
-}
-
-// Ids and values of every scene's grouped records.
-template <int S>
-__global__ void __launch_bounds__(kGroupThreads)
-values_multi_kernel(StepWork w) {
-    __shared__ SceneWork sw;
-    __shared__ int s_begin[kMaxBatchScenes + 1];
-    __shared__ int s_item;
-    const int t = threadIdx.x;
-    launch_dependents();
-    grid_dependency_wait();
-    scene_prefix<kPassValues>(w, s_begin);
-    const int total = s_begin[w.n_scenes];
-    int cur = -1;
-    for (;;) {
-        if (t == 0) s_item = (int)atomicAdd(&w.queues[kQValues], 1u);
-        __syncthreads();
-        const int item = s_item;
-        if (item >= total) break;
-        const int sc = scene_of(s_begin, w.n_scenes, item);
-        if (sc != cur) {
+            if (t == 0 && cur >= 0 && s_updated) atomicAdd(&sw.u.ctl->n_updated, s_updated);
+            __syncthreads();
+            if (t == 0) s_updated = 0;
+            updated = 0;
+            if (done) break;
             cta_copy(&sw, &w.scenes[sc]);
             __syncthreads();
             cur = sc;
         }
-        const uint32_t n = (uint32_t)min((long long)sw.u.ctl->x_used, (long long)sw.u.record_cap);
-        const uint32_t k = (uint32_t)(item - s_begin[sc]) * kGroupThreads + t;
-        if (k < n) {
-            long long fix;
-            const uint32_t id = slot_record<S>(sw.v, sw.a, sw.u, sw.u.deferred[k], fix);
-            sw.u.deferred[k] = id;
-            sw.u.deferred_fix[k] = fix;
-        }
+        const uint32_t first = ((uint32_t)(item - s_begin[sc]) * kGroupThreads + t) * kGroupPerThread;
+        group_slots<S>(sw.v, sw.a, sw.u, first, (uint32_t)sw.n_slots, hist[t >> 5], updated);
         __syncthreads();
-    }
-}
-
-// Select and finish every scene's cap-crossing voxels: warp work items, one
-// per large group and one per pair of small groups.
-template <int S>
-__global__ void __launch_bounds__(kDeferThreads)
-deferred_multi_kernel(StepWork w) {
-    __shared__ uint32_t hist[kDeferWarps][256];
-    __shared__ int s_begin[kMaxBatchScenes + 1];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    launch_dependents();
-    grid_dependency_wait();
-    scene_prefix<kPassDeferred>(w, s_begin);
-    const int total = s_begin[w.n_scenes];
-    for (;;) {
-        int item = 0;
-        if (lane == 0) item = (int)atomicAdd(&w.queues[kQDeferred], 1u);
-        item = __shfl_sync(0xffffffffu, item, 0);
-        if (item >= total) break;
-        const int sc = scene_of(s_begin, w.n_scenes, item);
-        const SceneWork& sw = w.scenes[sc];
-        const DevVolume& v = sw.v;
-        const UpdateScratch& u = sw.u;
-        const uint32_t n_steps = 2u * (uint32_t)v.steps + 1u;
-        const unsigned long long lists = u.ctl->def_lists;
-        const int n_small = (int)(lists & 0xFFFFFFFFull), n_large = (int)(lists >> 32);
-        const int local = item - s_begin[sc];
-        int done = 0;
-        if (local < n_large) {
-            const int4 e = u.dvox[u.dvox_cap - 1 - local];
-            const long long fix = large_group_sum<S>(u, (uint32_t)sw.a.n, n_steps, e, hist[warp], lane);
-            if (lane == 0) finish_voxel<S>(v, u, (uint32_t)e.x, e.w, fix);
-            done = 1;
-        } else {
-            const int half = lane >> 4, hl = lane & 15;
-            const int d0 = 2 * (local - n_large);
-            const int d = d0 + half;
-            const bool live = d < n_small;
-            const int4 e = live ? u.dvox[d] : make_int4(0, 0, 0, 0);
-            const int n = e.z, keep = e.w;
-            const bool mine = live && hl < n;
-            uint32_t id = 0xFFFFFFFFu;
-            long long val = 0ll;
-            if (mine) group_record<S>(u, (uint32_t)sw.a.n, n_steps, (uint32_t)e.y + hl, id, val);
-            int rank = 0;
-#pragma unroll
-            for (int src = 0; src < 16; ++src) rank += __shfl_sync(0xffffffffu, id, src, 16) < id ? 1 : 0;
-            long long fix = (mine && rank < keep) ? val : 0ll;
-#pragma unroll
-            for (int o = 8; o > 0; o >>= 1) fix += __shfl_xor_sync(0xffffffffu, fix, o, 16);
-            if (live && hl == 0) finish_voxel<S>(v, u, (uint32_t)e.x, keep, fix);
-            done = d0 + 1 < n_small ? 2 : 1;
-        }
-        if (lane == 0) atomicAdd(&u.ctl->n_updated, done);
     }
 }
 
@@ -943,36 +841,11 @@ cudaError_t launch_group(const DevVolume& v, const BatchArgs& a, const UpdateScr
     const uint32_t n_slots = (uint32_t)a.n * (2u * (uint32_t)v.steps + 1u);
     if (n_slots == 0) return cudaSuccess;
     const uint32_t per_cta = kGroupThreads * (uint32_t)kGroupPerThread;
-    return launch_after(group_kernel, (n_slots + per_cta - 1u) / per_cta, kGroupThreads, s, u, n_slots);
-}
-
-cudaError_t launch_values(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u, int n_ctas,
-                          cudaStream_t s) {
-    // FP32 / FP16: the deferred pass reads each record's id and value from its
-    // band slot itself; only the FP64 oracle recomputes values from points.
-    if (v.storage != kStoreF64) return cudaSuccess;
+    const uint32_t grid = (n_slots + per_cta - 1u) / per_cta;
     switch (v.storage) {
-        case kStoreF16U16: return launch_after(values_kernel<kStoreF16U16>, n_ctas, kGroupThreads, s, v, a, u);
-        case kStoreF64: return launch_after(values_kernel<kStoreF64>, n_ctas, kGroupThreads, s, v, a, u);
-        default: return launch_after(values_kernel<kStoreF32>, n_ctas, kGroupThreads, s, v, a, u);
-    }
-}
-
-cudaError_t launch_deferred(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u, int sm_count,
-                            cudaStream_t s) {
-    switch (v.storage) {
-        case kStoreF16U16: {
-            return launch_after(deferred_kernel<kStoreF16U16>, resident_grid<deferred_kernel<kStoreF16U16>>(kDeferThreads, sm_count),
-                                kDeferThreads, s, v, a, u);
-        }
-        case kStoreF64: {
-            return launch_after(deferred_kernel<kStoreF64>, resident_grid<deferred_kernel<kStoreF64>>(kDeferThreads, sm_count),
-                                kDeferThreads, s, v, a, u);
-        }
-        default: {
-            return launch_after(deferred_kernel<kStoreF32>, resident_grid<deferred_kernel<kStoreF32>>(kDeferThreads, sm_count),
-                                kDeferThreads, s, v, a, u);
-        }
+        case kStoreF16U16: return launch_after(group_kernel<kStoreF16U16>, grid, kGroupThreads, s, v, a, u, n_slots);
+        case kStoreF64: return launch_after(group_kernel<kStoreF64>, grid, kGroupThreads, s, v, a, u, n_slots);
+        default: return launch_after(group_kernel<kStoreF32>, grid, kGroupThreads, s, v, a, u, n_slots);
     }
 }
 
@@ -988,15 +861,9 @@ cudaError_t finish_multi_t(const StepWork& w, int sm_count, cudaStream_t s) {
                         kFinishThreads, s, w);
 }
 template <int S>
-cudaError_t values_multi_t(const StepWork& w, int sm_count, cudaStream_t s) {
-    return launch_after(values_multi_kernel<S>, resident_grid<values_multi_kernel<S>>(kGroupThreads, sm_count),
+cudaError_t group_multi_t(const StepWork& w, int sm_count, cudaStream_t s) {
+    return launch_after(group_multi_kernel<S>, resident_grid<group_multi_kernel<S>>(kGroupThreads, sm_count),
                         kGroupThreads, s, w);
-}
-template <int S>
-cudaError_t deferred_multi_t(const StepWork& w, int sm_count, cudaStream_t s) {
-    return launch_after(deferred_multi_kernel<S>,
-                        resident_grid<deferred_multi_kernel<S>>(kDeferThreads, sm_count), kDeferThreads, s,
-                        w);
 }
 }  // namespace
 
@@ -1014,25 +881,11 @@ cudaError_t launch_finish_multi(const StepWork& w, int storage, int pair, int sm
     }
 }
 
-cudaError_t launch_group_multi(const StepWork& w, int sm_count, cudaStream_t s) {
-    return launch_after(group_multi_kernel, resident_grid<group_multi_kernel>(kGroupThreads, sm_count),
-                        kGroupThreads, s, w);
-}
-
-cudaError_t launch_values_multi(const StepWork& w, int storage, int sm_count, cudaStream_t s) {
-    if (storage != kStoreF64) return cudaSuccess;  // deferred_multi reads the band slots itself
+cudaError_t launch_group_multi(const StepWork& w, int storage, int sm_count, cudaStream_t s) {
     switch (storage) {
-        case kStoreF16U16: return values_multi_t<kStoreF16U16>(w, sm_count, s);
-        case kStoreF64: return values_multi_t<kStoreF64>(w, sm_count, s);
-        default: return values_multi_t<kStoreF32>(w, sm_count, s);
-    }
-}
-
-cudaError_t launch_deferred_multi(const StepWork& w, int storage, int sm_count, cudaStream_t s) {
-    switch (storage) {
-        case kStoreF16U16: return deferred_multi_t<kStoreF16U16>(w, sm_count, s);
-        case kStoreF64: return deferred_multi_t<kStoreF64>(w, sm_count, s);
-        default: return deferred_multi_t<kStoreF32>(w, sm_count, s);
+        case kStoreF16U16: return group_multi_t<kStoreF16U16>(w, sm_count, s);
+        case kStoreF64: return group_multi_t<kStoreF64>(w, sm_count, s);
+        default: return group_multi_t<kStoreF32>(w, sm_count, s);
     }
 }
 

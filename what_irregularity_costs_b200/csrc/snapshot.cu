@@ -54,6 +54,8 @@ __global__ void rebuild_table_kernel(DevVolume v, int32_t n_blocks) {
     atomicOr(v.status, kStatusScratchOverflow);  // table full: cannot happen with block_count <= slots
 }
 
+}  // namespace
+
 size_t voxel_arrays(int storage, const DevVolume& d, void* out[5], size_t bytes[5]) {
     const int n = storage == kStoreF32 ? 5 : 2;
     out[0] = d.tsdf;
@@ -69,9 +71,14 @@ size_t voxel_arrays(int storage, const DevVolume& d, void* out[5], size_t bytes[
     return (size_t)n;
 }
 
-}  // namespace
+cudaError_t launch_rebuild_table(const DevVolume& v, int32_t n_blocks, cudaStream_t s) {
+    if (n_blocks <= 0) return cudaSuccess;
+    rebuild_table_kernel<<<(n_blocks + 255) / 256, 256, 0, s>>>(v, n_blocks);
+    return cudaGetLastError();
+}
 
 int64_t Volume::snapshot_bytes() {
+    if (dv_.slot_index) return -1;  // the pool-order layout only
     const int64_t b = std::min(block_count(), dv_.pool_capacity);
     void* arr[5];
     size_t per[5];
@@ -83,7 +90,7 @@ int64_t Volume::snapshot_bytes() {
 
 int64_t Volume::snapshot(void* host, int64_t cap) {
     const int64_t need = snapshot_bytes();  // waits for the stream
-    if (!host || cap < need) return -1;
+    if (need < 0 || !host || cap < need) return -1;
     const int32_t b = std::min(block_count(), dv_.pool_capacity);
     SnapshotHeader h{};
     std::memcpy(h.magic, kMagic, sizeof(kMagic));
@@ -114,7 +121,7 @@ int64_t Volume::snapshot(void* host, int64_t cap) {
 }
 
 int32_t Volume::restore(const void* host, int64_t size) {
-    if (!host || size < (int64_t)sizeof(SnapshotHeader)) return 1;
+    if (dv_.slot_index || !host || size < (int64_t)sizeof(SnapshotHeader)) return 1;
     SnapshotHeader h;
     std::memcpy(&h, host, sizeof(h));
     if (std::memcmp(h.magic, kMagic, sizeof(kMagic)) != 0 || h.version != 1) return 1;
@@ -140,10 +147,7 @@ int32_t Volume::restore(const void* host, int64_t size) {
         if (cudaMemcpyAsync(arr[k], p, bytes, cudaMemcpyHostToDevice, stream_) != cudaSuccess) return 3;
         p += bytes;
     }
-    if (b > 0) {
-        rebuild_table_kernel<<<(b + 255) / 256, 256, 0, stream_>>>(dv_, b);
-        if (cudaGetLastError() != cudaSuccess) return 3;
-    }
+    if (launch_rebuild_table(dv_, b, stream_) != cudaSuccess) return 3;
     if (cudaMemcpyAsync(dv_.block_count, &b, sizeof(int32_t), cudaMemcpyHostToDevice, stream_) !=
             cudaSuccess ||
         cudaMemcpyAsync(dv_.drop_count, &h.drop_count, sizeof(unsigned long long),

@@ -35,8 +35,10 @@ constexpr long long kNoKey = -4;  // "no request" marker inside warps; never sto
 constexpr long long kCoordBias = 1LL << 20;
 constexpr int kCoordBits = 21;
 constexpr uint32_t kScratchSlots = 1u << 20;
-// Bound on every device-side wait (iterations of ~100 ns): far above any
-// legitimate publication delay, far below a watchdog.
+// Default bound on every device-side wait (iterations of ~100 ns): far above
+// any legitimate publication delay, far below a watchdog. A volume may lower
+// its own bound (osn_tsdf_cuda_set_spin_limit), e.g. so a test can make a
+// wait run out quickly.
 constexpr int kSpinLimit = 1 << 20;
 
 // Bits of the device status word.
@@ -55,6 +57,9 @@ constexpr uint32_t kStatusScratchOverflow = 2u;
 //                 evaluated in double at the same band samples, float weights
 //                 (integers, exact). No colour arrays.
 enum Storage : int { kStoreF32 = 0, kStoreF16U16 = 1, kStoreF64 = 2 };
+
+// Table layouts (OSN_TSDF_LAYOUT_* in include/osn_tsdf_b200.h).
+enum Layout : int { kLayoutPool = 0, kLayoutSlotIndex = 1 };
 
 // The largest weight a uint16 voxel holds; the effective cap of kStoreF16U16.
 constexpr float kU16WeightMax = 65535.0f;
@@ -90,7 +95,14 @@ struct DevVolume {
     float weight_cap;  // effective cap: <= 0 disables (FP32/FP64); at most 65535 for uint16 weights
     int32_t steps;    // max(1, ceil(trunc * inv_voxel)) (volume.cpp:171)
     uint32_t* status;
-    int32_t storage;  // Storage
+    int32_t storage;     // Storage
+    int32_t spin_limit;  // iterations a publication wait may take (kSpinLimit by default)
+    int32_t* block_chunk;  // per pool block: chunk id of the last call that allocated or updated it
+    int32_t chunk;         // chunk id of the current call
+    // Slot-index layout (opt-in): the pool is the table, a block's pool index
+    // is its table slot, so a key found in the table needs no wait for its
+    // index (cpp/src/volume_cuda.cu:194-244).
+    int32_t slot_index;
 };
 
 // Bytes per voxel of the tsdf and weight arrays of a storage mode.
@@ -109,15 +121,21 @@ __device__ __forceinline__ float weight_at(const DevVolume& v, size_t i) {
         return __ldg(v.weight + i);
 }
 
-// Mean normalised TSDF of voxel i given its weight w > 0.
+// Mean normalised TSDF of voxel i given its weight w (sum * (1/w) for FP32
+// sums, marching_tets.cpp), the stored value loaded whatever the weight so
+// that a caller's weight and value loads are in flight together; meaningful
+// only for w > 0.
 template <int S>
-__device__ __forceinline__ float mean_at(const DevVolume& v, size_t i, float w) {
-    if constexpr (S == kStoreF16U16)
-        return __half2float(reinterpret_cast<const __half*>(v.tsdf)[i]);
-    else if constexpr (S == kStoreF64)
-        return (float)(reinterpret_cast<const double*>(v.tsdf)[i] / (double)w);
-    else
-        return __fmul_rn(v.tsdf[i], __fdiv_rn(1.0f, w));  // marching_tets.cpp: sum * (1/w)
+__device__ __forceinline__ float mean_from(const DevVolume& v, size_t i, float w) {
+    if constexpr (S == kStoreF16U16) {
+        return __half2float(__ldg(reinterpret_cast<const __half*>(v.tsdf) + i));
+    } else if constexpr (S == kStoreF64) {
+        const double d = __ldg(reinterpret_cast<const double*>(v.tsdf) + i);
+        return w > 0.0f ? (float)(d / (double)w) : 0.0f;
+    } else {
+        const float t = __ldg(v.tsdf + i);
+        return w > 0.0f ? __fmul_rn(t, __fdiv_rn(1.0f, w)) : 0.0f;
+    }
 }
 
 // A depth image as the point source of a batch: pixel i = v * width + u
@@ -344,7 +362,7 @@ struct InsertResult {
 // Wait, with an iteration bound, until a claimed slot's index is published
 // or its claim is rolled back (pool full). A timeout sets a status bit.
 __device__ __forceinline__ int32_t wait_published(const DevVolume& v, HashEntry* e, long long want) {
-    for (int it = 0; it < kSpinLimit; ++it) {
+    for (int it = 0; it < v.spin_limit; ++it) {
         const int idx = ld_acquire_s32(&e->block_idx);
         if (idx >= 0) return idx;
         if (ld_relaxed_s64(&e->key) != want) return -1;
@@ -359,10 +377,17 @@ __device__ __forceinline__ int32_t wait_published(const DevVolume& v, HashEntry*
 // coordinate, fence, publish the index (volume_cuda.cu:82-95). When the pool
 // is already full no slot is claimed; a claim that overflows the pool is
 // rolled back to kReleasedKey.
+//
+// In the slot-index layout (and the slot-index measurement mode) the block's
+// index is its slot: a claim publishes it at once (coordinate, count, fence,
+// index) and a thread that finds the key returns the slot without waiting.
 template <int MODE>
 __device__ __forceinline__ InsertResult find_or_insert(const DevVolume& v, int32_t bx, int32_t by,
                                                        int32_t bz, long long want) {
     InsertResult res{-1, 0};
+    const bool by_slot = MODE == kAllocSlotIndex || (MODE == kAllocInsert && v.slot_index);
+    // The measurement mode uses the first pool_capacity slots as the table;
+    // the layout's pool is the whole table.
     const uint32_t mask = (MODE == kAllocSlotIndex) ? (uint32_t)v.pool_capacity - 1u : v.hash_mask;
     const uint32_t size = mask + 1;
     const uint32_t start = hash_slot(bx, by, bz, mask);
@@ -373,13 +398,13 @@ __device__ __forceinline__ InsertResult find_or_insert(const DevVolume& v, int32
         const long long key = ld_relaxed_s64(&e->key);
         if (key == want) {
             if (MODE == kAllocNoCas) { res.idx = 0; return res; }
-            if (MODE == kAllocSlotIndex) { res.idx = (int32_t)slot; return res; }
+            if (by_slot) { res.idx = (int32_t)slot; return res; }
             res.idx = wait_published(v, e, want);
             return res;
         }
         if (key == kEmptyKey) {
             if (MODE == kAllocNoCas) return res;
-            if (MODE != kAllocSlotIndex && ld_acquire_s32(v.block_count) >= v.pool_capacity) {
+            if (!by_slot && ld_acquire_s32(v.block_count) >= v.pool_capacity) {
                 // The pool is full, so no claim can succeed any more -- but the
                 // claim that filled it may have been this very key, made after
                 // we read the slot. Claimers fence between their CAS and their
@@ -398,8 +423,9 @@ __device__ __forceinline__ InsertResult find_or_insert(const DevVolume& v, int32
                                                         (unsigned long long)kEmptyKey,
                                                         (unsigned long long)want);
             if (prev == kEmptyKey) {
-                if (MODE == kAllocSlotIndex) {
+                if (by_slot) {
                     v.block_coord[slot] = BlockCoord{bx, by, bz};
+                    if (v.block_chunk) v.block_chunk[slot] = v.chunk;
                     atomicAdd(v.block_count, 1);
                     __threadfence();
                     atomicExch(&e->block_idx, (int)slot);
@@ -414,13 +440,14 @@ __device__ __forceinline__ InsertResult find_or_insert(const DevVolume& v, int32
                     return res;
                 }
                 v.block_coord[idx] = BlockCoord{bx, by, bz};
+                if (v.block_chunk) v.block_chunk[idx] = v.chunk;
                 __threadfence();  // coordinate visible before the index
                 atomicExch(&e->block_idx, idx);
                 res.idx = idx;
                 return res;
             }
             if (prev == want) {
-                if (MODE == kAllocSlotIndex) { res.idx = (int32_t)slot; return res; }
+                if (by_slot) { res.idx = (int32_t)slot; return res; }
                 res.idx = wait_published(v, e, want);
                 return res;
             }

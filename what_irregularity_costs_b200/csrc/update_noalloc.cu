@@ -1,30 +1,30 @@
 // update_voxels without any device allocation.
 //
-// The regular update_voxels keeps its per-call scratch (one record per band
-// slot, the grouped records of voxels that cross the cap, and their list) in
-// buffers the volume grows with cudaMalloc the first time a batch needs more
-// room, which also waits for the volume's stream and frees the old buffers. Some callers cannot allow that: code
-// that records the integrate into a CUDA graph (allocation is not permitted
-// while a stream is being captured), serving loops that admit work against a
-// fixed device-memory budget and must not see memory appear behind their
-// back, and latency-critical threads that cannot absorb the synchronisation
-// cudaMalloc/cudaFree imply. This entry point gives them the same update
-// with its scratch in one fixed array compiled into the library.
+// The regular update_voxels keeps its per-call scratch (one record and one
+// normalised SDF per band slot, and the grouped records of voxels that
+// cross the cap) in buffers the volume grows with cudaMalloc the first time
+// a batch needs more room, which also waits for the volume's stream and
+// frees the old buffers. Some callers cannot allow that: serving loops that
+// admit work against a fixed device-memory budget (memory appearing behind
+// their back breaks the budget, and a failed cudaMalloc in the middle of a
+// request has no good recovery), and latency-critical threads that cannot
+// absorb the device-wide synchronisation cudaMalloc and cudaFree imply. This
+// entry point gives them the same update with its scratch in one fixed
+// array compiled into the library.
 //
 // The array is a file-scope __device__ variable of kNoAllocScratchBytes
-// (56 MiB + 256 bytes): the control counters, kNoAllocMaxRecords 4-byte band
-// records and 4-byte slot values, as many 4-byte ids and 8-byte values of
-// crossing voxels' records, and half as many 16-byte crossing-voxel entries,
-// i.e. batches with
-// n_points * (2 * steps + 1) <= 2,097,152 (a 480x360 frame at 9 band steps
-// per point fits; a 640x480 frame must be split in two). The per-voxel and
-// per-block state the update also uses belongs to the volume and was
-// allocated with it. Every GPU on which
-// the library's code is loaded holds the array until the process exits.
+// (32 MiB + 256 bytes): the control counters, then kNoAllocMaxRecords 4-byte
+// band records, as many 4-byte normalised SDFs and as many 8-byte group
+// entries, i.e. batches with n_points * (2 * steps + 1) <= 2,097,152 (a
+// 480x360 frame at 9 band steps per point fits; a 640x480 frame must be
+// split in two). The per-voxel and per-block state the update also uses
+// belongs to the volume and was allocated with it. Every GPU on which the
+// library's code is loaded holds the array until the process exits.
 // Every call shares it and it keeps the last call's contents; the counters
 // that must start at zero are cleared at the start of each call. Two calls
 // whose work overlaps on the GPU (two volumes on different streams, say)
-// race on the array and corrupt each other's results: serialise them.
+// race on the array and corrupt each other's results: serialise them. The
+// calling thread's current device must be the volume's.
 #include <algorithm>
 #include <cstdio>
 #include <mutex>
@@ -38,14 +38,11 @@ namespace {
 
 constexpr size_t kNoAllocHeaderBytes = 256;  // UpdateControl, padded
 constexpr int64_t kNoAllocMaxRecords = OSN_TSDF_NOALLOC_MAX_RECORDS;
-constexpr int64_t kNoAllocMaxDeferred = kNoAllocMaxRecords / 2;
 constexpr size_t kNoAllocRecordBytes = (size_t)kNoAllocMaxRecords * sizeof(uint32_t);
-constexpr size_t kNoAllocDeferredBytes = (size_t)kNoAllocMaxRecords * sizeof(uint32_t);
-constexpr size_t kNoAllocFixBytes = (size_t)kNoAllocMaxRecords * sizeof(long long);
 constexpr size_t kNoAllocSlotValBytes = (size_t)kNoAllocMaxRecords * sizeof(float);
-constexpr size_t kNoAllocScratchBytes = kNoAllocHeaderBytes + kNoAllocRecordBytes +
-                                        kNoAllocDeferredBytes + kNoAllocFixBytes +
-                                        (size_t)kNoAllocMaxDeferred * sizeof(int4) + kNoAllocSlotValBytes;
+constexpr size_t kNoAllocGroupBytes = (size_t)kNoAllocMaxRecords * sizeof(unsigned long long);
+constexpr size_t kNoAllocScratchBytes =
+    kNoAllocHeaderBytes + kNoAllocRecordBytes + kNoAllocSlotValBytes + kNoAllocGroupBytes;
 static_assert(sizeof(UpdateControl) <= kNoAllocHeaderBytes, "control block must fit the header");
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
@@ -83,20 +80,23 @@ cudaError_t Volume::update_static_scratch(const BatchArgs& a, void* scratch) {
     UpdateScratch u = us_;
     u.ctl = reinterpret_cast<UpdateControl*>(base);
     u.records = reinterpret_cast<uint32_t*>(base + kNoAllocHeaderBytes);
-    u.deferred = reinterpret_cast<uint32_t*>(base + kNoAllocHeaderBytes + kNoAllocRecordBytes);
-    u.deferred_fix = reinterpret_cast<long long*>(base + kNoAllocHeaderBytes + kNoAllocRecordBytes +
-                                                  kNoAllocDeferredBytes);
-    u.dvox = reinterpret_cast<int4*>(base + kNoAllocHeaderBytes + kNoAllocRecordBytes +
-                                     kNoAllocDeferredBytes + kNoAllocFixBytes);
     u.slot_val = dv_.storage == kStoreF64
                      ? nullptr
-                     : reinterpret_cast<float*>(base + kNoAllocScratchBytes - kNoAllocSlotValBytes);
+                     : reinterpret_cast<float*>(base + kNoAllocHeaderBytes + kNoAllocRecordBytes);
+    u.grp = reinterpret_cast<unsigned long long*>(base + kNoAllocHeaderBytes + kNoAllocRecordBytes +
+                                                  kNoAllocSlotValBytes);
     u.record_cap = kNoAllocMaxRecords;
-    u.dvox_cap = (int32_t)kNoAllocMaxDeferred;
     // Only the control counters must start at zero (run_update clears them);
-    // every record slot is rewritten before it is read, and deferred records
-    // and entries are read only where this call placed them.
-    return run_update(a, u, false);
+    // every record slot is rewritten before it is read, and group entries are
+    // read only where this call placed them.
+    cudaError_t e = run_update(a, u, false);
+    if (e != cudaSuccess) return e;
+    // The call's counters into the volume's own control block (stream order),
+    // so last_update_stats keeps describing this volume whatever later calls
+    // on other volumes leave in the shared array.
+    e = cudaMemcpyAsync(us_.ctl, u.ctl, sizeof(UpdateControl), cudaMemcpyDeviceToDevice, stream_);
+    if (e == cudaSuccess) last_ctl_ = us_.ctl;
+    return e;
 }
 
 }  // namespace osn_b200
@@ -117,6 +117,15 @@ extern "C" int32_t osn_tsdf_cuda_update_voxels_noalloc(OsnTsdfCudaVolume* v,
     }
     int device = 0;
     if (cudaGetDevice(&device) != cudaSuccess) return 3;
+    if (device != vol->device()) {
+        // The array's address is per device: another device's copy would be
+        // a wrong (or unreachable) address for this volume's kernels.
+        std::fprintf(stderr,
+                     "[osn_tsdf_b200] update_voxels_noalloc: current device %d is not the volume's "
+                     "device %d; make the volume's device current first\n",
+                     device, vol->device());
+        return 1;
+    }
     void* scratch = osn_b200::scratch_address(device);
     if (!scratch) return 3;
     osn_b200::BatchArgs a{};

@@ -33,15 +33,24 @@ uint32_t next_pow2(uint32_t v) {  // cpp/src/volume.cpp:14-19
 }  // namespace
 
 Volume::Volume(float voxel, int32_t pool, float trunc_m, float weight_cap, uint32_t hash_slots,
-               int storage) {
+               int storage, int layout) {
     if (!(voxel > 0.0f) || pool <= 0) return;
     if (storage != kStoreF32 && storage != kStoreF16U16 && storage != kStoreF64) return;
+    if (layout != kLayoutPool && layout != kLayoutSlotIndex) return;
+    if (hash_slots != 0 && (hash_slots < 2 || (hash_slots & (hash_slots - 1)) != 0)) return;
+    if (layout == kLayoutSlotIndex) {
+        // The pool is the table: one block of voxels per slot.
+        const uint64_t size = hash_slots ? hash_slots : next_pow2((uint32_t)pool * 2u);
+        if (size > (uint64_t)kMaxPoolBlocks) return;
+        pool = (int32_t)size;
+        hash_slots = (uint32_t)size;
+        dv_.slot_index = 1;
+    }
     if (pool > kMaxPoolBlocks) {
         std::fprintf(stderr, "[osn_tsdf_b200] pool of %d blocks exceeds the supported %d\n", pool,
                      kMaxPoolBlocks);
         return;
     }
-    if (hash_slots != 0 && (hash_slots < 2 || (hash_slots & (hash_slots - 1)) != 0)) return;
     dv_.voxel_size = voxel;
     dv_.inv_voxel = 1.0f / voxel;
     dv_.trunc = trunc_m > 0.0f ? trunc_m : 4.0f * voxel;  // types.hpp:104-106
@@ -55,6 +64,7 @@ Volume::Volume(float voxel, int32_t pool, float trunc_m, float weight_cap, uint3
     weight_cap_ = weight_cap;
     dv_.pool_capacity = pool;
     dv_.steps = std::max(1, (int32_t)std::ceil(dv_.trunc * dv_.inv_voxel));
+    dv_.spin_limit = kSpinLimit;
     ok_ = alloc_device(hash_slots);
 }
 
@@ -64,6 +74,7 @@ bool Volume::alloc_device(uint32_t hash_slots) {
     const size_t n_vox = (size_t)dv_.pool_capacity * kBlockVoxels;
     int dev = 0;
     OSN_TRY(cudaGetDevice(&dev));
+    device_ = dev;
     OSN_TRY(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, dev));
     OSN_TRY(cudaStreamCreate(&stream_));
     OSN_TRY(cudaMalloc(&dv_.table, ((size_t)size + kScratchSlots) * sizeof(HashEntry)));
@@ -71,6 +82,7 @@ bool Volume::alloc_device(uint32_t hash_slots) {
     OSN_TRY(cudaMalloc(&dv_.drop_count, sizeof(unsigned long long)));
     OSN_TRY(cudaMalloc(&dv_.status, sizeof(uint32_t)));
     OSN_TRY(cudaMalloc(&dv_.block_coord, (size_t)dv_.pool_capacity * sizeof(BlockCoord)));
+    OSN_TRY(cudaMalloc(&dv_.block_chunk, (size_t)dv_.pool_capacity * sizeof(int32_t)));
     const size_t t_bytes = n_vox * (size_t)tsdf_bytes(dv_.storage);
     const size_t w_bytes = n_vox * (size_t)weight_bytes(dv_.storage);
     const bool rgb = dv_.storage == kStoreF32;
@@ -84,11 +96,15 @@ bool Volume::alloc_device(uint32_t hash_slots) {
     OSN_TRY(cudaMalloc(&us_.vcnt, n_vox * sizeof(uint32_t)));
     OSN_TRY(cudaMalloc(&us_.vacc, n_vox * sizeof(unsigned long long)));
     OSN_TRY(cudaMalloc(&us_.blk_touch, (size_t)dv_.pool_capacity * sizeof(uint32_t)));
-    OSN_TRY(cudaMalloc(&us_.blk_cross, (size_t)dv_.pool_capacity * sizeof(uint32_t)));
+    OSN_TRY(cudaMalloc(&us_.xbits, (size_t)dv_.pool_capacity * kXWords * sizeof(uint32_t)));
     OSN_TRY(cudaMalloc(&us_.touched, (size_t)dv_.pool_capacity * sizeof(int32_t)));
     OSN_TRY(cudaMalloc(&us_.ctl, sizeof(UpdateControl)));
     us_.status = dv_.status;
     OSN_TRY(cudaMalloc(&mesh_ctl_, 2 * sizeof(int32_t)));
+    if (dv_.slot_index) {
+        OSN_TRY(cudaMalloc(&block_list_, (size_t)dv_.pool_capacity * sizeof(int32_t)));
+        OSN_TRY(cudaMalloc(&list_count_, sizeof(int32_t)));
+    }
     OSN_TRY(cudaMallocHost(&host_small_, 8 * sizeof(int64_t)));
 
     // The table must hold kEmptyKey, not zero: zero is a valid packed key.
@@ -98,6 +114,7 @@ bool Volume::alloc_device(uint32_t hash_slots) {
     OSN_TRY(cudaMemsetAsync(dv_.block_count, 0, sizeof(int32_t), stream_));
     OSN_TRY(cudaMemsetAsync(dv_.drop_count, 0, sizeof(unsigned long long), stream_));
     OSN_TRY(cudaMemsetAsync(dv_.status, 0, sizeof(uint32_t), stream_));
+    OSN_TRY(cudaMemsetAsync(dv_.block_chunk, 0, (size_t)dv_.pool_capacity * sizeof(int32_t), stream_));
     OSN_TRY(cudaMemsetAsync(dv_.tsdf, 0, t_bytes, stream_));
     OSN_TRY(cudaMemsetAsync(dv_.weight, 0, w_bytes, stream_));
     if (rgb) {
@@ -108,7 +125,7 @@ bool Volume::alloc_device(uint32_t hash_slots) {
     OSN_TRY(cudaMemsetAsync(us_.vcnt, 0, n_vox * sizeof(uint32_t), stream_));
     OSN_TRY(cudaMemsetAsync(us_.vacc, 0, n_vox * sizeof(unsigned long long), stream_));
     OSN_TRY(cudaMemsetAsync(us_.blk_touch, 0, (size_t)dv_.pool_capacity * sizeof(uint32_t), stream_));
-    OSN_TRY(cudaMemsetAsync(us_.blk_cross, 0, (size_t)dv_.pool_capacity * sizeof(uint32_t), stream_));
+    OSN_TRY(cudaMemsetAsync(us_.xbits, 0, (size_t)dv_.pool_capacity * kXWords * sizeof(uint32_t), stream_));
     OSN_TRY(cudaMemsetAsync(us_.ctl, 0, sizeof(UpdateControl), stream_));
     OSN_TRY(cudaStreamSynchronize(stream_));
     return true;
@@ -122,6 +139,7 @@ Volume::~Volume() {
     cudaFree(dv_.drop_count);
     cudaFree(dv_.status);
     cudaFree(dv_.block_coord);
+    cudaFree(dv_.block_chunk);
     cudaFree(dv_.tsdf);
     cudaFree(dv_.weight);
     cudaFree(dv_.r);
@@ -130,17 +148,17 @@ Volume::~Volume() {
     cudaFree(us_.vcnt);
     cudaFree(us_.vacc);
     cudaFree(us_.blk_touch);
-    cudaFree(us_.blk_cross);
+    cudaFree(us_.xbits);
     cudaFree(us_.touched);
     cudaFree(us_.ctl);
     cudaFree(us_.records);
     cudaFree(us_.slot_val);
-    cudaFree(us_.deferred);
-    cudaFree(us_.deferred_fix);
-    cudaFree(us_.dvox);
+    cudaFree(us_.grp);
     cudaFree(mesh_posnor_);
     cudaFree(mesh_rgb_);
     cudaFree(mesh_ctl_);
+    cudaFree(block_list_);
+    cudaFree(list_count_);
     cudaFree(d_frames_);
     cudaFree(d_poses_);
     if (host_small_) cudaFreeHost(host_small_);
@@ -216,29 +234,18 @@ bool Volume::ensure_records(int64_t n_records) {
     synchronize();
     cudaFree(us_.records);
     cudaFree(us_.slot_val);
-    cudaFree(us_.deferred);
-    cudaFree(us_.deferred_fix);
-    cudaFree(us_.dvox);
+    cudaFree(us_.grp);
     us_.records = nullptr;
     us_.slot_val = nullptr;
-    us_.deferred = nullptr;
-    us_.deferred_fix = nullptr;
-    us_.dvox = nullptr;
+    us_.grp = nullptr;
     us_.record_cap = 0;
-    us_.dvox_cap = 0;
-    // A crossing voxel holds at least two records, so half the records bound
-    // the two crossing-voxel lists together.
-    const int64_t n_dvox = n_records / 2 + 1;
     if (cudaMalloc(&us_.records, (size_t)n_records * sizeof(uint32_t)) != cudaSuccess) return false;
     if (dv_.storage != kStoreF64 &&
         cudaMalloc(&us_.slot_val, (size_t)n_records * sizeof(float)) != cudaSuccess)
         return false;
-    if (cudaMalloc(&us_.deferred, (size_t)n_records * sizeof(uint32_t)) != cudaSuccess) return false;
-    if (cudaMalloc(&us_.deferred_fix, (size_t)n_records * sizeof(long long)) != cudaSuccess)
-        return false;
-    if (cudaMalloc(&us_.dvox, (size_t)n_dvox * sizeof(int4)) != cudaSuccess) return false;
+    // Groups partition the records of crossing voxels: at most one place per record.
+    if (cudaMalloc(&us_.grp, (size_t)n_records * sizeof(unsigned long long)) != cudaSuccess) return false;
     us_.record_cap = n_records;
-    us_.dvox_cap = (int32_t)std::min<int64_t>(n_dvox, INT32_MAX);
     if (pipelined_) {  // the second set's records and slot values grow with the first
         cudaFree(us2_.records);
         cudaFree(us2_.slot_val);
@@ -330,7 +337,6 @@ cudaError_t Volume::run_update(const BatchArgs& a, const UpdateScratch& scratch,
     if (++update_tag_ == 0u) {
         join();
         cudaMemsetAsync(us_.blk_touch, 0, (size_t)dv_.pool_capacity * sizeof(uint32_t), stream_);
-        cudaMemsetAsync(us_.blk_cross, 0, (size_t)dv_.pool_capacity * sizeof(uint32_t), stream_);
         update_tag_ = 1u;
     }
     UpdateScratch u = scratch;
@@ -370,16 +376,6 @@ cudaError_t Volume::run_update(const BatchArgs& a, const UpdateScratch& scratch,
     mark_start(kKGroup, tail);
     e = launch_group(dv_, a, u, tail);
     mark_end(kKGroup, tail);
-    if (e != cudaSuccess) return e;
-    if (dv_.storage == kStoreF64) {  // other storages: deferred reads the band slots
-        mark_start(kKValues, tail);
-        e = launch_values(dv_, a, u, sm_count_ * 4, tail);
-        mark_end(kKValues, tail);
-        if (e != cudaSuccess) return e;
-    }
-    mark_start(kKDeferred, tail);
-    e = launch_deferred(dv_, a, u, sm_count_, tail);
-    mark_end(kKDeferred, tail);
     if (e != cudaSuccess) return e;
     if (pipe) {
         if ((e = cudaEventRecord(tail_done_[p], tail_)) != cudaSuccess) return e;
@@ -445,10 +441,11 @@ int32_t Volume::extract(float* posnor, uint8_t* rgb, int32_t cap, float min_w, f
         d_rgb = rgb ? mesh_rgb_ : nullptr;
     }
     if (cudaMemsetAsync(mesh_ctl_, 0, 2 * sizeof(int32_t), stream_) != cudaSuccess) return -1;
+    const int32_t nb = std::min(n_blocks, dv_.pool_capacity);
+    const int32_t* list = block_list(nb);
+    if (dv_.slot_index && !list) return -1;
     mark_start(kKExtract);
-    const cudaError_t e =
-        launch_extract(dv_, std::min(n_blocks, dv_.pool_capacity), min_w, iso, d_pos, d_rgb, cap,
-                       mesh_ctl_, stream_);
+    const cudaError_t e = launch_extract(dv_, nb, list, min_w, iso, d_pos, d_rgb, cap, mesh_ctl_, stream_);
     mark_end(kKExtract);
     if (e != cudaSuccess) return -1;
     int32_t* hs = reinterpret_cast<int32_t*>(host_small_);
@@ -470,6 +467,14 @@ int32_t Volume::extract(float* posnor, uint8_t* rgb, int32_t cap, float min_w, f
     return n;
 }
 
+const int32_t* Volume::block_list(int32_t n) {
+    if (!dv_.slot_index || n <= 0) return nullptr;
+    if (cudaMemsetAsync(list_count_, 0, sizeof(int32_t), stream_) != cudaSuccess ||
+        launch_list_blocks(dv_, block_list_, list_count_, stream_) != cudaSuccess)
+        return nullptr;
+    return block_list_;
+}
+
 bool Volume::reserve_batch(int32_t max_points) {
     // A batch drives the volume's updates with its own scratch use: serial.
     if (pipelined_) set_pipelined(false);
@@ -480,7 +485,6 @@ SceneWork Volume::batch_work(const BatchArgs& a, cudaStream_t s) {
     // Block tags are update numbers; at the (theoretical) wrap, clear them.
     if (++update_tag_ == 0u) {
         cudaMemsetAsync(us_.blk_touch, 0, (size_t)dv_.pool_capacity * sizeof(uint32_t), s);
-        cudaMemsetAsync(us_.blk_cross, 0, (size_t)dv_.pool_capacity * sizeof(uint32_t), s);
         update_tag_ = 1u;
     }
     SceneWork w{};
@@ -496,9 +500,11 @@ SceneWork Volume::batch_work(const BatchArgs& a, cudaStream_t s) {
 cudaError_t Volume::reset() {
     join();
     const int32_t n_blocks = std::min(block_count(), dv_.pool_capacity);
+    const int32_t* list = block_list(n_blocks);  // before the table is cleared
+    if (dv_.slot_index && n_blocks > 0 && !list) return cudaErrorUnknown;
     mark_start(kKReset);
-    cudaError_t e = launch_reset_table(dv_.table, dv_.hash_mask + 1, kEmptyKey, stream_);
-    if (e == cudaSuccess) e = launch_reset_voxels(dv_, n_blocks, stream_);
+    cudaError_t e = launch_reset_voxels(dv_, n_blocks, list, stream_);
+    if (e == cudaSuccess) e = launch_reset_table(dv_.table, dv_.hash_mask + 1, kEmptyKey, stream_);
     mark_end(kKReset);
     if (e == cudaSuccess) e = cudaMemsetAsync(dv_.block_count, 0, sizeof(int32_t), stream_);
     if (e == cudaSuccess) e = cudaMemsetAsync(dv_.drop_count, 0, sizeof(unsigned long long), stream_);
@@ -552,7 +558,7 @@ bool Volume::last_update_stats(int64_t out[4]) {
     out[0] = c.n_updated;
     out[1] = c.n_records;
     out[2] = c.n_touched;
-    out[3] = (int64_t)(c.def_lists & 0xFFFFFFFFull) + (int64_t)(c.def_lists >> 32);
+    out[3] = (int64_t)c.n_crossing;
     return true;
 }
 

@@ -18,11 +18,12 @@ enum KernelId : int {
     kKAllocate = 0,      // allocate-only band walk
     kKBand = 1,          // count-and-sum band walk (fused with allocation in integrate)
     kKFinish = 2,        // per touched block: finish every voxel that accepts all its records
-    kKGroup = 3,         // records of voxels that cross the cap, grouped per voxel
-    kKDeferred = 4,      // ordered cap selection of those voxels
+    kKGroup = 3,         // records of voxels that cross the cap: grouped per voxel, ordered
+                         // cap selection, voxel finished
+    kKUnused4 = 4,       // no longer launched (the selection runs inside the group pass)
     kKExtract = 5,
     kKReset = 6,
-    kKValues = 7,        // ids and values of the grouped records
+    kKUnused7 = 7,       // no longer launched
     kNumKernelIds = 8,
 };
 
@@ -33,12 +34,9 @@ struct UpdateControl {
     int32_t n_touched;   // blocks that received a band sample
     int32_t n_updated;   // voxels whose sums were rewritten
     int32_t pad0;
-    uint32_t x_used;     // deferred records reserved
+    uint32_t x_used;     // group places reserved by voxels that cross the cap
     int32_t pad1;
-    // Voxels that cross the cap inside the batch, in two lists sharing dvox:
-    // low word = entries of the small list (at most kLaneRecords records,
-    // from the front), high word = entries of the large list (from the back).
-    unsigned long long def_lists;
+    unsigned long long n_crossing;  // voxels that cross the cap inside the batch
     int32_t pad[8];
 };
 static_assert(sizeof(UpdateControl) == 64, "control block is read back as 64 bytes");
@@ -48,9 +46,8 @@ static_assert(sizeof(UpdateControl) == 64, "control block is read back as 64 byt
 // dropped or saturated sample.
 constexpr uint32_t kNoVoxel = 0xFFFFFFFFu;
 
-// Cap-crossing voxels with at most this many records are ranked by one lane
-// each (in registers); larger ones by a whole warp.
-constexpr int kLaneRecords = 16;
+// Words of a block's crossing bitmap (one bit per voxel).
+constexpr int kXWords = kBlockVoxels / 32;
 
 // Global voxel indices are 32-bit with one value reserved, which bounds the
 // pool at 2^23 - 1 blocks (4 G voxels).
@@ -85,17 +82,21 @@ struct UpdateScratch {
     uint32_t* records = nullptr;  // [record_cap] one per band slot
     float* slot_val = nullptr;    // [record_cap] normalised SDF of each counted slot (FP32 / FP16
                                   // storage; null for the FP64 oracle, which recomputes it)
-    uint32_t* deferred = nullptr;       // [record_cap] canonical ids of crossing voxels' records, grouped per voxel
-    long long* deferred_fix = nullptr;  // [record_cap] their normalised SDFs, 2^-40 fixed point
-    int4* dvox = nullptr;               // [dvox_cap] (voxel, group base, records, accepted)
+    // [record_cap] records of the voxels that cross the cap, grouped per
+    // voxel: canonical id | normalised SDF bits << 32 (the band slot for the
+    // FP64 oracle, which recomputes both).
+    unsigned long long* grp = nullptr;
     int64_t record_cap = 0;
-    int32_t dvox_cap = 0;
     // Owned by the volume. Per voxel: zero between updates.
-    uint32_t* vcnt = nullptr;            // records of the voxel in this batch
-    unsigned long long* vacc = nullptr;  // fixed-point sum of their sdf_n; group base of a crossing voxel
+    uint32_t* vcnt = nullptr;            // records of the voxel in this batch (of a crossing voxel:
+                                         // records still to be placed in its group)
+    unsigned long long* vacc = nullptr;  // fixed-point sum of their sdf_n (of a crossing voxel: group
+                                         // base + 1 << 32 | next place)
     // Per block, tagged with the update number instead of being cleared.
     uint32_t* blk_touch = nullptr;  // update that last touched the block
-    uint32_t* blk_cross = nullptr;  // update in which the block held a cap-crossing voxel
+    // [pool * kXWords] per block: bit lv set when voxel lv crosses the cap in
+    // this update; rewritten by finish for every block whose voxels it reads.
+    uint32_t* xbits = nullptr;
     int32_t* touched = nullptr;     // [pool] blocks touched by this update
     uint32_t* status = nullptr;     // the volume's status word
     uint32_t tag = 0;               // this update's number (never 0)
@@ -103,19 +104,23 @@ struct UpdateScratch {
 
 class Volume {
 public:
+    // layout: kLayoutPool (the reference's: pool indices from a counter) or
+    // kLayoutSlotIndex (the pool is the table; a block's index is its slot).
     Volume(float voxel, int32_t pool, float trunc_m, float weight_cap, uint32_t hash_slots,
-           int storage = kStoreF32);
+           int storage = kStoreF32, int layout = kLayoutPool);
     ~Volume();
     Volume(const Volume&) = delete;
     Volume& operator=(const Volume&) = delete;
 
     bool ok() const { return ok_; }
     const DevVolume& dev() const { return dv_; }
+    int device() const { return device_; }  // the CUDA device the volume was created on
     cudaStream_t stream() const { return stream_; }
     float voxel_size() const { return dv_.voxel_size; }
     float trunc() const { return dv_.trunc; }
     float weight_cap() const { return weight_cap_; }  // as given at creation
     int storage() const { return dv_.storage; }
+    int layout() const { return dv_.slot_index ? kLayoutSlotIndex : kLayoutPool; }
     int32_t pool() const { return dv_.pool_capacity; }
     uint32_t hash_mask() const { return dv_.hash_mask; }
 
@@ -129,7 +134,8 @@ public:
     // FP16 storage.
     cudaError_t integrate_frames(const BatchArgs& a, const FrameTable& t, const PoseTable* poses = nullptr);
     // update() with its control counters and records in caller-provided
-    // device memory instead of the volume's own (grown) buffer.
+    // device memory instead of the volume's own (grown) buffer; the counters
+    // are copied to the volume's own control block afterwards.
     cudaError_t update_static_scratch(const BatchArgs& a, void* scratch);
     int32_t extract(float* posnor, uint8_t* rgb, int32_t cap, float min_w, float iso, bool host_out);
     cudaError_t reset();
@@ -144,11 +150,30 @@ public:
     bool last_update_stats(int64_t out[4]);
 
     // Pipelined updates. When on, an update's band walk runs on stream() and
-    // its tail (finish, group, values, deferred) on an internal stream, so the
+    // its tail (finish, group) on an internal stream, so the
     // next update's walk overlaps this one's tail; the per-update scratch
     // alternates between two sets. Every reader of results joins first.
     // Not available for the FP64 oracle storage (its tail reads the points).
     bool set_pipelined(bool on);
+    // Chunk id that later calls give the blocks they allocate or update
+    // (streaming: evict_chunks moves a range of chunks to host memory).
+    void set_chunk(int32_t chunk) { dv_.chunk = chunk; }
+    int32_t chunk() const { return dv_.chunk; }
+    // Blocks whose chunk id lies in [lo, hi]: bytes of their pack, and the
+    // eviction itself (pack written to host, blocks removed, the others
+    // compacted to the front of the pool, table rebuilt); stream_in puts a
+    // pack's blocks back (blocks already present are left and counted in
+    // *skipped). chunks.cu.
+    int64_t evict_bytes(int32_t lo, int32_t hi);
+    int64_t evict_chunks(int32_t lo, int32_t hi, void* host, int64_t cap);
+    int32_t stream_in(const void* host, int64_t size, int32_t* skipped);
+    // Bound of every publication wait of this volume's later calls, in
+    // iterations of ~100 ns (1 .. kSpinLimit).
+    bool set_spin_limit(int32_t iterations) {
+        if (iterations < 1 || iterations > kSpinLimit) return false;
+        dv_.spin_limit = iterations;
+        return true;
+    }
     bool pipelined() const { return pipelined_; }
     // Make stream() wait for every queued update tail.
     void join();
@@ -178,9 +203,16 @@ private:
     cudaError_t run_update(const BatchArgs& a, const UpdateScratch& u, bool insert,
                            const FrameTable* frames = nullptr, const PoseTable* poses = nullptr);
     bool ensure_records(int64_t n_records);
+    // The allocated blocks' pool indices: 0..n-1 in the pool layout (returns
+    // nullptr), the occupied slots listed on the device in the slot-index
+    // layout (returns the list; n = block count).
+    const int32_t* block_list(int32_t n);
+    int32_t* block_list_ = nullptr;  // slot-index layout: [pool] occupied slots
+    int32_t* list_count_ = nullptr;
     bool ensure_mesh(int32_t cap, bool rgb);
 
     bool ok_ = false;
+    int device_ = -1;
     DevVolume dv_{};
     float weight_cap_ = 0.0f;
     cudaStream_t stream_ = nullptr;
@@ -247,12 +279,22 @@ cudaError_t launch_after(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaSt
 cudaError_t launch_allocate(const DevVolume& v, const BatchArgs& a, int mode,
                             unsigned long long* hist, int n_bins, int sm_count, cudaStream_t s);
 cudaError_t launch_reset_table(HashEntry* first, uint32_t count, long long key, cudaStream_t s);
-cudaError_t launch_reset_voxels(const DevVolume& v, int32_t n_blocks, cudaStream_t s);
-cudaError_t launch_extract(const DevVolume& v, int32_t n_blocks, float min_w, float iso,
+// Re-insert the keys of pool blocks 0..n-1 (coordinates from block_coord)
+// into an empty table, block i at pool index i (snapshot.cu).
+cudaError_t launch_rebuild_table(const DevVolume& v, int32_t n_blocks, cudaStream_t s);
+// The voxel arrays of a storage mode (tsdf, weight[, r, g, b]) and their
+// bytes per voxel; returns how many (snapshot.cu).
+size_t voxel_arrays(int storage, const DevVolume& d, void* out[5], size_t bytes[5]);
+// Zero the voxels of n blocks: pool indices 0..n-1, or those of a list.
+cudaError_t launch_reset_voxels(const DevVolume& v, int32_t n_blocks, const int32_t* list, cudaStream_t s);
+// List the occupied slots of the table (slot-index layout) into out.
+cudaError_t launch_list_blocks(const DevVolume& v, int32_t* out, int32_t* count, cudaStream_t s);
+// Extraction over n blocks: pool indices 0..n-1, or those of a list.
+cudaError_t launch_extract(const DevVolume& v, int32_t n_blocks, const int32_t* list, float min_w, float iso,
                            float* posnor, uint8_t* rgb, int32_t cap, int32_t* ctl, cudaStream_t s);
 
 // The update pipeline: band walk (counts, sums, records) -> finish -> group
-// -> values -> deferred.
+// (grouping, ordered selection and finishing of the voxels that cross the cap).
 cudaError_t launch_band_records(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
                                 bool insert, int sm_count, cudaStream_t s);
 // Several-frame integrate: the set-up kernel (control block zeroed, frame
@@ -270,10 +312,6 @@ cudaError_t launch_band_depth_frames(const DevVolume& v, const BatchArgs& a, con
 cudaError_t launch_finish(const DevVolume& v, const UpdateScratch& u, int sm_count, cudaStream_t s);
 cudaError_t launch_group(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
                          cudaStream_t s);
-cudaError_t launch_values(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u, int n_ctas,
-                          cudaStream_t s);
-cudaError_t launch_deferred(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u, int sm_count,
-                            cudaStream_t s);
 
 }  // namespace osn_b200
 
@@ -299,7 +337,7 @@ struct SceneWork {
 };
 
 // Work queues of one step, one counter per pass (zeroed by the prepare pass).
-enum BatchQueue : int { kQBand = 0, kQFinish, kQGroup, kQValues, kQDeferred, kNumBatchQueues };
+enum BatchQueue : int { kQBand = 0, kQFinish, kQGroup, kNumBatchQueues };
 
 // Tunable shape of a batched step (chosen by the batch autotuner).
 struct BatchShape {
@@ -320,8 +358,6 @@ struct StepWork {
 cudaError_t launch_batch_prepare(const StepWork& w, cudaStream_t s);
 cudaError_t launch_band_multi(const StepWork& w, int storage, int probe, int sm_count, cudaStream_t s);
 cudaError_t launch_finish_multi(const StepWork& w, int storage, int pair, int sm_count, cudaStream_t s);
-cudaError_t launch_group_multi(const StepWork& w, int sm_count, cudaStream_t s);
-cudaError_t launch_values_multi(const StepWork& w, int storage, int sm_count, cudaStream_t s);
-cudaError_t launch_deferred_multi(const StepWork& w, int storage, int sm_count, cudaStream_t s);
+cudaError_t launch_group_multi(const StepWork& w, int storage, int sm_count, cudaStream_t s);
 
 }  // namespace osn_b200

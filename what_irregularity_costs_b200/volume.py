@@ -20,10 +20,15 @@ from . import _lib
 
 MAX_FRAMES = 32  # OSN_TSDF_MAX_FRAMES: frames per integrate_frames call
 MAX_DEPTH_FRAMES = 16  # OSN_TSDF_MAX_DEPTH_FRAMES: images per integrate_depth_frames call
-KERNEL_NAMES = ["allocate", "band", "finish", "group", "deferred", "extract", "reset", "values"]
+# Kernel ids of the timing table (ids 4 and 7 are kept for the numbering and
+# record no launches: the ordered cap selection runs inside the group pass).
+KERNEL_NAMES = ["allocate", "band", "finish", "group", "unused4", "extract", "reset", "unused7"]
 
 # Voxel storage modes (OSN_TSDF_STORAGE_* in include/osn_tsdf_b200.h).
 STORAGE_FP32, STORAGE_FP16_U16, STORAGE_FP64 = 0, 1, 2
+# Table layouts (OSN_TSDF_LAYOUT_*): the reference's pool order, or the pool
+# as the table (a block's index is its slot).
+LAYOUT_POOL, LAYOUT_SLOT_INDEX = 0, 1
 STORAGE_NAMES = {STORAGE_FP32: "fp32", STORAGE_FP16_U16: "fp16_u16", STORAGE_FP64: "fp64"}
 
 
@@ -73,11 +78,13 @@ class CudaVolume:
     """One hash-blocked TSDF volume on the GPU (drop-in for the reference's CudaVolume)."""
 
     def __init__(self, voxel_size_m: float, pool_capacity_blocks: int, trunc_m: float = -1.0,
-                 weight_cap: float = 32.0, hash_slots: int = 0, storage: int = STORAGE_FP32):
+                 weight_cap: float = 32.0, hash_slots: int = 0, storage: int = STORAGE_FP32,
+                 layout: int = LAYOUT_POOL):
         self.lib = _lib.load()
         self.storage = int(storage)
-        self.h = self.lib.osn_tsdf_cuda_create_ex(voxel_size_m, pool_capacity_blocks, trunc_m,
-                                                  weight_cap, hash_slots, self.storage)
+        self.layout = int(layout)
+        self.h = self.lib.osn_tsdf_cuda_create_layout(voxel_size_m, pool_capacity_blocks, trunc_m,
+                                                      weight_cap, hash_slots, self.storage, self.layout)
         if not self.h:
             raise ValueError("osn_tsdf_cuda_create rejected the parameters or the device "
                              "allocation failed")
@@ -307,6 +314,63 @@ class CudaVolume:
         if rc:
             raise RuntimeError(f"set_pipelined failed (code {rc})")
 
+    # -- streaming by chunk id ---------------------------------------------
+    def set_chunk(self, chunk_id: int):
+        """Chunk id that later calls give the blocks they allocate or update."""
+        self._check(self.lib.osn_tsdf_cuda_set_chunk(self.h, int(chunk_id)), "set_chunk")
+
+    def evict_chunks(self, lo: int, hi: int) -> np.ndarray:
+        """Move every block whose chunk id lies in [lo, hi] to a host pack
+        (returned as bytes) and remove it from the volume; the remaining blocks
+        are compacted and the table rebuilt."""
+        n = self.lib.osn_tsdf_cuda_evict_chunks_bytes(self.h, int(lo), int(hi))
+        if n < 0:
+            raise RuntimeError("evict_chunks_bytes failed")
+        buf = np.empty(int(n), dtype=np.uint8)
+        wrote = self.lib.osn_tsdf_cuda_evict_chunks(self.h, int(lo), int(hi), buf.ctypes.data, int(n))
+        if wrote != n:
+            raise RuntimeError(f"evict_chunks failed ({wrote})")
+        return buf
+
+    def unpack_chunks(self, pack: np.ndarray):
+        """(coords (n, 3) int32, chunk ids (n,) int32, arrays) of a pack from
+        evict_chunks: arrays as (n, 512) per voxel array of the storage mode
+        (tsdf, weight[, r, g, b]; FP16: float16 means and uint16 weights)."""
+        pack = np.ascontiguousarray(pack, dtype=np.uint8)
+        n = int(pack[36:40].view(np.int32)[0])
+        off = 64
+        coords = pack[off:off + 12 * n].view(np.int32).reshape(n, 3)
+        off += 12 * n
+        chunks = pack[off:off + 4 * n].view(np.int32)
+        off += 4 * n
+        kinds = {STORAGE_FP32: ["<f4"] * 5, STORAGE_FP16_U16: ["<f2", "<u2"], STORAGE_FP64: ["<f8", "<f4"]}
+        arrays = []
+        for dt in kinds[self.storage]:
+            size = np.dtype(dt).itemsize * 512 * n
+            arrays.append(pack[off:off + size].view(dt).reshape(n, 512))
+            off += size
+        return coords, chunks, arrays
+
+    def stream_in(self, pack: np.ndarray) -> int:
+        """Insert a pack's blocks again; returns how many were skipped because
+        the volume holds them again. Raises when the pool filled."""
+        pack = np.ascontiguousarray(pack, dtype=np.uint8)
+        skipped = C.c_int32(0)
+        rc = self.lib.osn_tsdf_cuda_stream_in(self.h, pack.ctypes.data, int(pack.nbytes),
+                                              C.addressof(skipped))
+        if rc == 2:
+            raise RuntimeError("stream_in: the pool filled before every block was restored")
+        self._check(rc, "stream_in")
+        return int(skipped.value)
+
+    def set_spin_limit(self, iterations: int):
+        """Bound each device-side publication wait of later calls to this many
+        iterations of ~100 ns (1 .. 2^20, the default). A wait that runs out
+        drops its samples and sets bit 0 of status()."""
+        rc = self.lib.osn_tsdf_cuda_set_spin_limit(self.h, int(iterations))
+        if rc:
+            raise ValueError(f"set_spin_limit({iterations}) failed (code {rc})")
+
     def join(self):
         """Order the volume's stream after every queued update tail."""
         self.lib.osn_tsdf_cuda_join(self.h)
@@ -339,13 +403,27 @@ class CudaVolume:
         return {k: (float(ms[i]), int(launches[i])) for i, k in enumerate(KERNEL_NAMES)}
 
     # -- read-back helpers (tests, tools) ------------------------------------
+    def _rows(self, ptr, cols, typestr):
+        """Rows of a per-block device array for every allocated block, in pool
+        order (slot-index layout: the occupied slots, ascending)."""
+        view = self.device_view()
+        if self.layout == LAYOUT_SLOT_INDEX:
+            import torch
+            keys, idx = self.table()
+            slots = np.nonzero((keys >= 0) & (idx == np.arange(keys.shape[0])))[0]
+            if slots.size == 0:
+                return np.zeros((0, cols), dtype=np.dtype(typestr))
+            full = device_tensor(ptr, (view.pool_capacity, cols), typestr)
+            return full[torch.from_numpy(slots).cuda()].cpu().numpy()
+        n = min(self.block_count(), view.pool_capacity)
+        if n <= 0:
+            return np.zeros((0, cols), dtype=np.dtype(typestr))
+        return device_tensor(ptr, (n, cols), typestr).cpu().numpy()
+
     def coords(self) -> np.ndarray:
         """Block coordinates in pool order, (block_count, 3) int32."""
-        n = min(self.block_count(), self.device_view().pool_capacity)
-        if n <= 0:
-            return np.zeros((0, 3), dtype=np.int32)
-        view = self.device_view()
-        return device_tensor(view.block_coord, (n, 3), "<i4").cpu().numpy()
+        self.synchronize()
+        return self._rows(self.device_view().block_coord, 3, "<i4")
 
     def coord_set(self) -> set:
         return set(map(tuple, self.coords().tolist()))
@@ -353,19 +431,18 @@ class CudaVolume:
     def means(self):
         """(coords, mean TSDF, weight) in any storage mode: (block_count, 512) float64
         arrays; the mean is 0 where the weight is 0."""
-        n = min(self.block_count(), self.device_view().pool_capacity)
         view = self.device_view()
         coords = self.coords()
-        if n <= 0:
+        if coords.shape[0] == 0:
             z = np.zeros((0, 512), dtype=np.float64)
             return coords, z, z.copy()
         if self.storage == STORAGE_FP16_U16:
-            mean = device_tensor(view.tsdf, (n, 512), "<f2").cpu().numpy().astype(np.float64)
-            w = device_tensor(view.weight, (n, 512), "<u2").cpu().numpy().astype(np.float64)
+            mean = self._rows(view.tsdf, 512, "<f2").astype(np.float64)
+            w = self._rows(view.weight, 512, "<u2").astype(np.float64)
         else:
             typ = "<f8" if self.storage == STORAGE_FP64 else "<f4"
-            t = device_tensor(view.tsdf, (n, 512), typ).cpu().numpy().astype(np.float64)
-            w = device_tensor(view.weight, (n, 512), "<f4").cpu().numpy().astype(np.float64)
+            t = self._rows(view.tsdf, 512, typ).astype(np.float64)
+            w = self._rows(view.weight, 512, "<f4").astype(np.float64)
             mean = np.divide(t, w, out=np.zeros_like(t), where=w > 0)
         return coords, mean, w
 
@@ -374,14 +451,10 @@ class CudaVolume:
         (FP32 storage: the reference's weighted sums)."""
         if self.storage != STORAGE_FP32:
             raise ValueError("voxels() reads the FP32 layout; use means() for other storage")
-        n = min(self.block_count(), self.device_view().pool_capacity)
         view = self.device_view()
         out = [self.coords()]
         for ptr in (view.tsdf, view.weight, view.r, view.g, view.b):
-            if n <= 0:
-                out.append(np.zeros((0, 512), dtype=np.float32))
-            else:
-                out.append(device_tensor(ptr, (n, 512), "<f4").cpu().numpy())
+            out.append(self._rows(ptr, 512, "<f4"))
         return tuple(out)
 
     def table(self):
