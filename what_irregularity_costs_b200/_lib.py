@@ -115,11 +115,14 @@ def declared_symbols() -> list[str]:
     return sorted(set(re.findall(r"\b(osn_tsdf_(?:cuda|batch)_\w+)\s*\(", text)))
 
 
-def load(path: str = LIB_PATH):
-    """Load the CUDA library (once). Raises if it has not been built."""
+def load(path: str | None = None):
+    """Load the CUDA library (once). Raises if it has not been built.
+    OSN_TSDF_B200_LIB names another build of it (a variant compiled with
+    different tuning flags) in place of the in-tree one."""
     global _lib
     if _lib is not None:
         return _lib
+    path = path or os.environ.get("OSN_TSDF_B200_LIB") or LIB_PATH
     if not os.path.exists(path):
         raise ImportError(
             f"libosn_tsdf_b200.so not found at {path}; build it with "

@@ -48,18 +48,23 @@ def _stale(out: str, deps: list[str]) -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(verbose: bool = False, ptxas_info: bool = False) -> str:
-    os.makedirs(OBJ, exist_ok=True)
+def build(verbose: bool = False, ptxas_info: bool = False, defines=(), obj_dir: str = OBJ,
+          lib: str = LIB) -> str:
+    """Compile every csrc/*.cu and link the library. defines: extra -D flags
+    (tuning macros such as OSN_BAND_MIN_BLOCKS), with their own object folder
+    and library path."""
+    os.makedirs(obj_dir, exist_ok=True)
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
     headers += [os.path.join(ROOT, "include", f) for f in os.listdir(os.path.join(ROOT, "include"))]
     exe = nvcc()
     jobs = []
     for src in sources():
-        obj = os.path.join(OBJ, os.path.basename(src)[:-3] + ".o")
+        obj = os.path.join(obj_dir, os.path.basename(src)[:-3] + ".o")
         if ptxas_info or _stale(obj, [src] + headers):
-            cmd = [exe] + NVCC_FLAGS + (["-Xptxas", "-v"] if ptxas_info else []) + ["-c", src, "-o", obj]
+            cmd = ([exe] + NVCC_FLAGS + [f"-D{d}" for d in defines] + (["-Xptxas", "-v"] if ptxas_info else [])
+                   + ["-c", src, "-o", obj])
             jobs.append(cmd)
-    objs = [os.path.join(OBJ, os.path.basename(s)[:-3] + ".o") for s in sources()]
+    objs = [os.path.join(obj_dir, os.path.basename(s)[:-3] + ".o") for s in sources()]
 
     def run(cmd):
         r = subprocess.run(cmd, capture_output=True, text=True)
@@ -71,13 +76,13 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
                 sys.stderr.write(r.stdout + r.stderr)
             if r.returncode:
                 raise RuntimeError("nvcc failed: " + " ".join(cmd))
-    if jobs or _stale(LIB, objs):
-        cmd = [exe] + ARCH + ["-shared", "-o", LIB] + objs
+    if jobs or _stale(lib, objs):
+        cmd = [exe] + ARCH + ["-shared", "-o", lib] + objs
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode:
             sys.stderr.write(r.stdout + r.stderr)
             raise RuntimeError("link failed")
-    return LIB
+    return lib
 
 
 if __name__ == "__main__":

@@ -61,6 +61,19 @@ constexpr int kChunk = OSN_BAND_CHUNK;  // samples per ray held in registers (9:
 #endif
 constexpr int kBandMinBlocks = OSN_BAND_MIN_BLOCKS;  // resident CTAs per SM the register budget is sized for
 
+// Band records and slot values are read once more, by the group pass of the
+// same update: stored with the streaming hint (1, evict-first) or as
+// ordinary write-back stores that may stay in L2 (0).
+#ifndef OSN_BAND_STREAM_RECORDS
+#define OSN_BAND_STREAM_RECORDS 1
+#endif
+
+template <typename T>
+__device__ __forceinline__ void store_slot(T* p, T x) {
+    if (OSN_BAND_STREAM_RECORDS) __stcs(p, x);
+    else *p = x;
+}
+
 // Per-sample state: voxel within block (9 bits), run index (4 bits), valid.
 constexpr uint32_t kLvMask = 0x1FFu;
 constexpr int kRunShift = 9;
@@ -317,13 +330,13 @@ __device__ __forceinline__ void band_point(const DevVolume& v, const BatchArgs& 
                         fix = to_fix(sdf_n);
                         // Kept for the records of voxels that cross the cap, so the
                         // update tail never reads the batch's points again.
-                        __stcs(u.slot_val + (rec - u.records), sdf_n);
+                        store_slot(u.slot_val + (rec - u.records), sdf_n);
                     }
                     red_add(&u.vcnt[out], 1u);
                     red_add(&u.vacc[out], (unsigned long long)fix);
                     ++counted;
                 }
-                if (i < a.n) __stcs(rec, out);  // read again only for crossing voxels
+                if (i < a.n) store_slot(rec, out);  // read again by the group pass
                 rec += a.n;
             }
         }

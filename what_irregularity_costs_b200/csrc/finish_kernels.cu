@@ -31,10 +31,11 @@
 //            crossing bitmap (16 words per block, rewritten for every block
 //            finish visits).
 //   group    one pass over the band slots of the batch, eight per thread
-//            (records and normalised SDFs loaded as 128-bit vectors): a
-//            record whose voxel's bit is set takes the next place of the
-//            voxel's group (atomic add on the sum word) and stores its
-//            canonical id and value there, then counts the voxel's pending
+//            (records loaded as 128-bit vectors): a record whose voxel's bit
+//            is set takes the next place of the voxel's group (atomic add on
+//            the sum word; its normalised SDF loaded in the same round trip)
+//            and stores its canonical id and value there, then counts the
+//            voxel's pending
 //            records down with an acquire-release atomic. The record that
 //            brings the count to zero is the last of its group: its warp
 //            loads the whole group, keeps the keep records with the smallest
@@ -62,6 +63,11 @@ constexpr int kGroupThreads = 256;
 constexpr int kGroupWarps = kGroupThreads / 32;
 constexpr int kGroupPerThread = 8;  // band slots per thread (two 128-bit loads)
 constexpr int kRankRegs = 8;        // groups of up to 32 * 8 records are ranked in registers
+// Resident 256-thread CTAs per SM the group pass's registers are sized for:
+// the scan is latency-bound, so occupancy hides its round trips.
+#ifndef OSN_GROUP_MIN_BLOCKS
+#define OSN_GROUP_MIN_BLOCKS 6
+#endif
 static_assert(kFinishThreads >= kMaxBatchScenes && kGroupThreads >= kMaxBatchScenes,
               "one thread per scene builds the item prefix");
 
@@ -367,11 +373,31 @@ __device__ __forceinline__ uint32_t entry_id(const DevVolume& v, const BatchArgs
         return (uint32_t)e;
 }
 
+// What the selection of one cap-crossing voxel touches, as plain values: an
+// out-of-line selection takes these, so no kernel parameter is passed by
+// address (which would make every thread copy it to local memory).
+struct SelectArgs {
+    float* tsdf;
+    float* weight;
+    float* r;
+    float* g;
+    float* b;
+    unsigned long long* vacc;
+    uint32_t* vcnt;
+    const unsigned long long* grp;
+    int64_t record_cap;
+    uint32_t* status;
+    float cap;  // effective weight cap
+};
+
+__device__ __forceinline__ SelectArgs select_args(const DevVolume& v, const UpdateScratch& u) {
+    return SelectArgs{v.tsdf, v.weight, v.r, v.g, v.b, u.vacc, u.vcnt, u.grp, u.record_cap, u.status, v.weight_cap};
+}
+
 // Finish a cap-crossing voxel: keep contributions accepted, their values
 // summing to fix * 2^-40.
 template <int S>
-__device__ __forceinline__ void finish_voxel(const DevVolume& v, const UpdateScratch& u, uint32_t vi,
-                                             int keep, long long fix) {
+__device__ __forceinline__ void finish_voxel(const SelectArgs& v, uint32_t vi, int keep, long long fix) {
     if constexpr (S == kStoreF32) {
         const float wn = __fadd_rn(v.weight[vi], (float)keep);
         v.tsdf[vi] = add_fix(v.tsdf[vi], fix);
@@ -391,8 +417,17 @@ __device__ __forceinline__ void finish_voxel(const DevVolume& v, const UpdateScr
         d[vi] = d[vi] + (double)fix * kFixInv;
         v.weight[vi] = __fadd_rn(v.weight[vi], (float)keep);
     }
-    u.vacc[vi] = 0ull;
-    u.vcnt[vi] = 0u;
+    v.vacc[vi] = 0ull;
+    v.vcnt[vi] = 0u;
+}
+
+// The weight of voxel vi before the batch (finish leaves crossing voxels as they were).
+template <int S>
+__device__ __forceinline__ float weight_before(const SelectArgs& v, uint32_t vi) {
+    if constexpr (S == kStoreF16U16)
+        return (float)__ldg(reinterpret_cast<const unsigned short*>(v.weight) + vi);
+    else
+        return __ldg(v.weight + vi);
 }
 
 // Sum of the accepted values of a group of at most 32 * R records, by one
@@ -502,45 +537,39 @@ __device__ __forceinline__ long long large_group_sum(const DevVolume& v, const B
     return fix;
 }
 
-// The same out of line for the storages whose entries carry their values
-// (no volume or batch needed), so the common small groups keep the pass's
-// registers.
-template <int S>
-__device__ __noinline__ long long large_group_sum_out(const unsigned long long* grp, int n, int keep,
-                                                      uint32_t* hist, int lane) {
-    static_assert(S != kStoreF64, "the FP64 oracle recomputes values from its batch");
-    return large_group_sum<S>(DevVolume{}, BatchArgs{}, grp, n, keep, hist, lane);
-}
-
 // Select and finish the cap-crossing voxel vi whose group is complete, by
 // the whole warp (vi is warp-uniform). The sum word now holds the group's
-// base + 1 and its size; the weight is the one before the batch (finish
-// left crossing voxels untouched).
+// base + 1 and its size. Returns 1 on lane 0 (the voxel it finished), else 0.
+// v and a are read only by the FP64 oracle, whose entries carry band slots.
 template <int S>
-__device__ __forceinline__ void finish_group(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
-                                             uint32_t vi, uint32_t* hist, int lane, int& updated) {
-    const unsigned long long h = __ldcg(&u.vacc[vi]);
+__device__ __forceinline__ int select_group(const SelectArgs& sa, const DevVolume& v, const BatchArgs& a,
+                                            uint32_t vi, uint32_t* hist, int lane) {
+    const unsigned long long h = __ldcg(&sa.vacc[vi]);
     const uint32_t base = (uint32_t)(h >> 32) - 1u;
     const int n = (int)(uint32_t)h;
-    const int keep = accept_count(weight_at<S>(v, vi), v.weight_cap, n);
+    const int keep = accept_count(weight_before<S>(sa, vi), sa.cap, n);
     long long fix = 0ll;
-    if ((uint64_t)base + (uint64_t)n > (uint64_t)u.record_cap) {
+    if ((uint64_t)base + (uint64_t)n > (uint64_t)sa.record_cap) {
         // Counters left by a failed update: nothing to rank.
-        if (lane == 0) atomicOr(u.status, kStatusScratchOverflow);
+        if (lane == 0) atomicOr(sa.status, kStatusScratchOverflow);
     } else {
-        const unsigned long long* grp = u.grp + base;
-        if (n <= 32)
-            fix = rank_group<S, 1>(v, a, grp, n, keep, lane);
-        else if constexpr (S == kStoreF64)
-            fix = large_group_sum<S>(v, a, grp, n, keep, hist, lane);
-        else
-            fix = large_group_sum_out<S>(grp, n, keep, hist, lane);
+        const unsigned long long* grp = sa.grp + base;
+        fix = n <= 32 ? rank_group<S, 1>(v, a, grp, n, keep, lane)
+                      : large_group_sum<S>(v, a, grp, n, keep, hist, lane);
     }
     for (int o = 16; o > 0; o >>= 1) fix += __shfl_xor_sync(0xffffffffu, fix, o);
-    if (lane == 0) {
-        finish_voxel<S>(v, u, vi, keep, fix);
-        ++updated;
-    }
+    if (lane != 0) return 0;
+    finish_voxel<S>(sa, vi, keep, fix);
+    return 1;
+}
+
+// The same out of line for the storages whose entries carry their values
+// (no volume or batch needed): the selection runs about once per warp, so
+// the scan of the band slots keeps its few registers and its occupancy.
+template <int S>
+__device__ __noinline__ int select_group_out(const SelectArgs sa, uint32_t vi, uint32_t* hist, int lane) {
+    static_assert(S != kStoreF64, "the FP64 oracle recomputes values from its batch");
+    return select_group<S>(sa, DevVolume{}, BatchArgs{}, vi, hist, lane);
 }
 
 // Eight band slots from `first` of one batch, by every thread of the warp
@@ -552,26 +581,16 @@ __device__ __forceinline__ void group_slots(const DevVolume& v, const BatchArgs&
                                             uint32_t first, uint32_t n_slots, uint32_t* hist, int& updated) {
     const int lane = threadIdx.x & 31;
     uint32_t vi[kGroupPerThread];
-    float val[kGroupPerThread] = {};
     if (first + kGroupPerThread <= n_slots) {
         // Eight consecutive band slots: one step, neighbouring points.
         const uint4 r0 = __ldcs(reinterpret_cast<const uint4*>(u.records + first));
         const uint4 r1 = __ldcs(reinterpret_cast<const uint4*>(u.records + first) + 1);
         vi[0] = r0.x; vi[1] = r0.y; vi[2] = r0.z; vi[3] = r0.w;
         vi[4] = r1.x; vi[5] = r1.y; vi[6] = r1.z; vi[7] = r1.w;
-        if constexpr (S != kStoreF64) {
-            const float4 s0 = __ldcs(reinterpret_cast<const float4*>(u.slot_val + first));
-            const float4 s1 = __ldcs(reinterpret_cast<const float4*>(u.slot_val + first) + 1);
-            val[0] = s0.x; val[1] = s0.y; val[2] = s0.z; val[3] = s0.w;
-            val[4] = s1.x; val[5] = s1.y; val[6] = s1.z; val[7] = s1.w;
-        }
     } else {
 #pragma unroll
-        for (int m = 0; m < kGroupPerThread; ++m) {
-            const bool in = first + m < n_slots;
-            vi[m] = in ? u.records[first + m] : kNoVoxel;
-            if constexpr (S != kStoreF64) val[m] = in ? u.slot_val[first + m] : 0.0f;
-        }
+        for (int m = 0; m < kGroupPerThread; ++m)
+            vi[m] = first + m < n_slots ? u.records[first + m] : kNoVoxel;
     }
     // Crossing bits: one gather per distinct bitmap word among the eight.
     uint32_t word[kGroupPerThread];
@@ -589,15 +608,19 @@ __device__ __forceinline__ void group_slots(const DevVolume& v, const BatchArgs&
 #pragma unroll
     for (int m = 0; m < kGroupPerThread; ++m) {
         if (vi[m] == kNoVoxel || !((word[m] >> (vi[m] & 31u)) & 1u)) continue;
+        const uint32_t slot = first + m;
+        // The record's value (FP32 / FP16: the walk kept it) is loaded beside
+        // its place ticket, in the same round trip.
+        float val = 0.0f;
+        if constexpr (S != kStoreF64) val = __ldcs(u.slot_val + slot);
         const unsigned long long tk = atomicAdd(&u.vacc[vi[m]], 1ull);
         const uint64_t pos = (uint64_t)((uint32_t)(tk >> 32) - 1u) + (uint32_t)tk;
-        const uint32_t slot = first + m;
         unsigned long long e;
         if constexpr (S == kStoreF64)
             e = slot;
         else
             e = (unsigned long long)slot_id(slot, (uint32_t)a.n, n_steps) |
-                ((unsigned long long)__float_as_uint(val[m]) << 32);
+                ((unsigned long long)__float_as_uint(val) << 32);
         if (pos < (uint64_t)u.record_cap) u.grp[pos] = e;
         else atomicOr(u.status, kStatusScratchOverflow);  // state left by a failed update
         if (atom_add_acq_rel(&u.vcnt[vi[m]], 0xFFFFFFFFu) == 1u) last |= 1u << m;
@@ -615,12 +638,16 @@ __device__ __forceinline__ void group_slots(const DevVolume& v, const BatchArgs&
                 got = true;
             }
         if (lane == src) last &= last - 1u;  // its lowest pending group
-        finish_group<S>(v, a, u, __shfl_sync(0xffffffffu, pick, src), hist, lane, updated);
+        const uint32_t gv = __shfl_sync(0xffffffffu, pick, src);
+        if constexpr (S == kStoreF64)
+            updated += select_group<S>(select_args(v, u), v, a, gv, hist, lane);
+        else
+            updated += select_group_out<S>(select_args(v, u), gv, hist, lane);
     }
 }
 
 template <int S>
-__global__ void __launch_bounds__(kGroupThreads, 4)
+__global__ void __launch_bounds__(kGroupThreads, OSN_GROUP_MIN_BLOCKS)
 group_kernel(DevVolume v, BatchArgs a, UpdateScratch u, uint32_t n_slots) {
     __shared__ uint32_t hist[kGroupWarps][256];
     __shared__ int s_updated;
@@ -765,7 +792,7 @@ finish_multi_kernel(StepWork w) {
 // Group, select and finish the cap-crossing voxels of every scene that has
 // any: work items of 2048 band slots of one scene.
 template <int S>
-__global__ void __launch_bounds__(kGroupThreads, 4)
+__global__ void __launch_bounds__(kGroupThreads, OSN_GROUP_MIN_BLOCKS)
 group_multi_kernel(StepWork w) {
     __shared__ SceneWork sw;
     __shared__ uint32_t hist[kGroupWarps][256];
