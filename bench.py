@@ -718,6 +718,15 @@ def run_ours(args):
         except Exception as e:  # reported beside the line, never required
             batch32 = {"error": str(e)}
 
+    # -- serving: a bounded run of the 64-session configuration (each session's
+    # trajectory cut at serve_frames frames), realtime Poisson arrivals
+    serve64 = None
+    if rank == 0 and world == 1 and args.serve_frames > 0:
+        try:
+            serve64 = serve64_figures(args.serve_frames, torch)
+        except Exception as e:  # reported beside the line, never required
+            serve64 = {"error": str(e)}
+
     parity = None
     if rank == 0 and not args.no_parity:
         try:
@@ -788,6 +797,7 @@ def run_ours(args):
                            "unit": "block resolutions by slots probed (bin k = k slots)"},
             "parity": parity,
             "batch32": batch32,
+            "serve64": serve64,
             "update_gbps": update_alg_bytes / t_update / 1e9 if t_update else None,
             "update_gbps_updated_voxels": update_alg_bytes_voxels / t_update / 1e9 if t_update else None,
             "extract": {"blocks": ext_blocks, "vertices": ext_verts,
@@ -1086,6 +1096,36 @@ def run_serve64(args):
     return 0
 
 
+def serve64_figures(max_frames, torch):
+    """The serving configuration (run_serve64) with every session's trajectory
+    cut at max_frames frames, realtime arrivals only: frames/s and p50/p99
+    integrate and extract latency."""
+    import dataclasses
+    from what_irregularity_costs_b200 import workloads
+    from what_irregularity_costs_b200.serving import Server, poisson_schedule
+    specs = [dataclasses.replace(sp, frames=min(sp.frames, max_frames))
+             for sp in workloads.scene_mix(64, seed=5)]
+    frames = workloads.mix_frames(specs, 8)
+    rate, every, budget = 2000.0, 50, 120e9
+    reqs = poisson_schedule(specs, rate_fps=rate, extract_every=every, seed=11)
+    server = Server(budget_bytes=budget, graph=True, shape=(8, 0, 1))
+    try:
+        rt = server.run(specs, frames, reqs, realtime=True, open_first=True)
+        status = server.batch.status()
+    finally:
+        server.close()
+    torch.cuda.synchronize()
+    return {"metric": "frames/s (64-session serving, Poisson 2000 frames/s offered)",
+            "frames_per_s": rt["frames_per_s"], "frames": rt.get("frames"),
+            "latency_ms": {"integrate": rt["integrate_latency_ms"],
+                           "integrate_steady": rt.get("integrate_latency_ms_steady"),
+                           "extract": rt["extract_latency_ms"]},
+            "frames_per_step": rt.get("frames_per_step"), "status": status,
+            "config": f"64 sessions (scene_mix seed 5), each cut at {max_frames} frames, 8 distinct "
+                      f"frames cycled; extract every {every} frames; {budget / 1e9:.0f} GB budget; "
+                      "FP16/u16 storage"}
+
+
 def run_sweep(args):
     """Irregularity and precision sweep on the room trajectory (640x480 frames):
     voxel sizes 5 mm, 1, 2, 4 cm (trunc 4 voxels, cap 64) on a 2^18-slot table
@@ -1207,6 +1247,8 @@ def main():
     ap.add_argument("--batch-steps", type=int, default=5,
                     help="timed steps of the 32-scene batched comparison in the room line (0: skip)")
     ap.add_argument("--batch-warmup", type=int, default=3)
+    ap.add_argument("--serve-frames", type=int, default=50,
+                    help="frames per session of the bounded serving run in the room line (0: skip)")
     ap.add_argument("--no-parity", action="store_true",
                     help="skip the check of the headline run's volume against the oracle")
     ap.add_argument("--cpu-budget", type=float, default=15.0)

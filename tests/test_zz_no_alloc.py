@@ -1,13 +1,13 @@
 """The no-allocation update entry point, checked against update_voxels.
 
 osn_tsdf_cuda_update_voxels_noalloc exists for callers that cannot let the
-library allocate device memory during an integrate: code that records the
-integrate into a CUDA graph (allocation is not allowed while a stream is
-captured), serving loops that budget device memory up front, and
-latency-critical threads that cannot absorb the synchronisation a cudaMalloc
-or cudaFree implies. Its scratch is one fixed array compiled into the
-library, shared by every call, so these tests also run it twice in a row:
-the second call starts on whatever the first one left in that array.
+library allocate device memory during an integrate: serving loops that admit
+work against a fixed device-memory budget (memory appearing behind their back
+breaks the budget), and latency-critical threads that cannot absorb the
+device-wide synchronisation a cudaMalloc or cudaFree implies. Its scratch is
+one fixed array compiled into the library, shared by every call, so these
+tests also run it twice in a row: the second call starts on whatever the
+first one left in that array.
 
 This file is collected last on purpose, so a run that stops at its first
 failure has already run every other test.
@@ -61,3 +61,26 @@ def test_noalloc_rejects_batches_above_the_fixed_maximum(cuda):
         vol.synchronize()
         assert vol.block_count() == 0
         assert np.all(vol.voxels()[2] == 0)
+
+
+def test_noalloc_stats_belong_to_the_volume(cuda):
+    """The counters a no-alloc call leaves in the shared array are copied to
+    the volume's own control block: a later no-alloc call on another volume
+    does not change what the first volume reports."""
+    scene = scenes.RoomScene.make(2)
+    K = scenes.ROOM_K.scaled(320, 240)
+    fa, fb = scenes.room_frame(scene, 0, K), scenes.room_frame(scene, 5, K)
+    with CudaVolume(0.02, 1 << 16, 0.08, 64.0) as a, CudaVolume(0.02, 1 << 16, 0.08, 64.0) as b, \
+            CudaVolume(0.02, 1 << 16, 0.08, 64.0) as ref:
+        da = cuda.from_numpy(scenes.frame_points(fa)).cuda()
+        db = cuda.from_numpy(scenes.frame_points(fb)[::2].copy()).cuda()
+        for v in (a, ref):
+            v.allocate_blocks(da, fa.cam)
+        ref.update_voxels(da, fa.cam)
+        assert a.update_voxels_noalloc(da, fa.cam) == 0
+        want = ref.last_update_stats()
+        assert a.last_update_stats() == want and want["records"] > 0
+        b.allocate_blocks(db, fb.cam)
+        assert b.update_voxels_noalloc(db, fb.cam) == 0
+        assert b.last_update_stats()["records"] != want["records"]
+        assert a.last_update_stats() == want

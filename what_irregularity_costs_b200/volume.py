@@ -135,8 +135,10 @@ class CudaVolume:
                               n=None) -> int:
         """update_voxels with no device allocation (the library's fixed scratch array).
 
-        For callers that must not allocate during the call (graph capture,
-        fixed memory budgets). Returns the C ABI code: 0 queued, 4 when the
+        For callers that cannot let the library allocate during the call: a
+        serving loop that admits work against a fixed device-memory budget, a
+        latency-critical thread that cannot absorb the synchronisation of a
+        cudaMalloc/cudaFree. Returns the C ABI code: 0 queued, 4 when the
         batch exceeds OSN_TSDF_NOALLOC_MAX_RECORDS records (nothing queued).
         """
         count = _count(positions, n)
