@@ -620,10 +620,10 @@ def run_ours(args):
         a, b = int(offsets[k]), int(offsets[k + 1])
         hist += vol.allocate_probe_histogram(d_all[a:b], cams[k], n_bins=32)
     probes_mean = float(np.sum(hist * np.arange(32)) / max(1, int(hist.sum())))
-    integrate_kernels = ("band", "finish", "group")
+    integrate_kernels = ("band", "finish", "group", "select")
     # Launches of the headline arm: per integrate_frames call the set-up
-    # kernel and the three passes; reset's two per step.
-    launches_per_step = 4 * len(groups) + 2
+    # kernel and the four passes; reset's two per step.
+    launches_per_step = (1 + sum(1 for k in integrate_kernels if per_kernel[k][1] > 0)) * len(groups) + 2
     dominant = max(integrate_kernels, key=lambda k: per_kernel[k][0])
 
     peak, peak_kind = measured_peak()
@@ -638,7 +638,8 @@ def run_ours(args):
     alg_total = {
         "band": 12 * n_points + 4 * n_slots + 16 * n_rec,
         "finish": n_touch * 512 * (16 + 36),   # read cnt,w,t,sum; write t,w,r,g,b,cnt,sum
-        "group": 8 * n_slots,   # record and normalised SDF of every band slot
+        "group": 4 * n_slots,   # the record of every band slot
+        "select": 0,
     }
     # Update as the reference scopes it: positions + tsdf/weight tiles of the
     # touched blocks, read and written; the stricter figure counts only the

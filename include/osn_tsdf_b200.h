@@ -312,7 +312,7 @@ void* osn_tsdf_cuda_stream(const OsnTsdfCudaVolume* v);
 
 /* Pipelined updates. When enabled, an integrate/update call's band walk is
  * queued on the volume's stream as usual but its update tail (finish,
- * group) runs on an internal stream, so the next call's walk
+ * group, select) runs on an internal stream, so the next call's walk
  * overlaps this call's tail; the per-call scratch alternates between two sets
  * (twice the per-voxel batch state: +12 bytes per voxel). Results are
  * identical. The positions (or depth image) of a call may be reused once the
@@ -356,7 +356,7 @@ int32_t osn_tsdf_cuda_last_update_stats(const OsnTsdfCudaVolume* v, int64_t* out
  * device-memory budget, latency-critical threads that cannot absorb the
  * device-wide synchronisation cudaMalloc/cudaFree imply -- call this
  * instead. Same results as update_voxels.
- * Its scratch is one fixed 32 MiB array inside the library, held on every
+ * Its scratch is one fixed 36 MiB array inside the library, held on every
  * GPU where the library's code is loaded until the process exits, and shared
  * by all calls: calls whose work overlaps on the GPU race and must be
  * serialised. The calling thread's current device must be the volume's. The
@@ -376,7 +376,7 @@ int32_t osn_tsdf_cuda_update_voxels_noalloc(OsnTsdfCudaVolume* v, const float* d
  * size and truncation, one storage mode for all) integrate one frame each
  * per step in one chain of work-queued passes on the batch's stream: a
  * table of the step's scenes is uploaded, then one pass of each kernel
- * (band walk, finish, group) covers every scene, its CTAs
+ * (band walk, finish, group, select) covers every scene, its CTAs
  * taking (scene, tile range) work items from atomic queues. Results are
  * bit-identical to integrating each scene alone with osn_tsdf_cuda_integrate.
  *
@@ -435,9 +435,9 @@ int32_t osn_tsdf_batch_size(OsnTsdfBatch* b);
  * waits for) the accumulated per-kernel milliseconds and launch counts.
  * Kernel ids: 0 allocate, 1 band (count-and-sum walk; allocates too in
  * integrate), 2 finish (per touched block), 3 group (records of voxels that
- * cross the cap, grouped per voxel, with the ordered cap selection and the
- * voxels' update), 5 extract, 6 reset; ids 4 and 7 are kept for the
- * numbering and record no launches.
+ * cross the cap, grouped per voxel), 4 select (ordered cap selection and
+ * update of those voxels), 5 extract, 6 reset; id 7 is kept for the
+ * numbering and records no launches.
  * Returns the number of ids written. */
 int32_t osn_tsdf_cuda_set_timing(OsnTsdfCudaVolume* v, int32_t enabled);
 int32_t osn_tsdf_cuda_kernel_times(OsnTsdfCudaVolume* v, double* ms, int64_t* launches,

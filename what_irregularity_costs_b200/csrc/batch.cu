@@ -9,11 +9,10 @@
 //   prepare       zero the active scenes' update counters and the queues;
 //   band_multi    allocate + count-and-sum walk of every scene: work items
 //                 of a few 128-point tiles of one scene from an atomic queue;
-//   finish_multi, group_multi
+//   finish_multi, group_multi, select_multi
 //                 the single-volume passes over every scene's touched
-//                 blocks and band records (grouping, ordered selection and
-//                 finishing of cap-crossing voxels), work-queued the same way
-//                 (per-scene item counts prefix-summed on device).
+//                 blocks, band records and cap-crossing voxels, work-queued
+//                 the same way (per-scene item counts prefix-summed on device).
 //
 // The passes after the upload are launched with programmatic stream
 // serialisation and can be captured once into a CUDA graph and replayed
@@ -278,6 +277,7 @@ private:
         if (e == cudaSuccess) e = launch_band_multi(w, storage_, shape.probe, sm_count_, stream_);
         if (e == cudaSuccess) e = launch_finish_multi(w, storage_, shape.finish_pair, sm_count_, stream_);
         if (e == cudaSuccess) e = launch_group_multi(w, storage_, sm_count_, stream_);
+        if (e == cudaSuccess) e = launch_select_multi(w, storage_, sm_count_, stream_);
         return e;
     }
 

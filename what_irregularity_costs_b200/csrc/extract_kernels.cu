@@ -290,7 +290,9 @@ extract_kernel(DevVolume v, int32_t n_blocks, const int32_t* list, float min_w, 
     sink.base = s_base;
     int at = (warp ? s_warp[warp - 1] : 0) + x - n_vert;  // block-relative
 
-    for (int k = 0; k < 6; ++k) {
+    // Only cubes with every corner valid emit (n_vert counted nothing else);
+    // the others still reach the barrier before the copy-out.
+    for (int k = 0; k < (n_vert > 0 ? 6 : 0); ++k) {
         const int* tq = c_tets[k];
         const int code = ((below >> tq[0]) & 1) | (((below >> tq[1]) & 1) << 1) |
                          (((below >> tq[2]) & 1) << 2) | (((below >> tq[3]) & 1) << 3);

@@ -63,6 +63,16 @@ constexpr int kGroupThreads = 256;
 constexpr int kGroupWarps = kGroupThreads / 32;
 constexpr int kGroupPerThread = 8;  // band slots per thread (two 128-bit loads)
 constexpr int kRankRegs = 8;        // groups of up to 32 * 8 records are ranked in registers
+// Where the ordered selection of cap-crossing voxels runs: 1, in its own
+// pass over a list of the crossing voxels that finish writes (no memory
+// ordering inside a pass: the pass boundary orders everything); 0, inside
+// the group pass, by the warp whose record completes a voxel's group (one
+// fence per thread that placed records, one per selected group).
+#ifndef OSN_SPLIT_SELECT
+#define OSN_SPLIT_SELECT 1
+#endif
+constexpr int kSelectThreads = 128;
+constexpr int kSelectWarps = kSelectThreads / 32;
 // Resident 256-thread CTAs per SM the group pass's registers are sized for:
 // the scan is latency-bound, so occupancy hides its round trips.
 #ifndef OSN_GROUP_MIN_BLOCKS
@@ -80,15 +90,6 @@ __device__ __forceinline__ int accept_count(float w0, float cap, int n) {
     if (w0 >= cap) return 0;
     const double room = ceil((double)cap - (double)w0);
     return room >= (double)n ? n : (int)room;
-}
-
-// Atomic add with acquire-release semantics at GPU scope: the caller's
-// earlier stores are visible to whoever reads the result of a later add to
-// the same word, and the caller sees what earlier adders stored.
-__device__ __forceinline__ uint32_t atom_add_acq_rel(uint32_t* p, uint32_t x) {
-    uint32_t old;
-    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(x) : "memory");
-    return old;
 }
 
 // ---- finish ----------------------------------------------------------------
@@ -211,7 +212,7 @@ __device__ __forceinline__ void finish_quad(const DevVolume& v, const UpdateScra
             ++my_cross;
         }
     }
-    uint32_t rec_base = 0u;
+    uint32_t rec_base = 0u, x_at = 0u;
     if (__ballot_sync(0xffffffffu, my_records > 0u)) {
         uint32_t rec_incl = my_records, x_incl = my_cross;
         for (int o = 1; o < 32; o <<= 1) {
@@ -222,13 +223,15 @@ __device__ __forceinline__ void finish_quad(const DevVolume& v, const UpdateScra
                 x_incl += xy;
             }
         }
-        uint32_t rb = 0u;
+        uint32_t rb = 0u, xb = 0u;
         if (lane == 31) {
             rb = atomicAdd(&u.ctl->x_used, rec_incl);
-            atomicAdd(&u.ctl->n_crossing, (unsigned long long)x_incl);
+            xb = (uint32_t)atomicAdd(&u.ctl->n_crossing, (unsigned long long)x_incl);
         }
         rb = __shfl_sync(0xffffffffu, rb, 31);
+        xb = __shfl_sync(0xffffffffu, xb, 31);
         rec_base = rb + rec_incl - my_records;
+        x_at = xb + x_incl - my_cross;  // this lane's first place in the crossing list
     }
     uint32_t xmask = 0u;  // bit q: voxel 4t + q crosses the cap
 #pragma unroll
@@ -246,10 +249,11 @@ __device__ __forceinline__ void finish_quad(const DevVolume& v, const UpdateScra
             // last of them finishes it. The sum word holds the group's base
             // + 1 (high half) and the next free place (low half); the count
             // word the records still to be placed.
-            if ((uint64_t)rec_base + n[q] <= (uint64_t)u.record_cap) {
+            if ((uint64_t)rec_base + n[q] <= (uint64_t)u.record_cap && x_at < (uint32_t)u.xlist_cap) {
                 acc[q] = (unsigned long long)(rec_base + 1u) << 32;
                 cnt[q] = n[q];
                 xmask |= 1u << q;
+                if (OSN_SPLIT_SELECT) u.xlist[x_at] = (uint32_t)bi * kBlockVoxels + 4u * t + q;
             } else {
                 // Out of scratch (only after a failed update left stale
                 // counters): the voxel's records are dropped, the status
@@ -258,6 +262,7 @@ __device__ __forceinline__ void finish_quad(const DevVolume& v, const UpdateScra
                 acc[q] = 0ull;
             }
             rec_base += n[q];
+            ++x_at;
         }
     }
     // The block's crossing bitmap: voxel 32w + j is bit j of word w, and the
@@ -544,6 +549,11 @@ __device__ __forceinline__ long long large_group_sum(const DevVolume& v, const B
 template <int S>
 __device__ __forceinline__ int select_group(const SelectArgs& sa, const DevVolume& v, const BatchArgs& a,
                                             uint32_t vi, uint32_t* hist, int lane) {
+    // Fused selection: the group's other records were placed by other
+    // threads of this pass, each with a fence between its entry stores and
+    // its countdown; this fence orders the reads below after the countdown
+    // that saw the group complete.
+    if (!OSN_SPLIT_SELECT) __threadfence();
     const unsigned long long h = __ldcg(&sa.vacc[vi]);
     const uint32_t base = (uint32_t)(h >> 32) - 1u;
     const int n = (int)(uint32_t)h;
@@ -604,7 +614,7 @@ __device__ __forceinline__ void group_slots(const DevVolume& v, const BatchArgs&
     for (int m = 1; m < kGroupPerThread; ++m)
         if (same[m]) word[m] = word[m - 1];
     const uint32_t n_steps = 2u * (uint32_t)v.steps + 1u;
-    uint32_t last = 0u;  // bit m: slot m's record completed its voxel's group
+    uint32_t placed = 0u;  // bit m: slot m's record took a place in its group
 #pragma unroll
     for (int m = 0; m < kGroupPerThread; ++m) {
         if (vi[m] == kNoVoxel || !((word[m] >> (vi[m] & 31u)) & 1u)) continue;
@@ -623,7 +633,17 @@ __device__ __forceinline__ void group_slots(const DevVolume& v, const BatchArgs&
                 ((unsigned long long)__float_as_uint(val) << 32);
         if (pos < (uint64_t)u.record_cap) u.grp[pos] = e;
         else atomicOr(u.status, kStatusScratchOverflow);  // state left by a failed update
-        if (atom_add_acq_rel(&u.vcnt[vi[m]], 0xFFFFFFFFu) == 1u) last |= 1u << m;
+        placed |= 1u << m;
+    }
+    if (OSN_SPLIT_SELECT) return;  // the select pass ranks the complete groups
+    // Fused selection: this thread's entries are visible before its
+    // countdowns; the record that brings a count to zero completed its group.
+    uint32_t last = 0u;  // bit m: slot m's record completed its voxel's group
+    if (placed) {
+        __threadfence();
+#pragma unroll
+        for (int m = 0; m < kGroupPerThread; ++m)
+            if (((placed >> m) & 1u) && atomicSub(&u.vcnt[vi[m]], 1u) == 1u) last |= 1u << m;
     }
     // Every group completed here is selected by the whole warp, one at a
     // time, lowest lane first.
@@ -659,6 +679,26 @@ group_kernel(DevVolume v, BatchArgs a, UpdateScratch u, uint32_t n_slots) {
     int updated = 0;
     group_slots<S>(v, a, u, (blockIdx.x * kGroupThreads + threadIdx.x) * kGroupPerThread, n_slots,
                    hist[threadIdx.x >> 5], updated);
+    cta_add(&s_updated, updated, &u.ctl->n_updated);
+}
+
+// The ordered selection of every cap-crossing voxel of the batch, from the
+// list finish wrote: one warp per voxel (OSN_SPLIT_SELECT).
+template <int S>
+__global__ void __launch_bounds__(kSelectThreads)
+select_kernel(DevVolume v, BatchArgs a, UpdateScratch u) {
+    __shared__ uint32_t hist[kSelectWarps][256];
+    __shared__ int s_updated;
+    if (threadIdx.x == 0) s_updated = 0;
+    __syncthreads();
+    launch_dependents();
+    grid_dependency_wait();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const long long n = min((long long)u.ctl->n_crossing, (long long)u.xlist_cap);
+    const SelectArgs sa = select_args(v, u);
+    int updated = 0;
+    for (long long d = (long long)blockIdx.x * kSelectWarps + warp; d < n; d += (long long)gridDim.x * kSelectWarps)
+        updated += select_group<S>(sa, v, a, u.xlist[d], hist[warp], lane);
     cta_add(&s_updated, updated, &u.ctl->n_updated);
 }
 
@@ -701,7 +741,7 @@ __global__ void batch_prepare_kernel(StepWork w) {
 
 // Work items a pass has in one scene (read by thread 0 after the previous
 // pass completed).
-enum MultiPass : int { kPassFinishPairs, kPassFinishSingle, kPassGroup };
+enum MultiPass : int { kPassFinishPairs, kPassFinishSingle, kPassGroup, kPassSelect };
 
 template <int PASS>
 __device__ __forceinline__ int scene_items(const SceneWork& sw) {
@@ -714,6 +754,7 @@ __device__ __forceinline__ int scene_items(const SceneWork& sw) {
         return PASS == kPassFinishPairs ? (nt + 1) / 2 : nt;
     }
     if (c->n_crossing == 0ull) return 0;  // no voxel crossed the cap in this scene
+    if (PASS == kPassSelect) return (int)min((long long)c->n_crossing, (long long)sw.u.xlist_cap);
     return (int)(((uint32_t)sw.n_slots + kGroupThreads * kGroupPerThread - 1) /
                  (kGroupThreads * kGroupPerThread));
 }
@@ -830,6 +871,31 @@ group_multi_kernel(StepWork w) {
     }
 }
 
+// The ordered selection of every scene's cap-crossing voxels: warp work
+// items, one per listed voxel (OSN_SPLIT_SELECT).
+template <int S>
+__global__ void __launch_bounds__(kSelectThreads)
+select_multi_kernel(StepWork w) {
+    __shared__ uint32_t hist[kSelectWarps][256];
+    __shared__ int s_begin[kMaxBatchScenes + 1];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    launch_dependents();
+    grid_dependency_wait();
+    scene_prefix<kPassSelect>(w, s_begin);
+    const int total = s_begin[w.n_scenes];
+    for (;;) {
+        int item = 0;
+        if (lane == 0) item = (int)atomicAdd(&w.queues[kQSelect], 1u);
+        item = __shfl_sync(0xffffffffu, item, 0);
+        if (item >= total) break;
+        const int sc = scene_of(s_begin, w.n_scenes, item);
+        const SceneWork& sw = w.scenes[sc];
+        const int done = select_group<S>(select_args(sw.v, sw.u), sw.v, sw.a, sw.u.xlist[item - s_begin[sc]],
+                                         hist[warp], lane);
+        if (done) atomicAdd(&sw.u.ctl->n_updated, 1);
+    }
+}
+
 }  // namespace
 
 // CTAs of Kernel resident at once on the device (one wave), queried once
@@ -876,6 +942,23 @@ cudaError_t launch_group(const DevVolume& v, const BatchArgs& a, const UpdateScr
     }
 }
 
+cudaError_t launch_select(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u, int sm_count,
+                          cudaStream_t s) {
+    if (!OSN_SPLIT_SELECT) return cudaSuccess;  // the group pass selects
+    switch (v.storage) {
+        case kStoreF16U16:
+            return launch_after(select_kernel<kStoreF16U16>,
+                                resident_grid<select_kernel<kStoreF16U16>>(kSelectThreads, sm_count),
+                                kSelectThreads, s, v, a, u);
+        case kStoreF64:
+            return launch_after(select_kernel<kStoreF64>, resident_grid<select_kernel<kStoreF64>>(kSelectThreads, sm_count),
+                                kSelectThreads, s, v, a, u);
+        default:
+            return launch_after(select_kernel<kStoreF32>, resident_grid<select_kernel<kStoreF32>>(kSelectThreads, sm_count),
+                                kSelectThreads, s, v, a, u);
+    }
+}
+
 cudaError_t launch_batch_prepare(const StepWork& w, cudaStream_t s) {
     return launch_after(batch_prepare_kernel, 1, 256, s, w);
 }
@@ -886,6 +969,11 @@ cudaError_t finish_multi_t(const StepWork& w, int sm_count, cudaStream_t s) {
     return launch_after(finish_multi_kernel<S, P>,
                         resident_grid<finish_multi_kernel<S, P>>(kFinishThreads, sm_count),
                         kFinishThreads, s, w);
+}
+template <int S>
+cudaError_t select_multi_t(const StepWork& w, int sm_count, cudaStream_t s) {
+    return launch_after(select_multi_kernel<S>, resident_grid<select_multi_kernel<S>>(kSelectThreads, sm_count),
+                        kSelectThreads, s, w);
 }
 template <int S>
 cudaError_t group_multi_t(const StepWork& w, int sm_count, cudaStream_t s) {
@@ -916,4 +1004,15 @@ cudaError_t launch_group_multi(const StepWork& w, int storage, int sm_count, cud
     }
 }
 
+}  // namespace osn_b200
+
+namespace osn_b200 {
+cudaError_t launch_select_multi(const StepWork& w, int storage, int sm_count, cudaStream_t s) {
+    if (!OSN_SPLIT_SELECT) return cudaSuccess;  // the group pass selects
+    switch (storage) {
+        case kStoreF16U16: return select_multi_t<kStoreF16U16>(w, sm_count, s);
+        case kStoreF64: return select_multi_t<kStoreF64>(w, sm_count, s);
+        default: return select_multi_t<kStoreF32>(w, sm_count, s);
+    }
+}
 }  // namespace osn_b200

@@ -13,9 +13,10 @@
 // array compiled into the library.
 //
 // The array is a file-scope __device__ variable of kNoAllocScratchBytes
-// (32 MiB + 256 bytes): the control counters, then kNoAllocMaxRecords 4-byte
+// (36 MiB + 256 bytes): the control counters, then kNoAllocMaxRecords 4-byte
 // band records, as many 4-byte normalised SDFs and as many 8-byte group
-// entries, i.e. batches with n_points * (2 * steps + 1) <= 2,097,152 (a
+// entries, and half as many 4-byte crossing-voxel entries, i.e. batches with
+// n_points * (2 * steps + 1) <= 2,097,152 (a
 // 480x360 frame at 9 band steps per point fits; a 640x480 frame must be
 // split in two). The per-voxel and per-block state the update also uses
 // belongs to the volume and was allocated with it. Every GPU on which the
@@ -41,8 +42,10 @@ constexpr int64_t kNoAllocMaxRecords = OSN_TSDF_NOALLOC_MAX_RECORDS;
 constexpr size_t kNoAllocRecordBytes = (size_t)kNoAllocMaxRecords * sizeof(uint32_t);
 constexpr size_t kNoAllocSlotValBytes = (size_t)kNoAllocMaxRecords * sizeof(float);
 constexpr size_t kNoAllocGroupBytes = (size_t)kNoAllocMaxRecords * sizeof(unsigned long long);
-constexpr size_t kNoAllocScratchBytes =
-    kNoAllocHeaderBytes + kNoAllocRecordBytes + kNoAllocSlotValBytes + kNoAllocGroupBytes;
+constexpr int64_t kNoAllocMaxCrossing = kNoAllocMaxRecords / 2;  // at least two records each
+constexpr size_t kNoAllocCrossBytes = (size_t)kNoAllocMaxCrossing * sizeof(uint32_t);
+constexpr size_t kNoAllocScratchBytes = kNoAllocHeaderBytes + kNoAllocRecordBytes + kNoAllocSlotValBytes +
+                                        kNoAllocGroupBytes + kNoAllocCrossBytes;
 static_assert(sizeof(UpdateControl) <= kNoAllocHeaderBytes, "control block must fit the header");
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
@@ -85,7 +88,10 @@ cudaError_t Volume::update_static_scratch(const BatchArgs& a, void* scratch) {
                      : reinterpret_cast<float*>(base + kNoAllocHeaderBytes + kNoAllocRecordBytes);
     u.grp = reinterpret_cast<unsigned long long*>(base + kNoAllocHeaderBytes + kNoAllocRecordBytes +
                                                   kNoAllocSlotValBytes);
+    u.xlist = reinterpret_cast<uint32_t*>(base + kNoAllocHeaderBytes + kNoAllocRecordBytes +
+                                          kNoAllocSlotValBytes + kNoAllocGroupBytes);
     u.record_cap = kNoAllocMaxRecords;
+    u.xlist_cap = kNoAllocMaxCrossing;
     // Only the control counters must start at zero (run_update clears them);
     // every record slot is rewritten before it is read, and group entries are
     // read only where this call placed them.

@@ -154,6 +154,7 @@ Volume::~Volume() {
     cudaFree(us_.records);
     cudaFree(us_.slot_val);
     cudaFree(us_.grp);
+    cudaFree(us_.xlist);
     cudaFree(mesh_posnor_);
     cudaFree(mesh_rgb_);
     cudaFree(mesh_ctl_);
@@ -235,17 +236,23 @@ bool Volume::ensure_records(int64_t n_records) {
     cudaFree(us_.records);
     cudaFree(us_.slot_val);
     cudaFree(us_.grp);
+    cudaFree(us_.xlist);
     us_.records = nullptr;
     us_.slot_val = nullptr;
     us_.grp = nullptr;
+    us_.xlist = nullptr;
     us_.record_cap = 0;
+    us_.xlist_cap = 0;
     if (cudaMalloc(&us_.records, (size_t)n_records * sizeof(uint32_t)) != cudaSuccess) return false;
     if (dv_.storage != kStoreF64 &&
         cudaMalloc(&us_.slot_val, (size_t)n_records * sizeof(float)) != cudaSuccess)
         return false;
     // Groups partition the records of crossing voxels: at most one place per record.
     if (cudaMalloc(&us_.grp, (size_t)n_records * sizeof(unsigned long long)) != cudaSuccess) return false;
+    const int64_t n_cross = n_records / 2 + 1;  // a crossing voxel holds at least two records
+    if (cudaMalloc(&us_.xlist, (size_t)n_cross * sizeof(uint32_t)) != cudaSuccess) return false;
     us_.record_cap = n_records;
+    us_.xlist_cap = n_cross;
     if (pipelined_) {  // the second set's records and slot values grow with the first
         cudaFree(us2_.records);
         cudaFree(us2_.slot_val);
@@ -376,6 +383,10 @@ cudaError_t Volume::run_update(const BatchArgs& a, const UpdateScratch& scratch,
     mark_start(kKGroup, tail);
     e = launch_group(dv_, a, u, tail);
     mark_end(kKGroup, tail);
+    if (e != cudaSuccess) return e;
+    mark_start(kKSelect, tail);
+    e = launch_select(dv_, a, u, sm_count_, tail);
+    mark_end(kKSelect, tail);
     if (e != cudaSuccess) return e;
     if (pipe) {
         if ((e = cudaEventRecord(tail_done_[p], tail_)) != cudaSuccess) return e;

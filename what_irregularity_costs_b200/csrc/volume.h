@@ -20,7 +20,7 @@ enum KernelId : int {
     kKFinish = 2,        // per touched block: finish every voxel that accepts all its records
     kKGroup = 3,         // records of voxels that cross the cap: grouped per voxel, ordered
                          // cap selection, voxel finished
-    kKUnused4 = 4,       // no longer launched (the selection runs inside the group pass)
+    kKSelect = 4,        // ordered cap selection of the crossing voxels (its own pass)
     kKExtract = 5,
     kKReset = 6,
     kKUnused7 = 7,       // no longer launched
@@ -87,6 +87,10 @@ struct UpdateScratch {
     // FP64 oracle, which recomputes both).
     unsigned long long* grp = nullptr;
     int64_t record_cap = 0;
+    // [xlist_cap] the voxels that cross the cap in this update (written by
+    // finish for the select pass); a crossing voxel has at least two records.
+    uint32_t* xlist = nullptr;
+    int64_t xlist_cap = 0;
     // Owned by the volume. Per voxel: zero between updates.
     uint32_t* vcnt = nullptr;            // records of the voxel in this batch (of a crossing voxel:
                                          // records still to be placed in its group)
@@ -312,6 +316,8 @@ cudaError_t launch_band_depth_frames(const DevVolume& v, const BatchArgs& a, con
 cudaError_t launch_finish(const DevVolume& v, const UpdateScratch& u, int sm_count, cudaStream_t s);
 cudaError_t launch_group(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
                          cudaStream_t s);
+cudaError_t launch_select(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u, int sm_count,
+                          cudaStream_t s);
 
 }  // namespace osn_b200
 
@@ -337,7 +343,7 @@ struct SceneWork {
 };
 
 // Work queues of one step, one counter per pass (zeroed by the prepare pass).
-enum BatchQueue : int { kQBand = 0, kQFinish, kQGroup, kNumBatchQueues };
+enum BatchQueue : int { kQBand = 0, kQFinish, kQGroup, kQSelect, kNumBatchQueues };
 
 // Tunable shape of a batched step (chosen by the batch autotuner).
 struct BatchShape {
@@ -359,5 +365,6 @@ cudaError_t launch_batch_prepare(const StepWork& w, cudaStream_t s);
 cudaError_t launch_band_multi(const StepWork& w, int storage, int probe, int sm_count, cudaStream_t s);
 cudaError_t launch_finish_multi(const StepWork& w, int storage, int pair, int sm_count, cudaStream_t s);
 cudaError_t launch_group_multi(const StepWork& w, int storage, int sm_count, cudaStream_t s);
+cudaError_t launch_select_multi(const StepWork& w, int storage, int sm_count, cudaStream_t s);
 
 }  // namespace osn_b200

@@ -20,9 +20,9 @@ from . import _lib
 
 MAX_FRAMES = 32  # OSN_TSDF_MAX_FRAMES: frames per integrate_frames call
 MAX_DEPTH_FRAMES = 16  # OSN_TSDF_MAX_DEPTH_FRAMES: images per integrate_depth_frames call
-# Kernel ids of the timing table (ids 4 and 7 are kept for the numbering and
-# record no launches: the ordered cap selection runs inside the group pass).
-KERNEL_NAMES = ["allocate", "band", "finish", "group", "unused4", "extract", "reset", "unused7"]
+# Kernel ids of the timing table (id 7 is kept for the numbering and records
+# no launches).
+KERNEL_NAMES = ["allocate", "band", "finish", "group", "select", "extract", "reset", "unused7"]
 
 # Voxel storage modes (OSN_TSDF_STORAGE_* in include/osn_tsdf_b200.h).
 STORAGE_FP32, STORAGE_FP16_U16, STORAGE_FP64 = 0, 1, 2
@@ -339,7 +339,7 @@ class CudaVolume:
         evict_chunks: arrays as (n, 512) per voxel array of the storage mode
         (tsdf, weight[, r, g, b]; FP16: float16 means and uint16 weights)."""
         pack = np.ascontiguousarray(pack, dtype=np.uint8)
-        n = int(pack[36:40].view(np.int32)[0])
+        n = int(pack[28:32].view(np.int32)[0])  # header: magic, version, storage, 3 floats, n
         off = 64
         coords = pack[off:off + 12 * n].view(np.int32).reshape(n, 3)
         off += 12 * n
