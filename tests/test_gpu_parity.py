@@ -334,18 +334,22 @@ def test_extract_device_and_rgb(cuda):
 
 
 def test_mesh_bitwise_when_voxels_bitwise(cuda):
-    """Where every voxel receives at most two contributions the float sums are
-    order-free, the voxel arrays are bit-identical, and so is the mesh."""
-    # A 21x21 grid of the reference's plane patch: rays 2.5 cm apart at 1 cm
-    # voxels, so no voxel meets more than two band samples (232 voxels meet two).
-    pts = oracle.plane_points(0.30, 0.25, 21)
-    gpu, ref = _pair(cuda, [(pts, (0.0, 0.0, 0.0))], 0.01, 1 << 12)
+    """Where every voxel receives one contribution the sums have nothing to
+    reorder, the voxel arrays are bit-identical, and so is the mesh. A 40x40
+    grid of points at voxel centres on the plane z = 0.305, seen from a
+    camera 100 m away on the axis: the rays are all but parallel, so each
+    band voxel meets exactly one sample, and the band is closed."""
+    i = np.arange(40, dtype=np.float32)
+    x = (i + np.float32(0.5)) * np.float32(0.01) - np.float32(0.2)
+    gx, gy = np.meshgrid(x, x)
+    pts = np.stack([gx.ravel(), gy.ravel(), np.full(gx.size, 0.305, np.float32)], 1).astype(np.float32)
+    gpu, ref = _pair(cuda, [(pts, (0.0, 0.0, -100.0))], 0.01, 1 << 12)
     _, rt, rw = [a for a in oracle_sorted(ref)[:3]]
-    assert rw.max() == 2, "the input must give some voxel two contributions, none more"
+    assert rw.max() == 1 and int((rw == 1).sum()) == 12800
     assert_same_voxels(gpu, ref, exact_tsdf=True)
     gm = gpu.extract_mesh(1 << 20, 0.5, 0.0)
     rm = ref.extract(0.5, 0.0, 1 << 20)
-    assert gm is not None and gm.shape[0] > 0
+    assert gm is not None and gm.shape[0] == rm.shape[0] == 36504
     assert np.array_equal(canonical_triangles(gm).view(np.uint32),
                           canonical_triangles(rm).view(np.uint32))
 
