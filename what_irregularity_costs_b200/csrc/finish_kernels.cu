@@ -682,8 +682,111 @@ group_kernel(DevVolume v, BatchArgs a, UpdateScratch u, uint32_t n_slots) {
     cta_add(&s_updated, updated, &u.ctl->n_updated);
 }
 
+constexpr int kRoundGroups = 8;  // small groups whose entries are in flight together
+
+// The ordered selection of up to 32 listed crossing voxels by one warp
+// (FP32 / FP16 storage): lane l owns voxel xlist[d0 + l]. Every lane loads
+// its voxel's group header (base, size), weight and stored TSDF at once;
+// the small groups' entries (at most 32 records: one per lane) are then
+// loaded eight groups at a time into registers and ranked there, so a round
+// waits for a handful of round trips instead of three per voxel; larger
+// groups are ranked by the whole warp afterwards; finally every lane
+// finishes its own voxel from the values it already holds. Returns the
+// voxels this lane finished.
+template <int S>
+__device__ __forceinline__ int select_round(const SelectArgs& sa, const uint32_t* xlist, long long d0,
+                                            long long n, uint32_t* hist, int lane) {
+    static_assert(S != kStoreF64, "the FP64 oracle ranks one voxel at a time");
+    const bool mine = d0 + lane < n;
+    const uint32_t vi = mine ? xlist[d0 + lane] : 0u;
+    unsigned long long h = 0ull;
+    float w0 = 0.0f, t0 = 0.0f;
+    if (mine) {
+        h = __ldcg(&sa.vacc[vi]);
+        if constexpr (S == kStoreF16U16) {
+            w0 = (float)reinterpret_cast<const unsigned short*>(sa.weight)[vi];
+            t0 = __half2float(reinterpret_cast<const __half*>(sa.tsdf)[vi]);
+        } else {
+            w0 = sa.weight[vi];
+            t0 = sa.tsdf[vi];
+        }
+    }
+    const uint32_t base = (uint32_t)(h >> 32) - 1u;
+    const int cnt = mine ? (int)(uint32_t)h : 0;
+    const int keep = accept_count(w0, sa.cap, cnt);
+    bool valid = mine && (uint64_t)base + (uint64_t)cnt <= (uint64_t)sa.record_cap;
+    if (mine && !valid) atomicOr(sa.status, kStatusScratchOverflow);  // counters left by a failed update
+    const int m = (int)min(32ll, n - d0);  // warp-uniform
+    long long my_fix = 0ll;
+    // Small groups, eight at a time: entry `lane` of each in a register.
+    for (int j0 = 0; j0 < m; j0 += kRoundGroups) {
+        unsigned long long e[kRoundGroups];
+        int nj[kRoundGroups];
+#pragma unroll
+        for (int r = 0; r < kRoundGroups; ++r) {
+            const int j = j0 + r;
+            const int src = j < m ? j : 0;
+            const uint32_t bj = __shfl_sync(0xffffffffu, base, src);
+            const int cj = __shfl_sync(0xffffffffu, valid ? cnt : 0, src);
+            nj[r] = (j < m && cj <= 32) ? cj : 0;
+            e[r] = lane < nj[r] ? __ldcg(sa.grp + bj + lane) : ~0ull;
+        }
+#pragma unroll
+        for (int r = 0; r < kRoundGroups; ++r) {
+            if (nj[r] == 0) continue;  // warp-uniform
+            const int j = j0 + r;
+            const int kj = __shfl_sync(0xffffffffu, keep, j);
+            uint32_t id;
+            long long val;
+            if (lane < nj[r]) {
+                id = (uint32_t)e[r];
+                val = to_fix(__uint_as_float((uint32_t)(e[r] >> 32)));
+            } else {
+                id = 0xFFFFFFFFu;
+                val = 0ll;
+            }
+            int rank = 0;
+            for (int q = 0; q < nj[r]; ++q) rank += __shfl_sync(0xffffffffu, id, q) < id ? 1 : 0;
+            long long fix = (lane < nj[r] && rank < kj) ? val : 0ll;
+            for (int o = 16; o > 0; o >>= 1) fix += __shfl_xor_sync(0xffffffffu, fix, o);
+            if (lane == j) my_fix = fix;
+        }
+    }
+    // Larger groups, one at a time by the whole warp.
+    unsigned large = __ballot_sync(0xffffffffu, valid && cnt > 32);
+    while (large) {
+        const int j = __ffs(large) - 1;
+        large &= large - 1u;
+        const uint32_t bj = __shfl_sync(0xffffffffu, base, j);
+        const int cj = __shfl_sync(0xffffffffu, cnt, j), kj = __shfl_sync(0xffffffffu, keep, j);
+        long long fix = large_group_sum<S>(DevVolume{}, BatchArgs{}, sa.grp + bj, cj, kj, hist, lane);
+        for (int o = 16; o > 0; o >>= 1) fix += __shfl_xor_sync(0xffffffffu, fix, o);
+        if (lane == j) my_fix = fix;
+    }
+    if (!mine) return 0;
+    // Finish the lane's voxel (finish_voxel with the values already loaded).
+    const int k = valid ? keep : 0;
+    const long long f = valid ? my_fix : 0ll;
+    if constexpr (S == kStoreF32) {
+        const float wn = __fadd_rn(w0, (float)k);
+        sa.tsdf[vi] = add_fix(t0, f);
+        sa.weight[vi] = wn;
+        const float c = __fmul_rn(128.0f, wn);
+        sa.r[vi] = c;
+        sa.g[vi] = c;
+        sa.b[vi] = c;
+    } else {
+        reinterpret_cast<__half*>(sa.tsdf)[vi] = __float2half_rn(new_mean_f16(t0, w0, k, f));
+        reinterpret_cast<unsigned short*>(sa.weight)[vi] = (unsigned short)__fadd_rn(w0, (float)k);
+    }
+    sa.vacc[vi] = 0ull;
+    sa.vcnt[vi] = 0u;
+    return 1;
+}
+
 // The ordered selection of every cap-crossing voxel of the batch, from the
-// list finish wrote: one warp per voxel (OSN_SPLIT_SELECT).
+// list finish wrote (OSN_SPLIT_SELECT): rounds of 32 voxels per warp; the
+// FP64 oracle storage, one voxel per warp.
 template <int S>
 __global__ void __launch_bounds__(kSelectThreads)
 select_kernel(DevVolume v, BatchArgs a, UpdateScratch u) {
@@ -696,9 +799,14 @@ select_kernel(DevVolume v, BatchArgs a, UpdateScratch u) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const long long n = min((long long)u.ctl->n_crossing, (long long)u.xlist_cap);
     const SelectArgs sa = select_args(v, u);
+    const long long gw = (long long)blockIdx.x * kSelectWarps + warp, nw = (long long)gridDim.x * kSelectWarps;
     int updated = 0;
-    for (long long d = (long long)blockIdx.x * kSelectWarps + warp; d < n; d += (long long)gridDim.x * kSelectWarps)
-        updated += select_group<S>(sa, v, a, u.xlist[d], hist[warp], lane);
+    if constexpr (S == kStoreF64) {
+        for (long long d = gw; d < n; d += nw) updated += select_group<S>(sa, v, a, u.xlist[d], hist[warp], lane);
+    } else {
+        for (long long d0 = 32 * gw; d0 < n; d0 += 32 * nw)
+            updated += select_round<S>(sa, u.xlist, d0, n, hist[warp], lane);
+    }
     cta_add(&s_updated, updated, &u.ctl->n_updated);
 }
 
@@ -754,7 +862,10 @@ __device__ __forceinline__ int scene_items(const SceneWork& sw) {
         return PASS == kPassFinishPairs ? (nt + 1) / 2 : nt;
     }
     if (c->n_crossing == 0ull) return 0;  // no voxel crossed the cap in this scene
-    if (PASS == kPassSelect) return (int)min((long long)c->n_crossing, (long long)sw.u.xlist_cap);
+    if (PASS == kPassSelect) {
+        const long long x = min((long long)c->n_crossing, (long long)sw.u.xlist_cap);
+        return (int)(sw.v.storage == kStoreF64 ? x : (x + 31) / 32);  // voxels, or rounds of 32
+    }
     return (int)(((uint32_t)sw.n_slots + kGroupThreads * kGroupPerThread - 1) /
                  (kGroupThreads * kGroupPerThread));
 }
@@ -890,9 +1001,16 @@ select_multi_kernel(StepWork w) {
         if (item >= total) break;
         const int sc = scene_of(s_begin, w.n_scenes, item);
         const SceneWork& sw = w.scenes[sc];
-        const int done = select_group<S>(select_args(sw.v, sw.u), sw.v, sw.a, sw.u.xlist[item - s_begin[sc]],
-                                         hist[warp], lane);
-        if (done) atomicAdd(&sw.u.ctl->n_updated, 1);
+        const SelectArgs sa = select_args(sw.v, sw.u);
+        int done;
+        if constexpr (S == kStoreF64) {
+            done = select_group<S>(sa, sw.v, sw.a, sw.u.xlist[item - s_begin[sc]], hist[warp], lane);
+        } else {
+            const long long n = min((long long)sw.u.ctl->n_crossing, (long long)sw.u.xlist_cap);
+            done = select_round<S>(sa, sw.u.xlist, 32ll * (item - s_begin[sc]), n, hist[warp], lane);
+        }
+        done = __reduce_add_sync(0xffffffffu, done);
+        if (lane == 0 && done) atomicAdd(&sw.u.ctl->n_updated, done);
     }
 }
 
