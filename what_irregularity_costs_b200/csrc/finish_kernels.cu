@@ -51,6 +51,7 @@
 // results do not depend on the order in which threads meet the records:
 // repeated runs are bit-identical, and a voxel with one contribution per
 // batch gets exactly the reference's fl(tsdf + sdf_n).
+#include <algorithm>
 #include <mutex>
 
 #include "volume.h"
@@ -586,11 +587,9 @@ __device__ __noinline__ int select_group_out(const SelectArgs sa, uint32_t vi, u
 // (warp-synchronous): records of voxels whose crossing bit is set take their
 // place in the voxel's group; the warp then selects and finishes every group
 // one of its records completed.
-template <int S>
-__device__ __forceinline__ void group_slots(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
-                                            uint32_t first, uint32_t n_slots, uint32_t* hist, int& updated) {
-    const int lane = threadIdx.x & 31;
-    uint32_t vi[kGroupPerThread];
+// The records of eight band slots from `first` (kNoVoxel past the batch).
+__device__ __forceinline__ void load_records(const UpdateScratch& u, uint32_t first, uint32_t n_slots,
+                                             uint32_t (&vi)[kGroupPerThread]) {
     if (first + kGroupPerThread <= n_slots) {
         // Eight consecutive band slots: one step, neighbouring points.
         const uint4 r0 = __ldcs(reinterpret_cast<const uint4*>(u.records + first));
@@ -602,6 +601,13 @@ __device__ __forceinline__ void group_slots(const DevVolume& v, const BatchArgs&
         for (int m = 0; m < kGroupPerThread; ++m)
             vi[m] = first + m < n_slots ? u.records[first + m] : kNoVoxel;
     }
+}
+
+// Records of voxels whose crossing bit is set take their place in the
+// voxel's group; returns bit m set for slot m placed.
+template <int S>
+__device__ __forceinline__ uint32_t place_records(const BatchArgs& a, const DevVolume& v, const UpdateScratch& u,
+                                                  uint32_t first, const uint32_t (&vi)[kGroupPerThread]) {
     // Crossing bits: one gather per distinct bitmap word among the eight.
     uint32_t word[kGroupPerThread];
     bool same[kGroupPerThread];
@@ -635,6 +641,16 @@ __device__ __forceinline__ void group_slots(const DevVolume& v, const BatchArgs&
         else atomicOr(u.status, kStatusScratchOverflow);  // state left by a failed update
         placed |= 1u << m;
     }
+    return placed;
+}
+
+template <int S>
+__device__ __forceinline__ void group_slots(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
+                                            uint32_t first, uint32_t n_slots, uint32_t* hist, int& updated) {
+    const int lane = threadIdx.x & 31;
+    uint32_t vi[kGroupPerThread];
+    load_records(u, first, n_slots, vi);
+    const uint32_t placed = place_records<S>(a, v, u, first, vi);
     if (OSN_SPLIT_SELECT) return;  // the select pass ranks the complete groups
     // Fused selection: this thread's entries are visible before its
     // countdowns; the record that brings a count to zero completed its group.
@@ -677,27 +693,43 @@ group_kernel(DevVolume v, BatchArgs a, UpdateScratch u, uint32_t n_slots) {
     grid_dependency_wait();
     if (u.ctl->n_crossing == 0ull) return;  // no voxel crossed the cap in this batch
     int updated = 0;
-    group_slots<S>(v, a, u, (blockIdx.x * kGroupThreads + threadIdx.x) * kGroupPerThread, n_slots,
-                   hist[threadIdx.x >> 5], updated);
+    if (OSN_SPLIT_SELECT) {
+        // Persistent grid: each thread walks chunks of eight slots a grid
+        // apart, the next chunk's records loaded before this one's are placed.
+        const uint32_t stride = gridDim.x * kGroupThreads * kGroupPerThread;
+        uint32_t first = (blockIdx.x * kGroupThreads + threadIdx.x) * kGroupPerThread;
+        uint32_t cur[kGroupPerThread], nxt[kGroupPerThread];
+        load_records(u, first, n_slots, cur);
+        for (; first < n_slots; first += stride) {
+            load_records(u, first + stride, n_slots, nxt);
+            place_records<S>(a, v, u, first, cur);
+#pragma unroll
+            for (int m = 0; m < kGroupPerThread; ++m) cur[m] = nxt[m];
+        }
+    } else {
+        group_slots<S>(v, a, u, (blockIdx.x * kGroupThreads + threadIdx.x) * kGroupPerThread, n_slots,
+                       hist[threadIdx.x >> 5], updated);
+    }
     cta_add(&s_updated, updated, &u.ctl->n_updated);
 }
 
-constexpr int kRoundGroups = 8;  // small groups whose entries are in flight together
+constexpr int kRoundVoxels = 8;  // crossing voxels per warp round
 
-// The ordered selection of up to 32 listed crossing voxels by one warp
-// (FP32 / FP16 storage): lane l owns voxel xlist[d0 + l]. Every lane loads
-// its voxel's group header (base, size), weight and stored TSDF at once;
-// the small groups' entries (at most 32 records: one per lane) are then
-// loaded eight groups at a time into registers and ranked there, so a round
-// waits for a handful of round trips instead of three per voxel; larger
-// groups are ranked by the whole warp afterwards; finally every lane
-// finishes its own voxel from the values it already holds. Returns the
-// voxels this lane finished.
+// The ordered selection of up to eight listed crossing voxels by one warp
+// (FP32 / FP16 storage): lane l < 8 owns voxel xlist[d0 + l]. Those lanes
+// load their voxels' group headers (base, size), weights and stored TSDFs at
+// once; the small groups' entries (at most 32 records: one per lane) are
+// then all loaded together into registers and ranked there, so a round waits
+// for three round trips whatever its voxels; larger groups are ranked by the
+// whole warp afterwards; finally each owning lane finishes its voxel from the
+// values it already holds. Rounds of eight keep a warp's serial ranking work
+// short and give every resident warp a round. Returns the voxels this lane
+// finished.
 template <int S>
 __device__ __forceinline__ int select_round(const SelectArgs& sa, const uint32_t* xlist, long long d0,
                                             long long n, uint32_t* hist, int lane) {
     static_assert(S != kStoreF64, "the FP64 oracle ranks one voxel at a time");
-    const bool mine = d0 + lane < n;
+    const bool mine = lane < kRoundVoxels && d0 + lane < n;
     const uint32_t vi = mine ? xlist[d0 + lane] : 0u;
     unsigned long long h = 0ull;
     float w0 = 0.0f, t0 = 0.0f;
@@ -716,14 +748,15 @@ __device__ __forceinline__ int select_round(const SelectArgs& sa, const uint32_t
     const int keep = accept_count(w0, sa.cap, cnt);
     bool valid = mine && (uint64_t)base + (uint64_t)cnt <= (uint64_t)sa.record_cap;
     if (mine && !valid) atomicOr(sa.status, kStatusScratchOverflow);  // counters left by a failed update
-    const int m = (int)min(32ll, n - d0);  // warp-uniform
+    const int m = (int)min((long long)kRoundVoxels, n - d0);  // warp-uniform
     long long my_fix = 0ll;
-    // Small groups, eight at a time: entry `lane` of each in a register.
-    for (int j0 = 0; j0 < m; j0 += kRoundGroups) {
-        unsigned long long e[kRoundGroups];
-        int nj[kRoundGroups];
+    // Small groups: entry `lane` of each in a register, all loads in flight.
+    {
+        constexpr int j0 = 0;
+        unsigned long long e[kRoundVoxels];
+        int nj[kRoundVoxels];
 #pragma unroll
-        for (int r = 0; r < kRoundGroups; ++r) {
+        for (int r = 0; r < kRoundVoxels; ++r) {
             const int j = j0 + r;
             const int src = j < m ? j : 0;
             const uint32_t bj = __shfl_sync(0xffffffffu, base, src);
@@ -732,7 +765,7 @@ __device__ __forceinline__ int select_round(const SelectArgs& sa, const uint32_t
             e[r] = lane < nj[r] ? __ldcg(sa.grp + bj + lane) : ~0ull;
         }
 #pragma unroll
-        for (int r = 0; r < kRoundGroups; ++r) {
+        for (int r = 0; r < kRoundVoxels; ++r) {
             if (nj[r] == 0) continue;  // warp-uniform
             const int j = j0 + r;
             const int kj = __shfl_sync(0xffffffffu, keep, j);
@@ -785,8 +818,8 @@ __device__ __forceinline__ int select_round(const SelectArgs& sa, const uint32_t
 }
 
 // The ordered selection of every cap-crossing voxel of the batch, from the
-// list finish wrote (OSN_SPLIT_SELECT): rounds of 32 voxels per warp; the
-// FP64 oracle storage, one voxel per warp.
+// list finish wrote (OSN_SPLIT_SELECT): rounds of eight voxels per warp;
+// the FP64 oracle storage, one voxel per warp.
 template <int S>
 __global__ void __launch_bounds__(kSelectThreads)
 select_kernel(DevVolume v, BatchArgs a, UpdateScratch u) {
@@ -804,7 +837,7 @@ select_kernel(DevVolume v, BatchArgs a, UpdateScratch u) {
     if constexpr (S == kStoreF64) {
         for (long long d = gw; d < n; d += nw) updated += select_group<S>(sa, v, a, u.xlist[d], hist[warp], lane);
     } else {
-        for (long long d0 = 32 * gw; d0 < n; d0 += 32 * nw)
+        for (long long d0 = kRoundVoxels * gw; d0 < n; d0 += kRoundVoxels * nw)
             updated += select_round<S>(sa, u.xlist, d0, n, hist[warp], lane);
     }
     cta_add(&s_updated, updated, &u.ctl->n_updated);
@@ -864,7 +897,7 @@ __device__ __forceinline__ int scene_items(const SceneWork& sw) {
     if (c->n_crossing == 0ull) return 0;  // no voxel crossed the cap in this scene
     if (PASS == kPassSelect) {
         const long long x = min((long long)c->n_crossing, (long long)sw.u.xlist_cap);
-        return (int)(sw.v.storage == kStoreF64 ? x : (x + 31) / 32);  // voxels, or rounds of 32
+        return (int)(sw.v.storage == kStoreF64 ? x : (x + kRoundVoxels - 1) / kRoundVoxels);  // voxels, or rounds
     }
     return (int)(((uint32_t)sw.n_slots + kGroupThreads * kGroupPerThread - 1) /
                  (kGroupThreads * kGroupPerThread));
@@ -1007,7 +1040,8 @@ select_multi_kernel(StepWork w) {
             done = select_group<S>(sa, sw.v, sw.a, sw.u.xlist[item - s_begin[sc]], hist[warp], lane);
         } else {
             const long long n = min((long long)sw.u.ctl->n_crossing, (long long)sw.u.xlist_cap);
-            done = select_round<S>(sa, sw.u.xlist, 32ll * (item - s_begin[sc]), n, hist[warp], lane);
+            done = select_round<S>(sa, sw.u.xlist, (long long)kRoundVoxels * (item - s_begin[sc]), n, hist[warp],
+                                   lane);
         }
         done = __reduce_add_sync(0xffffffffu, done);
         if (lane == 0 && done) atomicAdd(&sw.u.ctl->n_updated, done);
@@ -1047,12 +1081,18 @@ cudaError_t launch_finish(const DevVolume& v, const UpdateScratch& u, int sm_cou
     }
 }
 
-cudaError_t launch_group(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
+cudaError_t launch_group(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u, int sm_count,
                          cudaStream_t s) {
     const uint32_t n_slots = (uint32_t)a.n * (2u * (uint32_t)v.steps + 1u);
     if (n_slots == 0) return cudaSuccess;
     const uint32_t per_cta = kGroupThreads * (uint32_t)kGroupPerThread;
-    const uint32_t grid = (n_slots + per_cta - 1u) / per_cta;
+    uint32_t grid = (n_slots + per_cta - 1u) / per_cta;
+    if (OSN_SPLIT_SELECT) {  // persistent: at most one resident wave
+        const int res = v.storage == kStoreF16U16 ? resident_grid<group_kernel<kStoreF16U16>>(kGroupThreads, sm_count)
+                        : v.storage == kStoreF64  ? resident_grid<group_kernel<kStoreF64>>(kGroupThreads, sm_count)
+                                                  : resident_grid<group_kernel<kStoreF32>>(kGroupThreads, sm_count);
+        grid = std::min<uint32_t>(grid, (uint32_t)res);
+    }
     switch (v.storage) {
         case kStoreF16U16: return launch_after(group_kernel<kStoreF16U16>, grid, kGroupThreads, s, v, a, u, n_slots);
         case kStoreF64: return launch_after(group_kernel<kStoreF64>, grid, kGroupThreads, s, v, a, u, n_slots);

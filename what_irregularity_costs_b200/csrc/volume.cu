@@ -381,7 +381,7 @@ cudaError_t Volume::run_update(const BatchArgs& a, const UpdateScratch& scratch,
     mark_end(kKFinish, tail);
     if (e != cudaSuccess) return e;
     mark_start(kKGroup, tail);
-    e = launch_group(dv_, a, u, tail);
+    e = launch_group(dv_, a, u, sm_count_, tail);
     mark_end(kKGroup, tail);
     if (e != cudaSuccess) return e;
     mark_start(kKSelect, tail);

@@ -314,7 +314,7 @@ cudaError_t launch_band_depth_frames(const DevVolume& v, const BatchArgs& a, con
                                      const FrameCam* d_frames, const FramePose* d_poses, int32_t n_frames,
                                      int sm_count, cudaStream_t s);
 cudaError_t launch_finish(const DevVolume& v, const UpdateScratch& u, int sm_count, cudaStream_t s);
-cudaError_t launch_group(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u,
+cudaError_t launch_group(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u, int sm_count,
                          cudaStream_t s);
 cudaError_t launch_select(const DevVolume& v, const BatchArgs& a, const UpdateScratch& u, int sm_count,
                           cudaStream_t s);
