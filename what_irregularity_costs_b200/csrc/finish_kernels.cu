@@ -72,6 +72,11 @@ constexpr int kRankRegs = 8;        // groups of up to 32 * 8 records are ranked
 #ifndef OSN_SPLIT_SELECT
 #define OSN_SPLIT_SELECT 1
 #endif
+// The group pass as a persistent grid whose threads load their next chunk of
+// records before placing the current one (1), or one chunk per thread (0).
+#ifndef OSN_GROUP_PERSISTENT
+#define OSN_GROUP_PERSISTENT 0
+#endif
 constexpr int kSelectThreads = 128;
 constexpr int kSelectWarps = kSelectThreads / 32;
 // Resident 256-thread CTAs per SM the group pass's registers are sized for:
@@ -693,7 +698,7 @@ group_kernel(DevVolume v, BatchArgs a, UpdateScratch u, uint32_t n_slots) {
     grid_dependency_wait();
     if (u.ctl->n_crossing == 0ull) return;  // no voxel crossed the cap in this batch
     int updated = 0;
-    if (OSN_SPLIT_SELECT) {
+    if (OSN_SPLIT_SELECT && OSN_GROUP_PERSISTENT) {
         // Persistent grid: each thread walks chunks of eight slots a grid
         // apart, the next chunk's records loaded before this one's are placed.
         const uint32_t stride = gridDim.x * kGroupThreads * kGroupPerThread;
@@ -713,113 +718,112 @@ group_kernel(DevVolume v, BatchArgs a, UpdateScratch u, uint32_t n_slots) {
     cta_add(&s_updated, updated, &u.ctl->n_updated);
 }
 
-constexpr int kRoundVoxels = 8;  // crossing voxels per warp round
+constexpr int kSelectChunk = 32;   // voxels whose headers a warp loads together (one per lane)
+constexpr int kSelectAhead = 4;    // groups whose entries are in flight ahead of the ranking
 
-// The ordered selection of up to eight listed crossing voxels by one warp
-// (FP32 / FP16 storage): lane l < 8 owns voxel xlist[d0 + l]. Those lanes
-// load their voxels' group headers (base, size), weights and stored TSDFs at
-// once; the small groups' entries (at most 32 records: one per lane) are
-// then all loaded together into registers and ranked there, so a round waits
-// for three round trips whatever its voxels; larger groups are ranked by the
-// whole warp afterwards; finally each owning lane finishes its voxel from the
-// values it already holds. Rounds of eight keep a warp's serial ranking work
-// short and give every resident warp a round. Returns the voxels this lane
-// finished.
+// Entry `lane` of group j of a chunk (groups of at most 32 records; none for
+// larger or invalid groups).
+__device__ __forceinline__ unsigned long long chunk_entry(const SelectArgs& sa, uint32_t base, int cnt, int j,
+                                                          int m, int lane) {
+    const int src = j < m ? j : 0;
+    const uint32_t bj = __shfl_sync(0xffffffffu, base, src);
+    const int cj = __shfl_sync(0xffffffffu, cnt, src);
+    return (j < m && lane < cj && cj <= 32) ? __ldcg(sa.grp + bj + lane) : ~0ull;
+}
+
+// The ordered selection of listed crossing voxels d0, d0 + step, ... < end
+// by one warp (FP32 / FP16 storage). The warp takes up to 32 of them at a
+// time, lane k owning the k-th: each lane loads its voxel's list entry,
+// then its group header (base, size), weight and stored TSDF, all lanes
+// together; the warp then ranks the groups in order, each group's entries
+// (at most 32 records: one per lane) loaded four groups ahead of the
+// ranking, larger groups by the whole warp on the spot; finally each lane
+// finishes its own voxel from the values it already holds. Returns the
+// voxels this lane finished.
 template <int S>
-__device__ __forceinline__ int select_round(const SelectArgs& sa, const uint32_t* xlist, long long d0,
-                                            long long n, uint32_t* hist, int lane) {
+__device__ __forceinline__ int select_stream(const SelectArgs& sa, const uint32_t* xlist, long long d0,
+                                             long long end, long long step, uint32_t* hist, int lane) {
     static_assert(S != kStoreF64, "the FP64 oracle ranks one voxel at a time");
-    const bool mine = lane < kRoundVoxels && d0 + lane < n;
-    const uint32_t vi = mine ? xlist[d0 + lane] : 0u;
-    unsigned long long h = 0ull;
-    float w0 = 0.0f, t0 = 0.0f;
-    if (mine) {
-        h = __ldcg(&sa.vacc[vi]);
-        if constexpr (S == kStoreF16U16) {
-            w0 = (float)reinterpret_cast<const unsigned short*>(sa.weight)[vi];
-            t0 = __half2float(reinterpret_cast<const __half*>(sa.tsdf)[vi]);
-        } else {
-            w0 = sa.weight[vi];
-            t0 = sa.tsdf[vi];
-        }
-    }
-    const uint32_t base = (uint32_t)(h >> 32) - 1u;
-    const int cnt = mine ? (int)(uint32_t)h : 0;
-    const int keep = accept_count(w0, sa.cap, cnt);
-    bool valid = mine && (uint64_t)base + (uint64_t)cnt <= (uint64_t)sa.record_cap;
-    if (mine && !valid) atomicOr(sa.status, kStatusScratchOverflow);  // counters left by a failed update
-    const int m = (int)min((long long)kRoundVoxels, n - d0);  // warp-uniform
-    long long my_fix = 0ll;
-    // Small groups: entry `lane` of each in a register, all loads in flight.
-    {
-        constexpr int j0 = 0;
-        unsigned long long e[kRoundVoxels];
-        int nj[kRoundVoxels];
-#pragma unroll
-        for (int r = 0; r < kRoundVoxels; ++r) {
-            const int j = j0 + r;
-            const int src = j < m ? j : 0;
-            const uint32_t bj = __shfl_sync(0xffffffffu, base, src);
-            const int cj = __shfl_sync(0xffffffffu, valid ? cnt : 0, src);
-            nj[r] = (j < m && cj <= 32) ? cj : 0;
-            e[r] = lane < nj[r] ? __ldcg(sa.grp + bj + lane) : ~0ull;
-        }
-#pragma unroll
-        for (int r = 0; r < kRoundVoxels; ++r) {
-            if (nj[r] == 0) continue;  // warp-uniform
-            const int j = j0 + r;
-            const int kj = __shfl_sync(0xffffffffu, keep, j);
-            uint32_t id;
-            long long val;
-            if (lane < nj[r]) {
-                id = (uint32_t)e[r];
-                val = to_fix(__uint_as_float((uint32_t)(e[r] >> 32)));
+    int done = 0;
+    for (long long c0 = d0; c0 < end; c0 += kSelectChunk * step) {
+        const long long dk = c0 + (long long)lane * step;
+        const bool mine = dk < end;
+        const uint32_t vi = mine ? xlist[dk] : 0u;
+        unsigned long long h = 0ull;
+        float w0 = 0.0f, t0 = 0.0f;
+        if (mine) {
+            h = __ldcg(&sa.vacc[vi]);
+            if constexpr (S == kStoreF16U16) {
+                w0 = (float)reinterpret_cast<const unsigned short*>(sa.weight)[vi];
+                t0 = __half2float(reinterpret_cast<const __half*>(sa.tsdf)[vi]);
             } else {
-                id = 0xFFFFFFFFu;
-                val = 0ll;
+                w0 = sa.weight[vi];
+                t0 = sa.tsdf[vi];
             }
-            int rank = 0;
-            for (int q = 0; q < nj[r]; ++q) rank += __shfl_sync(0xffffffffu, id, q) < id ? 1 : 0;
-            long long fix = (lane < nj[r] && rank < kj) ? val : 0ll;
+        }
+        const uint32_t base = (uint32_t)(h >> 32) - 1u;
+        const bool valid = mine && (uint64_t)base + (uint64_t)(uint32_t)h <= (uint64_t)sa.record_cap;
+        if (mine && !valid) atomicOr(sa.status, kStatusScratchOverflow);  // counters left by a failed update
+        const int cnt = valid ? (int)(uint32_t)h : 0;
+        const int keep = accept_count(w0, sa.cap, cnt);
+        const int m = (int)min((long long)kSelectChunk, (end - c0 + step - 1) / step);  // warp-uniform
+        unsigned long long e0 = chunk_entry(sa, base, cnt, 0, m, lane);
+        unsigned long long e1 = chunk_entry(sa, base, cnt, 1, m, lane);
+        unsigned long long e2 = chunk_entry(sa, base, cnt, 2, m, lane);
+        unsigned long long e3 = chunk_entry(sa, base, cnt, 3, m, lane);
+        long long my_fix = 0ll;
+        for (int j = 0; j < m; ++j) {
+            const unsigned long long ej = e0;
+            e0 = e1;
+            e1 = e2;
+            e2 = e3;
+            e3 = chunk_entry(sa, base, cnt, j + kSelectAhead, m, lane);
+            const int cj = __shfl_sync(0xffffffffu, cnt, j);
+            const int kj = __shfl_sync(0xffffffffu, keep, j);
+            long long fix = 0ll;
+            if (cj <= 32) {  // warp-uniform
+                const uint32_t id = lane < cj ? (uint32_t)ej : 0xFFFFFFFFu;
+                int rank = 0;
+#pragma unroll
+                for (int q = 0; q < 32; ++q) {
+                    const uint32_t other = __shfl_sync(0xffffffffu, id, q);
+                    rank += (q < cj && other < id) ? 1 : 0;
+                }
+                if (lane < cj && rank < kj) fix = to_fix(__uint_as_float((uint32_t)(ej >> 32)));
+            } else {
+                const uint32_t bj = __shfl_sync(0xffffffffu, base, j);
+                fix = large_group_sum<S>(DevVolume{}, BatchArgs{}, sa.grp + bj, cj, kj, hist, lane);
+            }
             for (int o = 16; o > 0; o >>= 1) fix += __shfl_xor_sync(0xffffffffu, fix, o);
             if (lane == j) my_fix = fix;
         }
+        if (!mine) continue;
+        // Finish the lane's voxel (finish_voxel with the values already loaded).
+        const int k = valid ? keep : 0;
+        const long long f = valid ? my_fix : 0ll;
+        if constexpr (S == kStoreF32) {
+            const float wn = __fadd_rn(w0, (float)k);
+            sa.tsdf[vi] = add_fix(t0, f);
+            sa.weight[vi] = wn;
+            const float c = __fmul_rn(128.0f, wn);
+            sa.r[vi] = c;
+            sa.g[vi] = c;
+            sa.b[vi] = c;
+        } else {
+            reinterpret_cast<__half*>(sa.tsdf)[vi] = __float2half_rn(new_mean_f16(t0, w0, k, f));
+            reinterpret_cast<unsigned short*>(sa.weight)[vi] = (unsigned short)__fadd_rn(w0, (float)k);
+        }
+        sa.vacc[vi] = 0ull;
+        sa.vcnt[vi] = 0u;
+        ++done;
     }
-    // Larger groups, one at a time by the whole warp.
-    unsigned large = __ballot_sync(0xffffffffu, valid && cnt > 32);
-    while (large) {
-        const int j = __ffs(large) - 1;
-        large &= large - 1u;
-        const uint32_t bj = __shfl_sync(0xffffffffu, base, j);
-        const int cj = __shfl_sync(0xffffffffu, cnt, j), kj = __shfl_sync(0xffffffffu, keep, j);
-        long long fix = large_group_sum<S>(DevVolume{}, BatchArgs{}, sa.grp + bj, cj, kj, hist, lane);
-        for (int o = 16; o > 0; o >>= 1) fix += __shfl_xor_sync(0xffffffffu, fix, o);
-        if (lane == j) my_fix = fix;
-    }
-    if (!mine) return 0;
-    // Finish the lane's voxel (finish_voxel with the values already loaded).
-    const int k = valid ? keep : 0;
-    const long long f = valid ? my_fix : 0ll;
-    if constexpr (S == kStoreF32) {
-        const float wn = __fadd_rn(w0, (float)k);
-        sa.tsdf[vi] = add_fix(t0, f);
-        sa.weight[vi] = wn;
-        const float c = __fmul_rn(128.0f, wn);
-        sa.r[vi] = c;
-        sa.g[vi] = c;
-        sa.b[vi] = c;
-    } else {
-        reinterpret_cast<__half*>(sa.tsdf)[vi] = __float2half_rn(new_mean_f16(t0, w0, k, f));
-        reinterpret_cast<unsigned short*>(sa.weight)[vi] = (unsigned short)__fadd_rn(w0, (float)k);
-    }
-    sa.vacc[vi] = 0ull;
-    sa.vcnt[vi] = 0u;
-    return 1;
+    return done;
 }
 
 // The ordered selection of every cap-crossing voxel of the batch, from the
-// list finish wrote (OSN_SPLIT_SELECT): rounds of eight voxels per warp;
-// the FP64 oracle storage, one voxel per warp.
+// list finish wrote (OSN_SPLIT_SELECT): warp w takes voxels w, w + warps,
+// ... (so large groups spread over the grid); the FP64 oracle storage, one
+// voxel at a time.
 template <int S>
 __global__ void __launch_bounds__(kSelectThreads)
 select_kernel(DevVolume v, BatchArgs a, UpdateScratch u) {
@@ -837,8 +841,7 @@ select_kernel(DevVolume v, BatchArgs a, UpdateScratch u) {
     if constexpr (S == kStoreF64) {
         for (long long d = gw; d < n; d += nw) updated += select_group<S>(sa, v, a, u.xlist[d], hist[warp], lane);
     } else {
-        for (long long d0 = kRoundVoxels * gw; d0 < n; d0 += kRoundVoxels * nw)
-            updated += select_round<S>(sa, u.xlist, d0, n, hist[warp], lane);
+        updated += select_stream<S>(sa, u.xlist, gw, n, nw, hist[warp], lane);
     }
     cta_add(&s_updated, updated, &u.ctl->n_updated);
 }
@@ -897,7 +900,7 @@ __device__ __forceinline__ int scene_items(const SceneWork& sw) {
     if (c->n_crossing == 0ull) return 0;  // no voxel crossed the cap in this scene
     if (PASS == kPassSelect) {
         const long long x = min((long long)c->n_crossing, (long long)sw.u.xlist_cap);
-        return (int)(sw.v.storage == kStoreF64 ? x : (x + kRoundVoxels - 1) / kRoundVoxels);  // voxels, or rounds
+        return (int)(sw.v.storage == kStoreF64 ? x : (x + kSelectChunk - 1) / kSelectChunk);  // voxels, or chunks
     }
     return (int)(((uint32_t)sw.n_slots + kGroupThreads * kGroupPerThread - 1) /
                  (kGroupThreads * kGroupPerThread));
@@ -1040,8 +1043,8 @@ select_multi_kernel(StepWork w) {
             done = select_group<S>(sa, sw.v, sw.a, sw.u.xlist[item - s_begin[sc]], hist[warp], lane);
         } else {
             const long long n = min((long long)sw.u.ctl->n_crossing, (long long)sw.u.xlist_cap);
-            done = select_round<S>(sa, sw.u.xlist, (long long)kRoundVoxels * (item - s_begin[sc]), n, hist[warp],
-                                   lane);
+            const long long c0 = (long long)kSelectChunk * (item - s_begin[sc]);
+            done = select_stream<S>(sa, sw.u.xlist, c0, min(n, c0 + kSelectChunk), 1, hist[warp], lane);
         }
         done = __reduce_add_sync(0xffffffffu, done);
         if (lane == 0 && done) atomicAdd(&sw.u.ctl->n_updated, done);
@@ -1087,7 +1090,7 @@ cudaError_t launch_group(const DevVolume& v, const BatchArgs& a, const UpdateScr
     if (n_slots == 0) return cudaSuccess;
     const uint32_t per_cta = kGroupThreads * (uint32_t)kGroupPerThread;
     uint32_t grid = (n_slots + per_cta - 1u) / per_cta;
-    if (OSN_SPLIT_SELECT) {  // persistent: at most one resident wave
+    if (OSN_SPLIT_SELECT && OSN_GROUP_PERSISTENT) {  // persistent: at most one resident wave
         const int res = v.storage == kStoreF16U16 ? resident_grid<group_kernel<kStoreF16U16>>(kGroupThreads, sm_count)
                         : v.storage == kStoreF64  ? resident_grid<group_kernel<kStoreF64>>(kGroupThreads, sm_count)
                                                   : resident_grid<group_kernel<kStoreF32>>(kGroupThreads, sm_count);
