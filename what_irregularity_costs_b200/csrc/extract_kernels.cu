@@ -108,13 +108,21 @@ __device__ __forceinline__ Vert interp(const Halo<COL>& h, const Cube& q, float 
 }
 
 // Where a CTA's vertices go: the block's output range is contiguous, so its
-// first kStageVerts vertices are staged in shared memory (with the range's
+// first stage_verts vertices are staged in shared memory (with the range's
 // offset inside its 16-byte group, so the copy-out is aligned) and written
 // out by the whole CTA with 16-byte streaming stores; any further vertices
 // of an unusually dense block go straight to global memory. The instance
 // with colours stages fewer (its halo holds the colours too).
 template <bool COL>
 __host__ __device__ constexpr int stage_verts() { return COL ? 1024 : 1536; }
+// A cube emits at most 6 tetrahedra x 2 triangles.
+constexpr int kMaxBlockTris = kBlockVoxels * 12;
+// Dynamic shared memory of one CTA: the vertex stage (pad + stage_verts * 6
+// floats), then the block's triangle list (one 16-bit item per triangle).
+template <bool COL>
+__host__ __device__ constexpr int extract_dyn_smem() {
+    return (4 + stage_verts<COL>() * 6) * 4 + kMaxBlockTris * 2;
+}
 template <bool COL>
 struct VertexSink {
     float* stage;     // shared: [pad + stage_verts * 6]
@@ -171,7 +179,10 @@ __global__ void __launch_bounds__(kExtractThreads, COL ? 1 : OSN_EXTRACT_MIN_BLO
 extract_kernel(DevVolume v, int32_t n_blocks, const int32_t* list, float min_w, float iso, float* out_posnor,
                uint8_t* out_rgb, int32_t cap, int32_t* ctl) {
     __shared__ Halo<COL> h;
-    __shared__ __align__(16) float s_stage[4 + stage_verts<COL>() * 6];
+    __shared__ uint8_t s_below[kBlockVoxels];
+    extern __shared__ __align__(16) float s_dyn[];
+    float* const s_stage = s_dyn;
+    uint16_t* const s_items = reinterpret_cast<uint16_t*>(s_dyn + 4 + stage_verts<COL>() * 6);
     __shared__ int s_nb[8];
     __shared__ int s_warp[kExtractThreads / 32];
     __shared__ int s_base, s_total;
@@ -237,20 +248,22 @@ extract_kernel(DevVolume v, int32_t n_blocks, const int32_t* list, float min_w, 
         if (h.val[hc] < iso) below |= 1u << c;
     }
 
-    int n_vert = 0;
+    // Triangles of this cube (every corner valid, or none).
+    int n_tri = 0;
     if (all_ok) {
         for (int k = 0; k < 6; ++k) {
             const int* tq = c_tets[k];
             const int code = ((below >> tq[0]) & 1) | (((below >> tq[1]) & 1) << 1) |
                              (((below >> tq[2]) & 1) << 2) | (((below >> tq[3]) & 1) << 3);
             int a, bb, c, d;
-            n_vert += 3 * tet_case(code, tq, a, bb, c, d);
+            n_tri += tet_case(code, tq, a, bb, c, d);
         }
     }
+    s_below[t] = (uint8_t)below;
 
-    // Block-wide exclusive scan of the vertex counts.
+    // Block-wide exclusive scan of the triangle counts.
     const int lane = t & 31, warp = t >> 5;
-    int x = n_vert;
+    int x = n_tri;
     for (int o = 1; o < 32; o <<= 1) {
         const int y = __shfl_up_sync(0xffffffffu, x, o);
         if (lane >= o) x += y;
@@ -265,7 +278,7 @@ extract_kernel(DevVolume v, int32_t n_blocks, const int32_t* list, float min_w, 
         }
         if (lane < kExtractThreads / 32) s_warp[lane] = w;
         if (lane == kExtractThreads / 32 - 1) {
-            const int total = w;
+            const int total = 3 * w;  // vertices
             int base = 0;
             if (total > 0) {
                 base = atomicAdd(&ctl[0], total);
@@ -288,31 +301,56 @@ extract_kernel(DevVolume v, int32_t n_blocks, const int32_t* list, float min_w, 
     sink.pad = (int)((reinterpret_cast<uintptr_t>(out_posnor + (int64_t)s_base * 6) >> 2) & 3);
     sink.posnor = out_posnor;
     sink.base = s_base;
-    int at = (warp ? s_warp[warp - 1] : 0) + x - n_vert;  // block-relative
 
-    // Only cubes with every corner valid emit (n_vert counted nothing else);
-    // the others still reach the barrier before the copy-out.
-    for (int k = 0; k < (n_vert > 0 ? 6 : 0); ++k) {
+    // The block's triangle list in output order (cube, tetrahedron, triangle):
+    // item = cube | tetrahedron << 9 | second triangle of a quad << 12.
+    {
+        int at = (warp ? s_warp[warp - 1] : 0) + x - n_tri;
+        for (int k = 0; k < (n_tri > 0 ? 6 : 0); ++k) {
+            const int* tq = c_tets[k];
+            const int code = ((below >> tq[0]) & 1) | (((below >> tq[1]) & 1) << 1) |
+                             (((below >> tq[2]) & 1) << 2) | (((below >> tq[3]) & 1) << 3);
+            int a, bb, c, d;
+            const int kind = tet_case(code, tq, a, bb, c, d);
+            for (int m = 0; m < kind; ++m) s_items[at++] = (uint16_t)(t | k << 9 | m << 12);
+        }
+    }
+    __syncthreads();
+
+    // One thread per triangle: the warps stay converged however sparse the
+    // surface is within the block.
+    const int n_tris = total / 3;
+    for (int j = t; j < n_tris; j += kExtractThreads) {
+        const int item = s_items[j];
+        const int cube = item & (kBlockVoxels - 1), k = (item >> 9) & 7, second = item >> 12;
+        Cube qc;
+        const int cx = cube & 7, cy = (cube >> 3) & 7, cz = cube >> 6;
+        qc.vx = bc.x * kBlockDim + cx;
+        qc.vy = bc.y * kBlockDim + cy;
+        qc.vz = bc.z * kBlockDim + cz;
+        qc.h0 = (cz * kHalo + cy) * kHalo + cx;
+        qc.vs = v.voxel_size;
+        const unsigned bl = s_below[cube];
         const int* tq = c_tets[k];
-        const int code = ((below >> tq[0]) & 1) | (((below >> tq[1]) & 1) << 1) |
-                         (((below >> tq[2]) & 1) << 2) | (((below >> tq[3]) & 1) << 3);
+        const int code = ((bl >> tq[0]) & 1) | (((bl >> tq[1]) & 1) << 1) | (((bl >> tq[2]) & 1) << 2) |
+                         (((bl >> tq[3]) & 1) << 3);
         int a, bb, c, d;
         const int kind = tet_case(code, tq, a, bb, c, d);
+        // marching_tets.cpp:142-163: a single triangle (a-b, a-c, a-d), or the
+        // quad's two (a-c, a-d, b-d) and (a-c, b-d, b-c).
+        int e0a = a, e0b = c, e1a = a, e1b = d, e2a = bb, e2b = d;
         if (kind == 1) {
-            const Vert v0 = interp(h, q, iso, a, bb);
-            const Vert v1 = interp(h, q, iso, a, c);
-            const Vert v2 = interp(h, q, iso, a, d);
-            emit_triangle<COL>(v0, v1, v2, sink, out_rgb, at);
-            at += 3;
-        } else if (kind == 2) {
-            const Vert ac = interp(h, q, iso, a, c);
-            const Vert ad = interp(h, q, iso, a, d);
-            const Vert bd = interp(h, q, iso, bb, d);
-            const Vert bcv = interp(h, q, iso, bb, c);
-            emit_triangle<COL>(ac, ad, bd, sink, out_rgb, at);
-            emit_triangle<COL>(ac, bd, bcv, sink, out_rgb, at + 3);
-            at += 6;
+            e0b = bb;
+            e1b = c;
+            e2a = a;
+        } else if (second) {
+            e1a = bb;
+            e2b = c;
         }
+        const Vert v0 = interp(h, qc, iso, e0a, e0b);
+        const Vert v1 = interp(h, qc, iso, e1a, e1b);
+        const Vert v2 = interp(h, qc, iso, e2a, e2b);
+        emit_triangle<COL>(v0, v1, v2, sink, out_rgb, 3 * j);
     }
     __syncthreads();
     // Copy-out of the staged vertices: 16-byte groups of the output, each
@@ -401,6 +439,17 @@ __global__ void reset_voxels_kernel(DevVolume v, size_t n_voxels) {
 
 }  // namespace
 
+template <int S, bool COL>
+static cudaError_t launch_extract_as(const DevVolume& v, int32_t n_blocks, const int32_t* list, float min_w,
+                                     float iso, float* posnor, uint8_t* rgb, int32_t cap, int32_t* ctl,
+                                     cudaStream_t s) {
+    constexpr int dyn = extract_dyn_smem<COL>();
+    cudaError_t e = cudaFuncSetAttribute(extract_kernel<S, COL>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+    if (e != cudaSuccess) return e;
+    extract_kernel<S, COL><<<n_blocks, kExtractThreads, dyn, s>>>(v, n_blocks, list, min_w, iso, posnor, rgb, cap, ctl);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_extract(const DevVolume& v, int32_t n_blocks, const int32_t* list, float min_w, float iso,
                            float* posnor, uint8_t* rgb, int32_t cap, int32_t* ctl, cudaStream_t s) {
     if (n_blocks <= 0) return cudaSuccess;
@@ -409,19 +458,15 @@ cudaError_t launch_extract(const DevVolume& v, int32_t n_blocks, const int32_t* 
     const bool col = rgb != nullptr;
     switch (v.storage) {
         case kStoreF16U16:
-            if (col) extract_kernel<kStoreF16U16, true><<<n_blocks, kExtractThreads, 0, s>>>(v, n_blocks, list, min_w, iso, posnor, rgb, cap, ctl);
-            else extract_kernel<kStoreF16U16, false><<<n_blocks, kExtractThreads, 0, s>>>(v, n_blocks, list, min_w, iso, posnor, nullptr, cap, ctl);
-            break;
+            return col ? launch_extract_as<kStoreF16U16, true>(v, n_blocks, list, min_w, iso, posnor, rgb, cap, ctl, s)
+                       : launch_extract_as<kStoreF16U16, false>(v, n_blocks, list, min_w, iso, posnor, nullptr, cap, ctl, s);
         case kStoreF64:
-            if (col) extract_kernel<kStoreF64, true><<<n_blocks, kExtractThreads, 0, s>>>(v, n_blocks, list, min_w, iso, posnor, rgb, cap, ctl);
-            else extract_kernel<kStoreF64, false><<<n_blocks, kExtractThreads, 0, s>>>(v, n_blocks, list, min_w, iso, posnor, nullptr, cap, ctl);
-            break;
+            return col ? launch_extract_as<kStoreF64, true>(v, n_blocks, list, min_w, iso, posnor, rgb, cap, ctl, s)
+                       : launch_extract_as<kStoreF64, false>(v, n_blocks, list, min_w, iso, posnor, nullptr, cap, ctl, s);
         default:
-            if (col) extract_kernel<kStoreF32, true><<<n_blocks, kExtractThreads, 0, s>>>(v, n_blocks, list, min_w, iso, posnor, rgb, cap, ctl);
-            else extract_kernel<kStoreF32, false><<<n_blocks, kExtractThreads, 0, s>>>(v, n_blocks, list, min_w, iso, posnor, nullptr, cap, ctl);
-            break;
+            return col ? launch_extract_as<kStoreF32, true>(v, n_blocks, list, min_w, iso, posnor, rgb, cap, ctl, s)
+                       : launch_extract_as<kStoreF32, false>(v, n_blocks, list, min_w, iso, posnor, nullptr, cap, ctl, s);
     }
-    return cudaGetLastError();
 }
 
 cudaError_t launch_reset_table(HashEntry* first, uint32_t count, long long key, cudaStream_t s) {

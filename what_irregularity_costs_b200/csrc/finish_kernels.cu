@@ -82,7 +82,7 @@ constexpr int kSelectWarps = kSelectThreads / 32;
 // Resident 256-thread CTAs per SM the group pass's registers are sized for:
 // the scan is latency-bound, so occupancy hides its round trips.
 #ifndef OSN_GROUP_MIN_BLOCKS
-#define OSN_GROUP_MIN_BLOCKS 5
+#define OSN_GROUP_MIN_BLOCKS 6
 #endif
 static_assert(kFinishThreads >= kMaxBatchScenes && kGroupThreads >= kMaxBatchScenes,
               "one thread per scene builds the item prefix");
@@ -625,47 +625,23 @@ __device__ __forceinline__ uint32_t place_records(const BatchArgs& a, const DevV
     for (int m = 1; m < kGroupPerThread; ++m)
         if (same[m]) word[m] = word[m - 1];
     const uint32_t n_steps = 2u * (uint32_t)v.steps + 1u;
-    bool cross[kGroupPerThread];
-#pragma unroll
-    for (int m = 0; m < kGroupPerThread; ++m)
-        cross[m] = vi[m] != kNoVoxel && ((word[m] >> (vi[m] & 31u)) & 1u);
-    // Neighbouring pixels at one band step often share a voxel: a run of
-    // consecutive slots of one crossing voxel takes all its places with one
-    // atomic. run[m] = the run's records from slot m on.
-    int run[kGroupPerThread];
-    run[kGroupPerThread - 1] = cross[kGroupPerThread - 1] ? 1 : 0;
-#pragma unroll
-    for (int m = kGroupPerThread - 2; m >= 0; --m)
-        run[m] = cross[m] ? ((cross[m + 1] && vi[m + 1] == vi[m]) ? run[m + 1] + 1 : 1) : 0;
-    // The records' values (FP32 / FP16: the walk kept them) are loaded beside
-    // the place tickets, in the same round trip.
-    float val[kGroupPerThread];
-#pragma unroll
-    for (int m = 0; m < kGroupPerThread; ++m) {
-        val[m] = 0.0f;
-        if constexpr (S != kStoreF64)
-            if (cross[m]) val[m] = __ldcs(u.slot_val + first + m);
-    }
-    unsigned long long tk[kGroupPerThread];
-#pragma unroll
-    for (int m = 0; m < kGroupPerThread; ++m) {
-        tk[m] = 0ull;
-        if (!cross[m]) continue;
-        const bool starts = !(m > 0 && cross[m - 1] && vi[m - 1] == vi[m]);
-        tk[m] = starts ? atomicAdd(&u.vacc[vi[m]], (unsigned long long)run[m]) : tk[m > 0 ? m - 1 : 0] + 1ull;
-    }
     uint32_t placed = 0u;  // bit m: slot m's record took a place in its group
 #pragma unroll
     for (int m = 0; m < kGroupPerThread; ++m) {
-        if (!cross[m]) continue;
+        if (vi[m] == kNoVoxel || !((word[m] >> (vi[m] & 31u)) & 1u)) continue;
         const uint32_t slot = first + m;
-        const uint64_t pos = (uint64_t)((uint32_t)(tk[m] >> 32) - 1u) + (uint32_t)tk[m];
+        // The record's value (FP32 / FP16: the walk kept it) is loaded beside
+        // its place ticket, in the same round trip.
+        float val = 0.0f;
+        if constexpr (S != kStoreF64) val = __ldcs(u.slot_val + slot);
+        const unsigned long long tk = atomicAdd(&u.vacc[vi[m]], 1ull);
+        const uint64_t pos = (uint64_t)((uint32_t)(tk >> 32) - 1u) + (uint32_t)tk;
         unsigned long long e;
         if constexpr (S == kStoreF64)
             e = slot;
         else
             e = (unsigned long long)slot_id(slot, (uint32_t)a.n, n_steps) |
-                ((unsigned long long)__float_as_uint(val[m]) << 32);
+                ((unsigned long long)__float_as_uint(val) << 32);
         if (pos < (uint64_t)u.record_cap) u.grp[pos] = e;
         else atomicOr(u.status, kStatusScratchOverflow);  // state left by a failed update
         placed |= 1u << m;
