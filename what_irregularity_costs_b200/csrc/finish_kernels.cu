@@ -690,31 +690,40 @@ __device__ __forceinline__ void group_slots(const DevVolume& v, const BatchArgs&
 template <int S>
 __global__ void __launch_bounds__(kGroupThreads, OSN_GROUP_MIN_BLOCKS)
 group_kernel(DevVolume v, BatchArgs a, UpdateScratch u, uint32_t n_slots) {
+    launch_dependents();
+    grid_dependency_wait();
+    if (u.ctl->n_crossing == 0ull) return;  // no voxel crossed the cap in this batch
+    if (OSN_SPLIT_SELECT) {
+        // Placing only: no voxel is finished here, so there is nothing to
+        // count and no CTA barrier (each warp leaves when its slots are done).
+        if (OSN_GROUP_PERSISTENT) {
+            // Persistent grid: each thread walks chunks of eight slots a grid
+            // apart, the next chunk's records loaded before this one's are placed.
+            const uint32_t stride = gridDim.x * kGroupThreads * kGroupPerThread;
+            uint32_t first = (blockIdx.x * kGroupThreads + threadIdx.x) * kGroupPerThread;
+            uint32_t cur[kGroupPerThread], nxt[kGroupPerThread];
+            load_records(u, first, n_slots, cur);
+            for (; first < n_slots; first += stride) {
+                load_records(u, first + stride, n_slots, nxt);
+                place_records<S>(a, v, u, first, cur);
+#pragma unroll
+                for (int m = 0; m < kGroupPerThread; ++m) cur[m] = nxt[m];
+            }
+        } else {
+            const uint32_t first = (blockIdx.x * kGroupThreads + threadIdx.x) * kGroupPerThread;
+            uint32_t vi[kGroupPerThread];
+            load_records(u, first, n_slots, vi);
+            place_records<S>(a, v, u, first, vi);
+        }
+        return;
+    }
     __shared__ uint32_t hist[kGroupWarps][256];
     __shared__ int s_updated;
     if (threadIdx.x == 0) s_updated = 0;
     __syncthreads();
-    launch_dependents();
-    grid_dependency_wait();
-    if (u.ctl->n_crossing == 0ull) return;  // no voxel crossed the cap in this batch
     int updated = 0;
-    if (OSN_SPLIT_SELECT && OSN_GROUP_PERSISTENT) {
-        // Persistent grid: each thread walks chunks of eight slots a grid
-        // apart, the next chunk's records loaded before this one's are placed.
-        const uint32_t stride = gridDim.x * kGroupThreads * kGroupPerThread;
-        uint32_t first = (blockIdx.x * kGroupThreads + threadIdx.x) * kGroupPerThread;
-        uint32_t cur[kGroupPerThread], nxt[kGroupPerThread];
-        load_records(u, first, n_slots, cur);
-        for (; first < n_slots; first += stride) {
-            load_records(u, first + stride, n_slots, nxt);
-            place_records<S>(a, v, u, first, cur);
-#pragma unroll
-            for (int m = 0; m < kGroupPerThread; ++m) cur[m] = nxt[m];
-        }
-    } else {
-        group_slots<S>(v, a, u, (blockIdx.x * kGroupThreads + threadIdx.x) * kGroupPerThread, n_slots,
-                       hist[threadIdx.x >> 5], updated);
-    }
+    group_slots<S>(v, a, u, (blockIdx.x * kGroupThreads + threadIdx.x) * kGroupPerThread, n_slots,
+                   hist[threadIdx.x >> 5], updated);
     cta_add(&s_updated, updated, &u.ctl->n_updated);
 }
 
