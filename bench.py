@@ -7,8 +7,9 @@ update of every frame through the C ABI. frames/s = frames integrated / time.
 
   value  device-resident points (uploaded once), CUDA events on the volume's
          stream around exactly K steps, max over ranks; the frames go through
-         osn_tsdf_cuda_integrate_frames, 3 consecutive frames per call
-         (--frames-per-call), with pipelined updates. value_per_frame: one
+         osn_tsdf_cuda_integrate_frames, 4 consecutive frames per call
+         (--frames-per-call), serial updates (value_frames_pipelined: the
+         same with pipelined updates). value_per_frame: one
          osn_tsdf_cuda_integrate call per frame, pipelined; value_serial:
          one call per frame, serial;
   e2e    the headline arm from pinned HOST buffers: every call's points are
@@ -51,7 +52,7 @@ VOXEL, TRUNC, CAP = 0.02, 0.08, 64.0
 SLOTS_PER_POINT = 2 * 4 + 1   # band samples per point: 2 * ceil(trunc / voxel) + 1
 HASH_SLOTS, POOL = 1 << 20, 1 << 19
 N_FRAMES, SEED = 100, 0
-FRAMES_PER_CALL = 3  # frames per osn_tsdf_cuda_integrate_frames call in the headline arm
+FRAMES_PER_CALL = 4  # frames per osn_tsdf_cuda_integrate_frames call in the headline arm
 METRIC = "frames/s (640x480 integrate)"
 PROFILES = os.path.join(ROOT, "profiles")
 
@@ -457,7 +458,13 @@ def run_ours(args):
     # tail overlaps the next walk)
     vol.set_pipelined(True)
     per_frame_ms = timed(step_device, args.steps)
-    # -- value: FRAMES_PER_CALL frames per integrate_frames call, pipelined
+    # -- value_frames_pipelined: FRAMES_PER_CALL frames per call, pipelined
+    frames_pipe_ms = timed(step_frames, args.steps)
+    # -- value: FRAMES_PER_CALL frames per integrate_frames call, serial
+    # updates (every kernel of a call launched behind its predecessor on the
+    # volume's stream; measured faster than the pipelined form at 3-8 frames
+    # per call, whose cross-stream waits cost more than the overlap gains)
+    vol.set_pipelined(False)
     ms = timed(step_frames, args.steps)
     blocks = vol.block_count()
     drops = vol.drop_count()
@@ -506,10 +513,12 @@ def run_ours(args):
 
     for s in range(2):
         free[s].record(vstream)
-    # e2e_per_frame: one integrate call per frame
+    # e2e_per_frame: one integrate call per frame, pipelined updates
+    vol.set_pipelined(True)
     e2e_pf_ms = timed(step_e2e, args.steps)
     e2e_per_frame = frames_total / (e2e_pf_ms / 1e3)
-    # e2e: the headline arm (FRAMES_PER_CALL frames per call)
+    # e2e: the headline arm (FRAMES_PER_CALL frames per call, serial updates)
+    vol.set_pipelined(False)
     e2e_ms = timed(step_e2e_frames, args.steps)
     e2e_value = frames_total / (e2e_ms / 1e3)
 
@@ -535,7 +544,9 @@ def run_ours(args):
         result[0] = vol.block_count()
         result[1] = vol.drop_count()
 
+    vol.set_pipelined(True)
     e2e_depth_ms = timed(step_e2e_depth, args.steps)
+    vol.set_pipelined(False)
     blocks_depth = vol.block_count()
 
     # -- the same with several depth images per call (integrate_depth_frames)
@@ -732,7 +743,7 @@ def run_ours(args):
     if rank == 0 and not args.no_parity:
         try:
             parity = parity_vs_oracle(headline_voxels, pts, cams,
-                                      f"osn_tsdf_cuda_integrate_frames, {fpc} frames per call, pipelined")
+                                      f"osn_tsdf_cuda_integrate_frames, {fpc} frames per call")
         except Exception as e:  # reported, never fatal to the line
             parity = {"ok": False, "error": str(e)}
 
@@ -757,7 +768,9 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world,
             "value_per_frame": frames_total / (per_frame_ms / 1e3),
             "value_serial": frames_total / (serial_ms / 1e3),
-            "mode": f"osn_tsdf_cuda_integrate_frames, {fpc} frames per call, pipelined updates; "
+            "value_frames_pipelined": frames_total / (frames_pipe_ms / 1e3),
+            "mode": f"osn_tsdf_cuda_integrate_frames, {fpc} frames per call, serial updates; "
+                    "value_frames_pipelined: the same with pipelined updates; "
                     "value_per_frame: one osn_tsdf_cuda_integrate per frame, pipelined; "
                     "value_serial: one per frame, serial",
             "frames_per_call": fpc,

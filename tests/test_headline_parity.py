@@ -2,8 +2,8 @@
 
 bench.py's headline figure integrates the full room trajectory (100 frames
 of 640x480, 2 cm voxels, trunc 8 cm, 2^20 table slots, pool 2^19, cap 64)
-with three consecutive frames per osn_tsdf_cuda_integrate_frames call and
-pipelined updates. This test runs exactly that sequence -- the same frames,
+with four consecutive frames per osn_tsdf_cuda_integrate_frames call
+(bench.FRAMES_PER_CALL) and serial updates. This test runs exactly that sequence -- the same frames,
 the same grouping (bench.frame_groups) and the same volume settings -- and
 compares the result with the CPU oracle fed one frame at a time: block set
 bit-exact, weights and colour sums exact, mean TSDF within 1e-5, and the
@@ -36,9 +36,8 @@ def test_headline_run_matches_oracle(cuda, trajectory):
     offsets = np.concatenate([[0], np.cumsum([p.shape[0] for p in pts])])
     d_all = cuda.from_numpy(np.concatenate(pts).astype(np.float32)).cuda()
     vol = CudaVolume(bench.VOXEL, bench.POOL, bench.TRUNC, bench.CAP, bench.HASH_SLOTS)
-    vol.set_pipelined(True)
     groups = bench.frame_groups(offsets, cams, bench.FRAMES_PER_CALL)
-    assert len(groups) == 34
+    assert len(groups) == -(-bench.N_FRAMES // bench.FRAMES_PER_CALL)
     crossing = 0
     for lo, hi, a, b, begin, gcams in groups:
         vol.integrate_frames(d_all[a:b], begin, gcams)

@@ -791,19 +791,25 @@ __device__ __forceinline__ int select_stream(const SelectArgs& sa, const uint32_
             const int kj = __shfl_sync(0xffffffffu, keep, j);
             long long fix = 0ll;
             if (cj <= 32) {  // warp-uniform
+                // Padding ids (0xFFFFFFFF) never rank below a record, so the
+                // ids are read four lanes at a time up to the group's size.
                 const uint32_t id = lane < cj ? (uint32_t)ej : 0xFFFFFFFFu;
                 int rank = 0;
+                for (int q = 0; q < cj; q += 4) {
 #pragma unroll
-                for (int q = 0; q < 32; ++q) {
-                    const uint32_t other = __shfl_sync(0xffffffffu, id, q);
-                    rank += (q < cj && other < id) ? 1 : 0;
+                    for (int r = 0; r < 4; ++r) rank += __shfl_sync(0xffffffffu, id, q + r) < id ? 1 : 0;
                 }
                 if (lane < cj && rank < kj) fix = to_fix(__uint_as_float((uint32_t)(ej >> 32)));
+                // One value per lane, |fix| <= 2^40: the warp sums of the
+                // 20-bit low parts and of the high parts fit 26 bits.
+                const uint32_t lo = __reduce_add_sync(0xffffffffu, (uint32_t)fix & 0xFFFFFu);
+                const int32_t hi = (int32_t)__reduce_add_sync(0xffffffffu, (uint32_t)(int32_t)(fix >> 20));
+                fix = ((long long)hi << 20) + (long long)lo;
             } else {
                 const uint32_t bj = __shfl_sync(0xffffffffu, base, j);
                 fix = large_group_sum<S>(DevVolume{}, BatchArgs{}, sa.grp + bj, cj, kj, hist, lane);
+                for (int o = 16; o > 0; o >>= 1) fix += __shfl_xor_sync(0xffffffffu, fix, o);
             }
-            for (int o = 16; o > 0; o >>= 1) fix += __shfl_xor_sync(0xffffffffu, fix, o);
             if (lane == j) my_fix = fix;
         }
         if (!mine) continue;
