@@ -28,35 +28,80 @@ constexpr int kHalo = 9;
 constexpr int kHaloCells = kHalo * kHalo * kHalo;
 
 // marching_tets.cpp:37-40: six tetrahedra around the 0-7 diagonal.
-__constant__ int c_tets[6][4] = {
+constexpr int kTetCorners[6][4] = {
     {0, 5, 1, 7}, {0, 1, 3, 7}, {0, 3, 2, 7}, {0, 6, 4, 7}, {0, 4, 5, 7}, {0, 2, 6, 7},
 };
+
+// A tetrahedron's case code (bit i: its corner i is below iso) gives its
+// crossing (marching_tets.cpp:165-182): none (0000, 1111), one triangle from
+// the corner on its own side (one or three bits set), or a quad split in two
+// (two bits set).
+constexpr int popc4(int x) { return (x & 1) + ((x >> 1) & 1) + ((x >> 2) & 1) + ((x >> 3) & 1); }
+constexpr int tris_of_code(int code) { return (popc4(code) & 1) ? 1 : (popc4(code) == 2 ? 2 : 0); }
+constexpr int tet_code(int below, int k) {
+    int code = 0;
+    for (int i = 0; i < 4; ++i) code |= ((below >> kTetCorners[k][i]) & 1) << i;
+    return code;
+}
+
+// Tables the kernel stages in shared memory (constant-bank reads with lane-
+// dependent indices would serialise):
+//   kinds[below]   the six tetrahedra's triangle counts (2 bits each) of a
+//                  cube whose corners below iso are the bits of `below`;
+//   cases[k][code] tetrahedron k's corners (a, b, c, d) in the order the
+//                  case table of marching_tets.cpp:165-182 names them (3 bits
+//                  each) and its triangle count (bits 12-13);
+//   corners[k]     tetrahedron k's four corners (3 bits each).
+struct alignas(4) TetTables {
+    uint16_t kinds[256];
+    uint16_t cases[6][16];
+    uint16_t corners[6];
+};
+constexpr int case_perm(int code) {  // (a, b, c, d) as positions in the tetrahedron
+    switch (code) {
+        case 0x01: case 0x0E: case 0x03: return 0 | 1 << 2 | 2 << 4 | 3 << 6;
+        case 0x02: case 0x0D: return 1 | 0 << 2 | 2 << 4 | 3 << 6;
+        case 0x04: case 0x0B: return 2 | 0 << 2 | 1 << 4 | 3 << 6;
+        case 0x08: case 0x07: return 3 | 0 << 2 | 1 << 4 | 2 << 6;
+        case 0x0C: return 2 | 3 << 2 | 0 << 4 | 1 << 6;
+        case 0x05: return 0 | 2 << 2 | 1 << 4 | 3 << 6;
+        case 0x0A: return 1 | 3 << 2 | 0 << 4 | 2 << 6;
+        case 0x06: return 1 | 2 << 2 | 0 << 4 | 3 << 6;
+        case 0x09: return 0 | 3 << 2 | 1 << 4 | 2 << 6;
+        default: return 0;
+    }
+}
+constexpr TetTables make_tet_tables() {
+    TetTables t{};
+    for (int b = 0; b < 256; ++b) {
+        int v = 0;
+        for (int k = 0; k < 6; ++k) v |= tris_of_code(tet_code(b, k)) << (2 * k);
+        t.kinds[b] = (uint16_t)v;
+    }
+    for (int k = 0; k < 6; ++k) {
+        int c = 0;
+        for (int i = 0; i < 4; ++i) c |= kTetCorners[k][i] << (3 * i);
+        t.corners[k] = (uint16_t)c;
+        for (int code = 0; code < 16; ++code) {
+            const int p = case_perm(code);
+            int e = 0;
+            for (int i = 0; i < 4; ++i) e |= kTetCorners[k][(p >> (2 * i)) & 3] << (3 * i);
+            t.cases[k][code] = (uint16_t)(e | tris_of_code(code) << 12);
+        }
+    }
+    return t;
+}
+__constant__ TetTables c_tet_tables = make_tet_tables();
+static_assert(make_tet_tables().kinds[0] == 0 && make_tet_tables().kinds[255] == 0, "no crossing");
+static_assert(make_tet_tables().kinds[1] == 0x555, "corner 0 alone: one triangle in every tetrahedron");
 
 // The block's 9^3 corner samples; colours only when the caller wants them.
 template <bool COL>
 struct Halo {
     float val[kHaloCells];
     float col[COL ? 3 : 1][COL ? kHaloCells : 1];
-    unsigned char ok[kHaloCells];
+    unsigned char flag[kHaloCells];  // bit 0: valid sample; bit 1: valid and below iso
 };
-
-// Case table of marching_tets.cpp:165-182 as (a, b, c, d, quad).
-__device__ __forceinline__ int tet_case(int code, const int* q, int& a, int& b, int& c, int& d) {
-    const int i0 = q[0], i1 = q[1], i2 = q[2], i3 = q[3];
-    switch (code) {
-        case 0x01: case 0x0E: a = i0; b = i1; c = i2; d = i3; return 1;
-        case 0x02: case 0x0D: a = i1; b = i0; c = i2; d = i3; return 1;
-        case 0x04: case 0x0B: a = i2; b = i0; c = i1; d = i3; return 1;
-        case 0x08: case 0x07: a = i3; b = i0; c = i1; d = i2; return 1;
-        case 0x03: a = i0; b = i1; c = i2; d = i3; return 2;
-        case 0x0C: a = i2; b = i3; c = i0; d = i1; return 2;
-        case 0x05: a = i0; b = i2; c = i1; d = i3; return 2;
-        case 0x0A: a = i1; b = i3; c = i0; d = i2; return 2;
-        case 0x06: a = i1; b = i2; c = i0; d = i3; return 2;
-        case 0x09: a = i0; b = i3; c = i1; d = i2; return 2;
-        default: return 0;
-    }
-}
 
 struct Cube {
     int vx, vy, vz;  // voxel coordinate of corner 0
@@ -83,14 +128,17 @@ struct Vert {
 // marching_tets.cpp:59-80: position-ordered interpolation.
 template <bool COL>
 __device__ __forceinline__ Vert interp(const Halo<COL>& h, const Cube& q, float iso, int ia, int ib) {
-    float pa[3], pb[3];
-    corner_pos(q, ia, pa);
-    corner_pos(q, ib, pb);
-    const bool sw = (pb[0] < pa[0]) || (pb[0] == pa[0] && pb[1] < pa[1]) ||
-                    (pb[0] == pa[0] && pb[1] == pa[1] && pb[2] < pa[2]);
+    // The corner with the smaller position (x, then y, then z) first. Corner
+    // positions are increasing functions of the corner's offset bits on each
+    // axis (same cube), so comparing the offsets (x, y, z) as a 3-bit number
+    // orders the positions exactly.
+    const int ka = ((ia & 1) << 2) | (ia & 2) | ((ia >> 2) & 1);
+    const int kb = ((ib & 1) << 2) | (ib & 2) | ((ib >> 2) & 1);
+    const bool sw = kb < ka;
     const int i0 = sw ? ib : ia, i1 = sw ? ia : ib;
-    const float* p0 = sw ? pb : pa;
-    const float* p1 = sw ? pa : pb;
+    float p0[3], p1[3];
+    corner_pos(q, i0, p0);
+    corner_pos(q, i1, p1);
     const int h0 = corner_halo(q, i0), h1 = corner_halo(q, i1);
     const float v0 = h.val[h0], v1 = h.val[h1];
     const float den = __fsub_rn(v1, v0);
@@ -180,6 +228,7 @@ extract_kernel(DevVolume v, int32_t n_blocks, const int32_t* list, float min_w, 
                uint8_t* out_rgb, int32_t cap, int32_t* ctl) {
     __shared__ Halo<COL> h;
     __shared__ uint8_t s_below[kBlockVoxels];
+    __shared__ TetTables s_tab;
     extern __shared__ __align__(16) float s_dyn[];
     float* const s_stage = s_dyn;
     uint16_t* const s_items = reinterpret_cast<uint16_t*>(s_dyn + 4 + stage_verts<COL>() * 6);
@@ -196,6 +245,8 @@ extract_kernel(DevVolume v, int32_t n_blocks, const int32_t* list, float min_w, 
         const int nx = bc.x + dx, ny = bc.y + dy, nz = bc.z + dz;
         s_nb[t] = t == 0 ? b : find_block(v, nx, ny, nz, pack_key(nx, ny, nz));
     }
+    for (int k = t; k < (int)(sizeof(TetTables) / 4); k += kExtractThreads)
+        reinterpret_cast<uint32_t*>(&s_tab)[k] = reinterpret_cast<const uint32_t*>(&c_tet_tables)[k];
     __syncthreads();
 
     // Stage the halo: corner samples of this block plus the +x/+y/+z faces,
@@ -203,7 +254,7 @@ extract_kernel(DevVolume v, int32_t n_blocks, const int32_t* list, float min_w, 
     for (int k = t; k < kHaloCells; k += kExtractThreads) {
         const int hx = k % kHalo, hy = (k / kHalo) % kHalo, hz = k / (kHalo * kHalo);
         const int nb = s_nb[(hx >> 3) | ((hy >> 3) << 1) | ((hz >> 3) << 2)];
-        unsigned char ok = 0;
+        unsigned char flag = 0;
         h.val[k] = 0.0f;
         if (nb >= 0) {
             const size_t idx = (size_t)nb * kBlockVoxels + (size_t)((((hz & 7) * kBlockDim) + (hy & 7)) * kBlockDim + (hx & 7));
@@ -211,7 +262,7 @@ extract_kernel(DevVolume v, int32_t n_blocks, const int32_t* list, float min_w, 
             const float w = weight_at<S>(v, idx);
             const float m = mean_from<S>(v, idx, w);
             if (!(w < min_w || w <= 0.0f)) {
-                ok = 1;
+                flag = m < iso ? 3 : 1;
                 h.val[k] = m;
                 if constexpr (COL) {
                     if constexpr (S == kStoreF32) {
@@ -228,7 +279,7 @@ extract_kernel(DevVolume v, int32_t n_blocks, const int32_t* list, float min_w, 
                 }
             }
         }
-        h.ok[k] = ok;
+        h.flag[k] = flag;
     }
     __syncthreads();
 
@@ -240,25 +291,18 @@ extract_kernel(DevVolume v, int32_t n_blocks, const int32_t* list, float min_w, 
     q.h0 = (lz * kHalo + ly) * kHalo + lx;
     q.vs = v.voxel_size;
 
-    bool all_ok = true;
+    unsigned all_ok = 1u;
     unsigned below = 0;  // bit c set when corner c is below iso
+#pragma unroll
     for (int c = 0; c < 8; ++c) {
-        const int hc = corner_halo(q, c);
-        all_ok = all_ok && h.ok[hc];
-        if (h.val[hc] < iso) below |= 1u << c;
+        const unsigned f = h.flag[corner_halo(q, c)];
+        all_ok &= f;
+        below |= (f >> 1) << c;
     }
 
     // Triangles of this cube (every corner valid, or none).
-    int n_tri = 0;
-    if (all_ok) {
-        for (int k = 0; k < 6; ++k) {
-            const int* tq = c_tets[k];
-            const int code = ((below >> tq[0]) & 1) | (((below >> tq[1]) & 1) << 1) |
-                             (((below >> tq[2]) & 1) << 2) | (((below >> tq[3]) & 1) << 3);
-            int a, bb, c, d;
-            n_tri += tet_case(code, tq, a, bb, c, d);
-        }
-    }
+    const unsigned kinds = (all_ok & 1u) ? s_tab.kinds[below] : 0u;
+    const int n_tri = __popc(kinds & 0x555u) + 2 * __popc(kinds & 0xAAAu);
     s_below[t] = (uint8_t)below;
 
     // Block-wide exclusive scan of the triangle counts.
@@ -307,11 +351,7 @@ extract_kernel(DevVolume v, int32_t n_blocks, const int32_t* list, float min_w, 
     {
         int at = (warp ? s_warp[warp - 1] : 0) + x - n_tri;
         for (int k = 0; k < (n_tri > 0 ? 6 : 0); ++k) {
-            const int* tq = c_tets[k];
-            const int code = ((below >> tq[0]) & 1) | (((below >> tq[1]) & 1) << 1) |
-                             (((below >> tq[2]) & 1) << 2) | (((below >> tq[3]) & 1) << 3);
-            int a, bb, c, d;
-            const int kind = tet_case(code, tq, a, bb, c, d);
+            const int kind = (int)(kinds >> (2 * k)) & 3;
             for (int m = 0; m < kind; ++m) s_items[at++] = (uint16_t)(t | k << 9 | m << 12);
         }
     }
@@ -331,15 +371,15 @@ extract_kernel(DevVolume v, int32_t n_blocks, const int32_t* list, float min_w, 
         qc.h0 = (cz * kHalo + cy) * kHalo + cx;
         qc.vs = v.voxel_size;
         const unsigned bl = s_below[cube];
-        const int* tq = c_tets[k];
-        const int code = ((bl >> tq[0]) & 1) | (((bl >> tq[1]) & 1) << 1) | (((bl >> tq[2]) & 1) << 2) |
-                         (((bl >> tq[3]) & 1) << 3);
-        int a, bb, c, d;
-        const int kind = tet_case(code, tq, a, bb, c, d);
+        const unsigned tc = s_tab.corners[k];
+        const int code = (int)(((bl >> (tc & 7u)) & 1u) | (((bl >> ((tc >> 3) & 7u)) & 1u) << 1) |
+                               (((bl >> ((tc >> 6) & 7u)) & 1u) << 2) | (((bl >> (tc >> 9)) & 1u) << 3));
+        const unsigned e = s_tab.cases[k][code];
+        const int a = (int)(e & 7u), bb = (int)((e >> 3) & 7u), c = (int)((e >> 6) & 7u), d = (int)((e >> 9) & 7u);
         // marching_tets.cpp:142-163: a single triangle (a-b, a-c, a-d), or the
         // quad's two (a-c, a-d, b-d) and (a-c, b-d, b-c).
         int e0a = a, e0b = c, e1a = a, e1b = d, e2a = bb, e2b = d;
-        if (kind == 1) {
+        if ((e >> 12) == 1u) {
             e0b = bb;
             e1b = c;
             e2a = a;
