@@ -667,7 +667,8 @@ def run_ours(args):
     roofline = {
         "bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
         "frac": achieved / peak, "peak_source": peak_kind,
-        "traffic": profile_traffic(dominant),
+        # The headline's walk launches are band_frames_kernel (several frames per call).
+        "traffic": profile_traffic("band_frames" if dominant == "band" and fpc > 1 else dominant),
         "alg_bytes_per_launch": dom_alg, "mean_launch_us": 1e3 * dom_ms / dom_n if dom_n else None,
     }
     # The roofs the L2-resident kernels are judged against: the band walk's
