@@ -56,12 +56,18 @@ static_assert(kBandThreads >= kMaxBatchScenes, "one thread per scene builds the 
 #define OSN_BAND_CHUNK 9
 #endif
 constexpr int kChunk = OSN_BAND_CHUNK;  // samples per ray held in registers (9: the whole band at 4 voxels)
-// Resident CTAs per SM the register budget is sized for: 7 (72 registers)
-// measured 1.4 % faster on the room trajectory than 8 (64 registers) and 6.
+// Resident CTAs per SM the register budget is sized for. The several-frame
+// and batched walks: 7 (72 registers), measured 1.4 % faster on the room
+// trajectory than 8 (64 registers) and 6; the one-frame walk: 8 (at 7 it
+// measured 6 % slower, its batches are a third of the size).
 #ifndef OSN_BAND_MIN_BLOCKS
-#define OSN_BAND_MIN_BLOCKS 7
+#define OSN_BAND_MIN_BLOCKS 8
+#endif
+#ifndef OSN_BAND_FRAMES_MIN_BLOCKS
+#define OSN_BAND_FRAMES_MIN_BLOCKS 7
 #endif
 constexpr int kBandMinBlocks = OSN_BAND_MIN_BLOCKS;
+constexpr int kBandFramesMinBlocks = OSN_BAND_FRAMES_MIN_BLOCKS;
 
 // Band records and slot values are read once more, by the group pass of the
 // same update: stored with the streaming hint (1, evict-first) or as
@@ -455,7 +461,7 @@ band_kernel(DevVolume v, BatchArgs a, UpdateScratch u, unsigned long long* hist,
 // Integrate (allocate + count-and-sum) of a batch of several frames: the
 // single-frame walk with each point's camera taken from the frame table.
 template <int S>
-__global__ void __launch_bounds__(kBandThreads, kBandMinBlocks)
+__global__ void __launch_bounds__(kBandThreads, kBandFramesMinBlocks)
 band_frames_kernel(DevVolume v, BatchArgs a, UpdateScratch u, const FrameCam* frames, int32_t n_frames) {
     band_tiles<kAllocInsert, true, S, true>(v, a, u, nullptr, 0, BatchPoints<0>{a}, FrameCursor(frames, n_frames));
 }
@@ -463,7 +469,7 @@ band_frames_kernel(DevVolume v, BatchArgs a, UpdateScratch u, const FrameCam* fr
 // The same for several depth images of equal size: each CTA stages the
 // images' poses in shared memory first.
 template <int S>
-__global__ void __launch_bounds__(kBandThreads, kBandMinBlocks)
+__global__ void __launch_bounds__(kBandThreads, kBandFramesMinBlocks)
 band_depth_frames_kernel(DevVolume v, BatchArgs a, UpdateScratch u, const FrameCam* frames,
                          const FramePose* poses, int32_t n_frames) {
     __shared__ FramePose s_pose[kMaxDepthFrames];
@@ -530,7 +536,7 @@ __device__ __forceinline__ int scene_of(const int* begin, int n, int item) {
 // item's scene descriptor in shared memory and flushes its per-scene
 // counters whenever it moves to another scene.
 template <int S, int PROBE>
-__global__ void __launch_bounds__(kBandThreads, kBandMinBlocks)
+__global__ void __launch_bounds__(kBandThreads, kBandFramesMinBlocks)
 band_multi_kernel(StepWork w) {
     __shared__ BandSmem sm;
     __shared__ SceneWork sw;
