@@ -72,6 +72,14 @@ constexpr int kBandFramesMinBlocks = OSN_BAND_FRAMES_MIN_BLOCKS;
 // Band records and slot values are read once more, by the group pass of the
 // same update: stored with the streaming hint (1, evict-first) or as
 // ordinary write-back stores that may stay in L2 (0).
+// 1: a several-frame walk is launched with programmatic stream serialisation
+// behind its one-CTA set-up kernel, so its CTAs are resident when the set-up
+// ends (they wait for it on the device; measured 0.8 % faster on the room
+// trajectory); 0: an ordinary launch.
+#ifndef OSN_BAND_PDL
+#define OSN_BAND_PDL 1
+#endif
+
 #ifndef OSN_BAND_STREAM_RECORDS
 #define OSN_BAND_STREAM_RECORDS 1
 #endif
@@ -463,6 +471,7 @@ band_kernel(DevVolume v, BatchArgs a, UpdateScratch u, unsigned long long* hist,
 template <int S>
 __global__ void __launch_bounds__(kBandThreads, kBandFramesMinBlocks)
 band_frames_kernel(DevVolume v, BatchArgs a, UpdateScratch u, const FrameCam* frames, int32_t n_frames) {
+    if (OSN_BAND_PDL) grid_dependency_wait();  // the set-up kernel's frame table and zeroed counters
     band_tiles<kAllocInsert, true, S, true>(v, a, u, nullptr, 0, BatchPoints<0>{a}, FrameCursor(frames, n_frames));
 }
 
@@ -473,6 +482,7 @@ __global__ void __launch_bounds__(kBandThreads, kBandFramesMinBlocks)
 band_depth_frames_kernel(DevVolume v, BatchArgs a, UpdateScratch u, const FrameCam* frames,
                          const FramePose* poses, int32_t n_frames) {
     __shared__ FramePose s_pose[kMaxDepthFrames];
+    if (OSN_BAND_PDL) grid_dependency_wait();  // the set-up kernel's tables and zeroed counters
     constexpr int kWords = (int)(sizeof(FramePose) / sizeof(double));
     for (int k = threadIdx.x; k < n_frames * kWords; k += blockDim.x)
         reinterpret_cast<double*>(s_pose)[k] = __ldg(reinterpret_cast<const double*>(poses) + k);
@@ -486,6 +496,7 @@ band_depth_frames_kernel(DevVolume v, BatchArgs a, UpdateScratch u, const FrameC
 // walk reads it (one CTA; static indices only, so the table stays in the
 // parameter space).
 __global__ void frames_setup_kernel(UpdateControl* ctl, FrameCam* dst, const FrameTable t) {
+    if (OSN_BAND_PDL) launch_dependents();  // the walk's CTAs may take their places now
     const int k = threadIdx.x;
     if (k < (int)(sizeof(UpdateControl) / sizeof(uint32_t))) reinterpret_cast<uint32_t*>(ctl)[k] = 0u;
 #pragma unroll
@@ -496,6 +507,7 @@ __global__ void frames_setup_kernel(UpdateControl* ctl, FrameCam* dst, const Fra
 // The same for several depth images, with their poses.
 __global__ void frames_setup_depth_kernel(UpdateControl* ctl, FrameCam* dst, const FrameTable t,
                                           FramePose* pdst, const PoseTable p) {
+    if (OSN_BAND_PDL) launch_dependents();
     const int k = threadIdx.x;
     if (k < (int)(sizeof(UpdateControl) / sizeof(uint32_t))) reinterpret_cast<uint32_t*>(ctl)[k] = 0u;
 #pragma unroll
@@ -679,6 +691,7 @@ cudaError_t launch_band_frames_t(const DevVolume& v, const BatchArgs& a, const U
     });
     const int tiles = (a.n + kBandThreads - 1) / kBandThreads;
     const int grid = std::min(tiles, per_sm * sm_count);
+    if (OSN_BAND_PDL) return launch_after(band_frames_kernel<S>, grid, kBandThreads, s, v, a, u, frames, n_frames);
     band_frames_kernel<S><<<grid, kBandThreads, 0, s>>>(v, a, u, frames, n_frames);
     return cudaGetLastError();
 }
@@ -696,6 +709,8 @@ cudaError_t launch_band_depth_frames_t(const DevVolume& v, const BatchArgs& a, c
     });
     const int tiles = (a.n + kBandThreads - 1) / kBandThreads;
     const int grid = std::min(tiles, per_sm * sm_count);
+    if (OSN_BAND_PDL)
+        return launch_after(band_depth_frames_kernel<S>, grid, kBandThreads, s, v, a, u, frames, poses, n_frames);
     band_depth_frames_kernel<S><<<grid, kBandThreads, 0, s>>>(v, a, u, frames, poses, n_frames);
     return cudaGetLastError();
 }
